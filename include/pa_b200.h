@@ -1,0 +1,184 @@
+/*
+ * pa_b200.h -- C-ABI of libpa_b200.so, the B200 (sm_100a) implementation of
+ * the density-fitting path of pysisyphus-addons.
+ *
+ * The f_* entry points keep the argument lists of the reference's bind(c)
+ * Fortran wrappers (file:line below, within the reference project), so a
+ * caller that binds those symbols (Cython `cdef extern`, ctypes, cffi) can
+ * link this library instead:
+ *   - all scalars are int32 passed by value;
+ *   - all arrays are column-major (Fortran order) host arrays;
+ *   - bas_centers (nshells x 3) and bas_spec (nshells x 5) hold 1-based
+ *     pointers into bas_data, packed as described in common/shells.f90:97-187;
+ *   - outputs are written in place; the library keeps no reference to any
+ *     argument after the call returns.
+ * Differences from the reference: every entry point returns an int status
+ * (PA_OK = 0; a caller that declared the function void ignores it) instead of
+ * terminating the process (`error stop`) or silently ignoring LAPACK errors,
+ * and pa_last_error() describes the last failure of the calling thread.
+ *
+ * The pa_* entry points are additions: options, statistics, and a
+ * device-resident variant of the path that takes device pointers and a CUDA
+ * stream (cudaStream_t passed as void*).
+ */
+#ifndef PA_B200_H
+#define PA_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define PA_OK 0
+#define PA_ERR_ARG 1        /* invalid argument (sizes, pointers, layout)        */
+#define PA_ERR_LMAX 2       /* angular momentum above the compiled maximum       */
+#define PA_ERR_NOT_SPD 3    /* metric (P|Q) not positive definite (dpotrf info>0) */
+#define PA_ERR_CUDA 4       /* CUDA runtime error                                 */
+#define PA_ERR_TIMEOUT 5    /* a bounded device-side wait gave up                 */
+#define PA_ERR_NO_DEVICE 6  /* no usable CUDA device                              */
+#define PA_ERR_SCRATCH 7    /* request exceeds a fixed scratch capacity           */
+
+/* Compiled angular-momentum limits (reference defaults, meson.options:1-4). */
+#define PA_LMAX_ORBITAL 4
+#define PA_LMAX_AUX 5
+
+/* Boys-function modes. */
+#define PA_BOYS_EXACT 0     /* ~1e-16 relative                                    */
+#define PA_BOYS_REFERENCE 1 /* behaviour of common/integrals/boys.f90 (default)    */
+
+/* Density layouts for the pa_* entry points. */
+#define PA_LAYOUT_FORTRAN 0 /* (ndens, nbf, nbf) column-major: d fastest          */
+#define PA_LAYOUT_C 1       /* (ndens, nbf, nbf) row-major: last index fastest    */
+
+/* ------------------------------------------------------------------------ */
+/* Reference-compatible entry points                                         */
+/* ------------------------------------------------------------------------ */
+
+/* Replaces f_init, common/integrals/init.f90:13-27: one-time set-up (device
+ * tables on the current device). Optional; every entry point calls it. */
+int f_init(void);
+
+/* Replaces f_int_schwarz_aux, intor/intor_wrapper.f90:12-24:
+ * integrals[c] = sqrt(||(c|c)||_F) for every shell c. */
+int f_int_schwarz_aux(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
+                      const double* bas_data, double* integrals);
+
+/* Replaces f_int_schwarz_bra, intor/intor_wrapper.f90:26-38:
+ * integrals[a(a+1)/2 + b] = sqrt(||(ab|ab)||_F), 0-based a >= b. */
+int f_int_schwarz_bra(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
+                      const double* bas_data, double* integrals);
+
+/* Replaces f_contract_coulomb_densities_2d, diabatization/intor_wrapper.f90:12-43:
+ * df_tensor(naux, ndens) = L^-1 sum_(a>=b) (ab|P) [D + (a!=b) D^T]. */
+int f_contract_coulomb_densities_2d(int nshells, int ndata, const int* bas_centers,
+                                    const int* bas_spec, const double* bas_data, int nshells_aux,
+                                    int ndata_aux, const int* bas_centers_aux,
+                                    const int* bas_spec_aux, const double* bas_data_aux,
+                                    int ndens, int nbfs, const double* densities, int naux,
+                                    double* df_tensor);
+
+/* Replaces f_contract_coulomb_densities_4d, diabatization/intor_wrapper.f90:45-76:
+ * coulomb_tensor(nstates, nstates, nstates, nstates), ndens = nstates(nstates+1)/2. */
+int f_contract_coulomb_densities_4d(int nshells, int ndata, const int* bas_centers,
+                                    const int* bas_spec, const double* bas_data, int nshells_aux,
+                                    int ndata_aux, const int* bas_centers_aux,
+                                    const int* bas_spec_aux, const double* bas_data_aux,
+                                    int ndens, int nbfs, const double* densities, int nstates,
+                                    double* coulomb_tensor);
+
+/* Replaces f_intor_eri2c, std/intor_wrapper.f90:12-35: eri2c(nbfs, nbfs) = T T^T
+ * with T = (mu mu|P) L^-T. */
+int f_intor_eri2c(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
+                  const double* bas_data, int nshells_aux, int ndata_aux,
+                  const int* bas_centers_aux, const int* bas_spec_aux,
+                  const double* bas_data_aux, int nbfs, double* eri2c_tensor);
+
+/* Replaces f_intor_df1c, std/intor_wrapper.f90:37-61: df1c(nbfs, nbfs_aux) =
+ * (mu mu|P) L^-T. */
+int f_intor_df1c(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
+                 const double* bas_data, int nshells_aux, int ndata_aux,
+                 const int* bas_centers_aux, const int* bas_spec_aux, const double* bas_data_aux,
+                 int nbfs, int nbfs_aux, double* df1c_tensor);
+
+/* Replaces f_intor_df2c_mo, std/intor_wrapper.f90:63-88: df2c_mo(nmos(nmos+1)/2,
+ * nbfs_aux) = MO-pair-packed (pq|P) L^-T for mo_tensor(nbfs, nmos). */
+int f_intor_df2c_mo(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
+                    const double* bas_data, int nshells_aux, int ndata_aux,
+                    const int* bas_centers_aux, const int* bas_spec_aux,
+                    const double* bas_data_aux, int nbfs, int nmos, const double* mo_tensor,
+                    int nbfs_aux, double* df2c_mo_tensor);
+
+/* ------------------------------------------------------------------------ */
+/* Additions                                                                 */
+/* ------------------------------------------------------------------------ */
+
+/* Message of the last failure on the calling thread ("" if none). */
+const char* pa_last_error(void);
+
+/* Options (process-wide). Boys mode: PA_BOYS_REFERENCE (default) or
+ * PA_BOYS_EXACT. Screening threshold: default (double)1e-10f, the reference's
+ * REAL(4) literal (diabatization/intor.f90:140). */
+int pa_set_boys_mode(int mode);
+int pa_get_boys_mode(void);
+int pa_set_screen_threshold(double thresh);
+
+/* Statistics of the last density-fitting call on this process. */
+typedef struct {
+  long long ntriplets;       /* shell triplets a >= b, c                       */
+  long long nskipped;        /* screened out (-1 when not counted)             */
+  long long nints;           /* spherical integrals of computed triplets (-1)  */
+  double ms_total;           /* device time of the whole path (CUDA events)    */
+  double ms_screen;          /* unit set-up, Schwarz vectors, class sorting    */
+  double ms_bra;             /* density folding of the bra units               */
+  double ms_metric;          /* metric (P|Q) and its Cholesky factor           */
+  double ms_3c;              /* three-center contraction and its reduction     */
+  double ms_solve;           /* L^-1 df and the Coulomb-tensor assembly        */
+  int kernel_launches;       /* kernels launched by the library in the call    */
+  int launches_3c;           /* of which three-center contraction kernels      */
+} pa_stats;
+int pa_get_stats(pa_stats* out);
+
+/* Device-resident path. A pa_basis holds an unpacked, normalized basis on the
+ * host and its copy in device memory of the current device. */
+typedef struct pa_basis_s* pa_basis;
+int pa_basis_create(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
+                    const double* bas_data, int lmax_allowed, pa_basis* out);
+int pa_basis_destroy(pa_basis basis);
+int pa_basis_info(pa_basis basis, int* nshells, int* nsph, int* lmax);
+
+/* df(naux, ndens), column-major, = L^-1 (ab|P) D; d_densities and d_df are
+ * device pointers; stream is a cudaStream_t (0 = default stream). Synchronous:
+ * returns after the result is complete (errors are reported here). */
+int pa_df_2d(pa_basis orbital, pa_basis aux, int ndens, int nbf, const double* d_densities,
+             int layout, double* d_df, void* stream);
+/* Coulomb tensor (nstates^4, column-major) from device densities. */
+int pa_df_4d(pa_basis orbital, pa_basis aux, int ndens, int nbf, const double* d_densities,
+             int layout, int nstates, double* d_coulomb, void* stream);
+/* Host-buffer variants of f_contract_coulomb_densities_{2d,4d} with an explicit
+ * density layout (PA_LAYOUT_C avoids a transposed host copy). */
+int pa_contract_coulomb_densities_2d(pa_basis orbital, pa_basis aux, int ndens, int nbf,
+                                     const double* densities, int layout, double* df_tensor);
+int pa_contract_coulomb_densities_4d(pa_basis orbital, pa_basis aux, int ndens, int nbf,
+                                     const double* densities, int layout, int nstates,
+                                     double* coulomb_tensor);
+
+/* Screening statistics for a basis pair: number of shell triplets that pass
+ * the Schwarz test and their spherical integral count (runs the Schwarz
+ * kernels; host-side counting). */
+int pa_count_triplets(pa_basis orbital, pa_basis aux, long long* ntriplets, long long* ncomputed,
+                      long long* nints);
+
+/* Building blocks exposed for tests: Boys values F_0..F_nmax(T) for n
+ * arguments on the device (results copied to host), and the metric (P|Q). */
+int pa_boys_eval(int mode, int nmax, int n, const double* T, double* out);
+int pa_metric(pa_basis aux, double* metric);
+/* Host-buffer Cholesky and forward substitution on the device: A (n x n,
+ * column-major) is replaced by its lower factor L, B (n x nrhs) by L^-1 B.
+ * PA_ERR_NOT_SPD when A is not positive definite. */
+int pa_cholesky_solve(int n, double* A, int nrhs, double* B);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PA_B200_H */

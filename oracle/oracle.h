@@ -1,0 +1,94 @@
+/*
+ * THE ORACLE -- test infrastructure, not product code.
+ *
+ * A C++ FP64 CPU restatement of the density-fitting path of pysisyphus-addons.
+ * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may
+ * load it, and only as the checker (or the timed CPU baseline), never as the
+ * thing measured or shipped. The product library (libpa_b200.so) never links
+ * or calls it.
+ *
+ * The drivers follow the reference's loop, screening, layout and threshold
+ * semantics (file:line citations in oracle.cpp). The integral values follow
+ * from the mathematics: contracted spherical Gaussian ERIs by the
+ * Obara-Saika vertical recurrence plus the Head-Gordon-Pople horizontal
+ * recurrence -- a different scheme from the McMurchie-Davidson kernels of the
+ * CUDA library, so agreement between the two is a genuine cross-check.
+ *
+ * All arrays are column-major (Fortran order) exactly as the reference's
+ * bind(c) wrappers expect; basis pointers are 1-based.
+ */
+#pragma once
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Boys-function mode: 0 = exact (series / asymptotic, ~1e-16 relative),
+ * 1 = reference-compatible (5-point Neville on a 0.01 grid for x < 27,
+ *     asymptotic formula for x >= 27; common/integrals/boys.f90:88-97). */
+void oracle_set_boys_mode(int mode);
+int oracle_get_boys_mode(void);
+void oracle_set_threads(int nthreads);
+int oracle_get_threads(void);
+/* Optional BLAS/LAPACK (Fortran calling convention) used by inv_chol / dtrmm /
+ * dgemm, exactly as the reference calls them; naive loops when unset. */
+void oracle_register_lapack(void* dpotrf, void* dtrtri, void* dtrmm, void* dgemm);
+
+void oracle_boys(int nmax, double x, double* out);
+double oracle_erfinv(double x);
+void oracle_contracted_center(int na, const double* axs, const double* das, const double* A,
+                              int nb, const double* bxs, const double* dbs, const double* B,
+                              double* R);
+
+/* Contracted spherical ERI block (ab|cd), order (ma, mb, mc, md) with md fastest.
+ * Shells are given raw (coefficients refer to normalized primitives and are
+ * renormalized like common/normalization.f90). A shell with L < 0 is a unit
+ * s function with exponent 0 (used for 2- and 3-center integrals). */
+int oracle_eri_block(int La, int na, const double* ea, const double* ca, const double* A,
+                     int Lb, int nb, const double* eb, const double* cb, const double* B,
+                     int Lc, int nc, const double* ec, const double* cc, const double* C,
+                     int Ld, int nd, const double* ed, const double* cd, const double* D,
+                     double* out);
+
+/* Mirrors of the reference's C-ABI (same argument lists). */
+void oracle_init(void);
+void oracle_int_schwarz_aux(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
+                            const double* bas_data, double* integrals);
+void oracle_int_schwarz_bra(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
+                            const double* bas_data, double* integrals);
+void oracle_int2c2e_metric(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
+                           const double* bas_data, int naux, double* metric);
+void oracle_contract_coulomb_densities_2d(
+    int nshells, int ndata, const int* bas_centers, const int* bas_spec, const double* bas_data,
+    int nshells_aux, int ndata_aux, const int* bas_centers_aux, const int* bas_spec_aux,
+    const double* bas_data_aux, int ndens, int nbfs, const double* densities, int naux,
+    double* df_tensor);
+void oracle_contract_coulomb_densities_4d(
+    int nshells, int ndata, const int* bas_centers, const int* bas_spec, const double* bas_data,
+    int nshells_aux, int ndata_aux, const int* bas_centers_aux, const int* bas_spec_aux,
+    const double* bas_data_aux, int ndens, int nbfs, const double* densities, int nstates,
+    double* coulomb_tensor);
+void oracle_intor_eri2c(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
+                        const double* bas_data, int nshells_aux, int ndata_aux,
+                        const int* bas_centers_aux, const int* bas_spec_aux,
+                        const double* bas_data_aux, int nbfs, double* eri2c);
+void oracle_intor_df1c(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
+                       const double* bas_data, int nshells_aux, int ndata_aux,
+                       const int* bas_centers_aux, const int* bas_spec_aux,
+                       const double* bas_data_aux, int nbfs, int nbfs_aux, double* df1c);
+void oracle_intor_df2c_mo(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
+                          const double* bas_data, int nshells_aux, int ndata_aux,
+                          const int* bas_centers_aux, const int* bas_spec_aux,
+                          const double* bas_data_aux, int nbfs, int nmos, const double* mo_tensor,
+                          int nbfs_aux, double* df2c_mo);
+
+/* Statistics of the last 3c2e driver call: computed and skipped shell triples,
+ * spherical integrals of computed triples, and phase times (seconds). */
+typedef struct {
+  long long ntriplets, nskipped, nints;
+  double t_screener, t_metric, t_chol, t_3c, t_trmm, t_total;
+} OracleStats;
+void oracle_last_stats(OracleStats* out);
+
+#ifdef __cplusplus
+}
+#endif

@@ -1,0 +1,264 @@
+"""ctypes front end of the oracle -- test infrastructure, not product code.
+
+Loads ``oracle/liboracle.so`` (a C++ FP64 CPU restatement of the reference's
+density-fitting path, see ``oracle.h``) and exposes the reference's Python
+entry points over it with the same argument meaning, so parity tests read like
+the reference's own tests. Only tests/, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` may import this module.
+
+BLAS/LAPACK: the reference calls dpotrf/dtrtri/dtrmm/dgemm. The oracle gets the
+same routines from scipy's bundled OpenBLAS (through ``scipy.linalg.cython_*``
+function pointers) when scipy is importable, and falls back to plain loops.
+"""
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle.so"
+
+_lib = None
+
+_i = ctypes.c_int
+_d = ctypes.c_double
+_pi = ctypes.POINTER(ctypes.c_int)
+_pd = ctypes.POINTER(ctypes.c_double)
+
+
+class OracleStats(ctypes.Structure):
+    _fields_ = [
+        ("ntriplets", ctypes.c_longlong),
+        ("nskipped", ctypes.c_longlong),
+        ("nints", ctypes.c_longlong),
+        ("t_screener", ctypes.c_double),
+        ("t_metric", ctypes.c_double),
+        ("t_chol", ctypes.c_double),
+        ("t_3c", ctypes.c_double),
+        ("t_trmm", ctypes.c_double),
+        ("t_total", ctypes.c_double),
+    ]
+
+
+def build():
+    """Compile liboracle.so with the committed Makefile."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+def _capsule_ptr(capsule):
+    get_name = ctypes.pythonapi.PyCapsule_GetName
+    get_name.restype = ctypes.c_char_p
+    get_name.argtypes = [ctypes.py_object]
+    get_ptr = ctypes.pythonapi.PyCapsule_GetPointer
+    get_ptr.restype = ctypes.c_void_p
+    get_ptr.argtypes = [ctypes.py_object, ctypes.c_char_p]
+    return get_ptr(capsule, get_name(capsule))
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        build()
+    L = ctypes.CDLL(str(LIB_PATH))
+    basis = [_i, _i, _pi, _pi, _pd]
+    L.oracle_boys.argtypes = [_i, _d, _pd]
+    L.oracle_erfinv.argtypes = [_d]
+    L.oracle_erfinv.restype = _d
+    L.oracle_contracted_center.argtypes = [_i, _pd, _pd, _pd, _i, _pd, _pd, _pd, _pd]
+    L.oracle_eri_block.argtypes = [_i, _i, _pd, _pd, _pd] * 4 + [_pd]
+    L.oracle_eri_block.restype = _i
+    L.oracle_int_schwarz_aux.argtypes = basis + [_pd]
+    L.oracle_int_schwarz_bra.argtypes = basis + [_pd]
+    L.oracle_int2c2e_metric.argtypes = basis + [_i, _pd]
+    L.oracle_contract_coulomb_densities_2d.argtypes = basis + basis + [_i, _i, _pd, _i, _pd]
+    L.oracle_contract_coulomb_densities_4d.argtypes = basis + basis + [_i, _i, _pd, _i, _pd]
+    L.oracle_intor_eri2c.argtypes = basis + basis + [_i, _pd]
+    L.oracle_intor_df1c.argtypes = basis + basis + [_i, _i, _pd]
+    L.oracle_intor_df2c_mo.argtypes = basis + basis + [_i, _i, _pd, _i, _pd]
+    L.oracle_set_boys_mode.argtypes = [_i]
+    L.oracle_get_boys_mode.restype = _i
+    L.oracle_set_threads.argtypes = [_i]
+    L.oracle_get_threads.restype = _i
+    L.oracle_register_lapack.argtypes = [ctypes.c_void_p] * 4
+    L.oracle_last_stats.argtypes = [ctypes.POINTER(OracleStats)]
+    if os.environ.get("PA_ORACLE_NO_LAPACK", "0") != "1":
+        try:
+            from scipy.linalg import cython_blas, cython_lapack
+
+            L.oracle_register_lapack(
+                _capsule_ptr(cython_lapack.__pyx_capi__["dpotrf"]),
+                _capsule_ptr(cython_lapack.__pyx_capi__["dtrtri"]),
+                _capsule_ptr(cython_blas.__pyx_capi__["dtrmm"]),
+                _capsule_ptr(cython_blas.__pyx_capi__["dgemm"]),
+            )
+        except ImportError:  # plain loops inside the oracle
+            pass
+    L.oracle_init()
+    _lib = L
+    return L
+
+
+def _p(arr, ctype):
+    return arr.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def _basis_args(shells):
+    bc, bs, bd = shells.as_arrays(fortran=True)
+    bc = np.asfortranarray(bc, dtype=np.int32)
+    bs = np.asfortranarray(bs, dtype=np.int32)
+    bd = np.ascontiguousarray(bd, dtype=np.float64)
+    keep = (bc, bs, bd)
+    return keep, [len(bc), len(bd), _p(bc, ctypes.c_int), _p(bs, ctypes.c_int), _p(bd, ctypes.c_double)]
+
+
+def set_boys_mode(mode):
+    lib().oracle_set_boys_mode({"exact": 0, "reference": 1}.get(mode, mode))
+
+
+def get_boys_mode():
+    return lib().oracle_get_boys_mode()
+
+
+def set_threads(n):
+    lib().oracle_set_threads(int(n))
+
+
+def get_threads():
+    return lib().oracle_get_threads()
+
+
+def last_stats():
+    st = OracleStats()
+    lib().oracle_last_stats(ctypes.byref(st))
+    return {name: getattr(st, name) for name, _ in OracleStats._fields_}
+
+
+def boys(nmax, x):
+    out = np.zeros(nmax + 1)
+    lib().oracle_boys(nmax, float(x), _p(out, ctypes.c_double))
+    return out
+
+
+def erfinv(x):
+    return lib().oracle_erfinv(float(x))
+
+
+def contracted_center(axs, das, A, bxs, dbs, B):
+    arrs = [np.ascontiguousarray(v, dtype=float) for v in (axs, das, A, bxs, dbs, B)]
+    R = np.zeros(3)
+    lib().oracle_contracted_center(
+        len(arrs[0]), *[_p(a, ctypes.c_double) for a in arrs[:3]],
+        len(arrs[3]), *[_p(a, ctypes.c_double) for a in arrs[3:]],
+        _p(R, ctypes.c_double),
+    )
+    return R
+
+
+def eri_block(a, b=None, c=None, d=None):
+    """Contracted spherical block (ab|cd) of Shell objects; None = unit s function."""
+    shells = [a, b, c, d]
+    args, keep = [], []
+    dims = []
+    for s, partner in zip(shells, [a, a, c if c is not None else a, c if c is not None else a]):
+        if s is None:
+            e = np.zeros(1)
+            co = np.ones(1)
+            X = np.ascontiguousarray(partner.center, dtype=float)
+            args += [-1, 1, _p(e, ctypes.c_double), _p(co, ctypes.c_double), _p(X, ctypes.c_double)]
+            keep += [e, co, X]
+            dims.append(1)
+        else:
+            e = np.ascontiguousarray(s.exps, dtype=float)
+            co = np.ascontiguousarray(s.coeffs, dtype=float)
+            X = np.ascontiguousarray(s.center, dtype=float)
+            args += [s.L, len(e), _p(e, ctypes.c_double), _p(co, ctypes.c_double), _p(X, ctypes.c_double)]
+            keep += [e, co, X]
+            dims.append(2 * s.L + 1)
+    out = np.zeros(int(np.prod(dims)))
+    rc = lib().oracle_eri_block(*args, _p(out, ctypes.c_double))
+    if rc != 0:
+        raise ValueError("angular momentum above the oracle's maximum")
+    return out.reshape(dims)
+
+
+def int_schwarz_aux(shells):
+    keep, b = _basis_args(shells)
+    out = np.zeros(len(shells))
+    lib().oracle_int_schwarz_aux(*b, _p(out, ctypes.c_double))
+    return out
+
+
+def int_schwarz_bra(shells):
+    keep, b = _basis_args(shells)
+    n = len(shells)
+    out = np.zeros(n * (n + 1) // 2)
+    lib().oracle_int_schwarz_bra(*b, _p(out, ctypes.c_double))
+    return out
+
+
+def int2c2e(shells):
+    keep, b = _basis_args(shells)
+    n = shells.sph_size
+    out = np.zeros((n, n), order="F")
+    lib().oracle_int2c2e_metric(*b, n, _p(out, ctypes.c_double))
+    return out
+
+
+def contract_coulomb_densities_2d(shells, shells_aux, densities):
+    k1, b1 = _basis_args(shells)
+    k2, b2 = _basis_args(shells_aux)
+    D = np.asfortranarray(densities, dtype=np.float64)
+    ndens, nbf, _ = D.shape
+    naux = shells_aux.sph_size
+    out = np.zeros((naux, ndens), order="F")
+    lib().oracle_contract_coulomb_densities_2d(*b1, *b2, ndens, nbf, _p(D, ctypes.c_double), naux,
+                                               _p(out, ctypes.c_double))
+    return out
+
+
+def contract_coulomb_densities_4d(shells, shells_aux, densities):
+    k1, b1 = _basis_args(shells)
+    k2, b2 = _basis_args(shells_aux)
+    D = np.asfortranarray(densities, dtype=np.float64)
+    ndens, nbf, _ = D.shape
+    nstates = int(round((np.sqrt(8 * ndens + 1) - 1) / 2))
+    assert nstates * (nstates + 1) // 2 == ndens
+    out = np.zeros((nstates,) * 4, order="F")
+    lib().oracle_contract_coulomb_densities_4d(*b1, *b2, ndens, nbf, _p(D, ctypes.c_double),
+                                               nstates, _p(out, ctypes.c_double))
+    return out
+
+
+def int_eri2c(shells, shells_aux):
+    k1, b1 = _basis_args(shells)
+    k2, b2 = _basis_args(shells_aux)
+    nbf = shells.sph_size
+    out = np.zeros((nbf, nbf), order="F")
+    lib().oracle_intor_eri2c(*b1, *b2, nbf, _p(out, ctypes.c_double))
+    return out
+
+
+def int_df1c(shells, shells_aux):
+    k1, b1 = _basis_args(shells)
+    k2, b2 = _basis_args(shells_aux)
+    nbf, naux = shells.sph_size, shells_aux.sph_size
+    out = np.zeros((nbf, naux), order="F")
+    lib().oracle_intor_df1c(*b1, *b2, nbf, naux, _p(out, ctypes.c_double))
+    return out
+
+
+def int_df2c_mo(shells, shells_aux, mo_tensor):
+    k1, b1 = _basis_args(shells)
+    k2, b2 = _basis_args(shells_aux)
+    C = np.asfortranarray(mo_tensor, dtype=np.float64)
+    nbf, nmos = C.shape
+    naux = shells_aux.sph_size
+    out = np.zeros((nmos * (nmos + 1) // 2, naux), order="F")
+    lib().oracle_intor_df2c_mo(*b1, *b2, nbf, nmos, _p(C, ctypes.c_double), naux,
+                               _p(out, ctypes.c_double))
+    return out

@@ -1,0 +1,49 @@
+// Launch interface of the three-center contraction (k_df3c.cu).
+#pragma once
+
+#include "pa_internal.h"
+
+namespace pa {
+
+// Arguments of one class (LAB, LC) launch. Pointers already point at the
+// class's first slot where noted.
+struct Df3cArgs {
+  DevBasis X;                        // auxiliary basis
+  DeviceTables dt;
+  int boys_mode = 1;
+  double thresh = 0.0;
+  // bra units of class LAB, sorted by Schwarz value (descending)
+  int unit_slot0 = 0, n_units = 0;   // global slot offset, count
+  const double* unit_Q = nullptr;    // [slot]
+  const double4* slot_pP = nullptr;  // [slot] (p, P)
+  const double* G = nullptr;         // class base: [s][tuv][d]
+  int units_per_chunk = 1;
+  // auxiliary shells of class LC, sorted by Schwarz value (descending)
+  int aux_slot0 = 0, n_aux = 0;
+  const int* sorted_aux = nullptr;   // [slot] -> shell
+  const double* aux_Q = nullptr;     // [slot]
+  int nd = 0;
+  double* partial = nullptr;         // [chunk][n_aux * NC][nd]
+};
+
+struct Df3cReduceArgs {
+  DevBasis X;
+  int aux_slot0 = 0, n_aux = 0, nc = 1, nd = 0, naux = 0;
+  const int* sorted_aux = nullptr;
+  int nclasses = 0;
+  const double* part[2 * PA_LMAX + 1] = {};
+  int ny[2 * PA_LMAX + 1] = {};
+  double* df = nullptr;              // [naux][nd] column-major (naux rows)
+};
+
+struct Df3cClassInfo {
+  int tc = 0, ub = 0, ndc = 0;
+  size_t smem = 0;
+};
+
+void df3c_class_info(int lab, int lc, Df3cClassInfo* ci);
+int launch_df3c_class(int lab, int lc, const Df3cArgs& a, int ny, cudaStream_t s);
+int launch_df3c_reduce(const Df3cReduceArgs& r, cudaStream_t s);
+cudaError_t upload_sph_dense(const double* vals, int n, const int* offs, cudaStream_t s);
+
+}  // namespace pa

@@ -1,0 +1,405 @@
+// Integral kernels of the density-fitting path (McMurchie-Davidson, FP64):
+//  * k_unit_setup   per primitive pair of an orbital shell pair ("bra unit"):
+//                   Gaussian-product data and the spherical Hermite expansion
+//                   E_sph[(ma,mb)][tuv] (contraction coefficients folded in);
+//  * k_schwarz_bra  sqrt(||(ab|ab)||_F) per shell pair
+//                   (common/integrals/intor.f90:131-160);
+//  * k_schwarz_aux  sqrt(||(c|c)||_F) per auxiliary shell (intor.f90:97-129);
+//  * k_metric       the symmetric (P|Q) matrix (intor.f90:40-95);
+//  * k_bra_prep     density folding G_d[tuv] = sum_(ma,mb) Dsym_d[ma,mb] E_sph[(ma,mb)][tuv]
+//                   with Dsym = D + (a != b) D^T as in diabatization/intor.f90:155-177.
+#include "boys.cuh"
+#include "k_integrals.cuh"
+#include "md.cuh"
+
+namespace pa {
+
+namespace {
+
+struct WarpSync {
+  __device__ void operator()() const { __syncwarp(); }
+};
+struct BlockSync {
+  __device__ void operator()() const { __syncthreads(); }
+};
+
+__device__ __forceinline__ int sph_row(int l, int m_plus_l) { return l * l + m_plus_l; }
+
+// Index of the sum of two Hermite/Cartesian multi-indices given by table index.
+__device__ __forceinline__ int cidx_sum(const IndexTables* __restrict__ it, int i, int j) {
+  const uchar4 a = *reinterpret_cast<const uchar4*>(it->xyz[i]);
+  const uchar4 b = *reinterpret_cast<const uchar4*>(it->xyz[j]);
+  return cidx(a.x + b.x, a.y + b.y, a.z + b.z);
+}
+
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_unit_setup(DevBasis B, const int2* __restrict__ pair_ab,
+                                                    UnitArrays U, int nunits, DeviceTables dt) {
+  const int u = blockIdx.x;
+  if (u >= nunits) return;
+  __shared__ double E[3][(PA_LMAX + 1) * (PA_LMAX + 1) * (2 * PA_LMAX + 1)];
+  __shared__ double sh[8];
+  const int pair = U.unit_pair[u];
+  const int2 ab = pair_ab[pair];
+  const int4 sa = B.shell[ab.x], sb = B.shell[ab.y];
+  const int la = sa.x, lb = sb.x;
+  const int2 pr = U.unit_prims[u];
+  if (threadIdx.x == 0) {
+    const double4 A = B.center[ab.x], Bc = B.center[ab.y];
+    const double2 pa_ = B.prim[pr.x], pb_ = B.prim[pr.y];
+    const double p = pa_.x + pb_.x;
+    const double Px = (pa_.x * A.x + pb_.x * Bc.x) / p;
+    const double Py = (pa_.x * A.y + pb_.x * Bc.y) / p;
+    const double Pz = (pa_.x * A.z + pb_.x * Bc.z) / p;
+    const double ABx = A.x - Bc.x, ABy = A.y - Bc.y, ABz = A.z - Bc.z;
+    const double K = exp(-pa_.x * pb_.x / p * (ABx * ABx + ABy * ABy + ABz * ABz));
+    sh[0] = p;
+    sh[1] = Px;
+    sh[2] = Py;
+    sh[3] = Pz;
+    sh[4] = pa_.y * pb_.y * K;
+    sh[5] = Px - A.x;
+    sh[6] = Py - A.y;
+    sh[7] = Pz - A.z;
+    U.unit_pP[u] = make_double4(p, Px, Py, Pz);
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    const int d = threadIdx.x;
+    const double4 Bc = B.center[ab.y];
+    const double Pd = sh[1 + d];
+    const double PB = Pd - (d == 0 ? Bc.x : (d == 1 ? Bc.y : Bc.z));
+    hermite_E_1d(la, lb, sh[5 + d], PB, 0.5 / sh[0], E[d]);
+  }
+  __syncthreads();
+  const IndexTables* it = dt.idx;
+  const int nsb = 2 * lb + 1;
+  const int nab = (2 * la + 1) * nsb;
+  const int NH = ncum(la + lb);
+  const int nt = la + lb + 1, nj = lb + 1;
+  const int offa = ncum(la - 1 < 0 ? -1 : la - 1), offb = ncum(lb - 1 < 0 ? -1 : lb - 1);
+  const double pref = sh[4];
+  double* out = U.esph + U.unit_esph[u];
+  for (int idx = threadIdx.x; idx < nab * NH; idx += blockDim.x) {
+    const int r = idx / NH, t = idx - r * NH;
+    const int ma = r / nsb, mb = r - ma * nsb;
+    const uchar4 tt = *reinterpret_cast<const uchar4*>(it->xyz[t]);
+    const int rowa = sph_row(la, ma), rowb = sph_row(lb, mb);
+    double v = 0.0;
+    for (int ka = dt.sph_start[rowa]; ka < dt.sph_start[rowa + 1]; ++ka) {
+      const uchar4 ea = *reinterpret_cast<const uchar4*>(it->xyz[offa + dt.sph_col[ka]]);
+      const double ca = dt.sph_val[ka];
+      for (int kb = dt.sph_start[rowb]; kb < dt.sph_start[rowb + 1]; ++kb) {
+        const uchar4 eb = *reinterpret_cast<const uchar4*>(it->xyz[offb + dt.sph_col[kb]]);
+        if (tt.x > ea.x + eb.x || tt.y > ea.y + eb.y || tt.z > ea.z + eb.z) continue;
+        v += ca * dt.sph_val[kb] * E[0][(ea.x * nj + eb.x) * nt + tt.x] *
+             E[1][(ea.y * nj + eb.y) * nt + tt.y] * E[2][(ea.z * nj + eb.z) * nt + tt.z];
+      }
+    }
+    out[idx] = pref * v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+constexpr int kSchwarzRowChunk = 8;
+
+__global__ void __launch_bounds__(256) k_schwarz_bra(DevBasis B, const int2* __restrict__ pair_ab,
+                                                     const int* __restrict__ pair_unit0,
+                                                     UnitArrays U, int npairs, DeviceTables dt,
+                                                     int boys_mode, double* __restrict__ Qab) {
+  extern __shared__ double smem[];
+  const int pair = blockIdx.x;
+  if (pair >= npairs) return;
+  const int2 ab = pair_ab[pair];
+  const int4 sa = B.shell[ab.x], sb = B.shell[ab.y];
+  const int la = sa.x, lb = sb.x;
+  const int nsb = 2 * lb + 1, nab = (2 * la + 1) * nsb;
+  const int NH = ncum(la + lb);
+  const int L4 = 2 * (la + lb);
+  const int NR = ncum(L4);
+  double* Rn = smem;                  // L4 + 1 (padded to 32)
+  double* R0 = Rn + 32;               // NR
+  double* R1 = R0 + NR;               // NR
+  double* Y = R1 + NR;                // kSchwarzRowChunk * NH
+  double* out = Y + kSchwarzRowChunk * NH;  // nab * nab
+  __shared__ double red[8];
+  const IndexTables* it = dt.idx;
+  for (int i = threadIdx.x; i < nab * nab; i += blockDim.x) out[i] = 0.0;
+  const int u0 = pair_unit0[pair];
+  const int nu = sa.y * sb.y;
+  for (int iu = 0; iu < nu; ++iu)
+    for (int ku = 0; ku < nu; ++ku) {
+      const double4 P = U.unit_pP[u0 + iu], Q = U.unit_pP[u0 + ku];
+      const double p = P.x, q = Q.x, pq = p + q, alpha = p * q / pq;
+      const double X = P.y - Q.y, Yd = P.z - Q.z, Z = P.w - Q.w;
+      const double T = alpha * (X * X + Yd * Yd + Z * Z);
+      const double pref = kTwoPi52 / (p * q * sqrt(pq));
+      __syncthreads();  // previous users of Rn / R buffers / Y are done
+      if (threadIdx.x <= L4) {
+        const int n = threadIdx.x;
+        Rn[n] = pref * pow(-2.0 * alpha, n) * boys_n(dt, boys_mode, n, T);
+      }
+      __syncthreads();
+      hermite_R(it, L4, Rn, X, Yd, Z, R0, R1, threadIdx.x, blockDim.x, BlockSync());
+      const double* Ei = U.esph + U.unit_esph[u0 + iu];
+      const double* Ek = U.esph + U.unit_esph[u0 + ku];
+      for (int r0 = 0; r0 < nab; r0 += kSchwarzRowChunk) {
+        const int rows = min(kSchwarzRowChunk, nab - r0);
+        for (int idx = threadIdx.x; idx < rows * NH; idx += blockDim.x) {
+          const int rr = idx / NH, tp = idx - rr * NH;
+          const double* e = Ei + (r0 + rr) * NH;
+          double y = 0.0;
+          for (int t = 0; t < NH; ++t) y = fma(e[t], R0[cidx_sum(it, t, tp)], y);
+          const int deg = it->xyz[tp][3];
+          Y[rr * NH + tp] = (deg & 1) ? -y : y;
+        }
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < rows * nab; idx += blockDim.x) {
+          const int rr = idx / nab, s = idx - rr * nab;
+          const double* e = Ek + s * NH;
+          const double* yr = Y + rr * NH;
+          double v = 0.0;
+          for (int tp = 0; tp < NH; ++tp) v = fma(yr[tp], e[tp], v);
+          out[(r0 + rr) * nab + s] += v;
+        }
+        __syncthreads();
+      }
+    }
+  double s2 = 0.0;
+  for (int i = threadIdx.x; i < nab * nab; i += blockDim.x) s2 += out[i] * out[i];
+  for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s2;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
+    Qab[pair] = sqrt(sqrt(tot));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Two-center block (P|Q)[mP][mQ] of two auxiliary shells, computed by one warp.
+// Scratch (per warp): Rn[16], R0/R1[ncum(lP+lQ)], Y[nsP * ncart(lQ)], out[nsP * nsQ].
+struct TwoCScratch {
+  double* Rn;
+  double* R0;
+  double* R1;
+  double* Y;
+  double* out;
+};
+
+__device__ void twoc_block_warp(const DevBasis& X, int P, int Q, const DeviceTables& dt,
+                                int boys_mode, TwoCScratch s, int lane) {
+  const IndexTables* it = dt.idx;
+  const int4 sP = X.shell[P], sQ = X.shell[Q];
+  const int lP = sP.x, lQ = sQ.x;
+  const int nsP = 2 * lP + 1, nsQ = 2 * lQ + 1, ncQ = ncart(lQ);
+  const int L = lP + lQ;
+  const int offP = ncum(lP - 1 < 0 ? -1 : lP - 1), offQ = ncum(lQ - 1 < 0 ? -1 : lQ - 1);
+  const double4 CP = X.center[P], CQ = X.center[Q];
+  const double Xd = CP.x - CQ.x, Yd = CP.y - CQ.y, Zd = CP.z - CQ.z;
+  const double RPQ2 = Xd * Xd + Yd * Yd + Zd * Zd;
+  for (int i = lane; i < nsP * nsQ; i += 32) s.out[i] = 0.0;
+  for (int kp = 0; kp < sP.y; ++kp)
+    for (int kq = 0; kq < sQ.y; ++kq) {
+      const double2 gp = X.prim[sP.z + kp], gq = X.prim[sQ.z + kq];
+      const double g = gp.x, h = gq.x, gh = g + h, alpha = g * h / gh;
+      double pref = kTwoPi52 / (g * h * sqrt(gh)) * gp.y * gq.y * pow(2.0 * g, -lP) *
+                    pow(2.0 * h, -lQ);
+      if (lQ & 1) pref = -pref;
+      const double T = alpha * RPQ2;
+      __syncwarp();
+      if (lane <= L) s.Rn[lane] = pref * pow(-2.0 * alpha, lane) * boys_n(dt, boys_mode, lane, T);
+      __syncwarp();
+      hermite_R(it, L, s.Rn, Xd, Yd, Zd, s.R0, s.R1, lane, 32, WarpSync());
+      for (int idx = lane; idx < nsP * ncQ; idx += 32) {
+        const int m = idx / ncQ, sg = idx - m * ncQ;
+        const int row = sph_row(lP, m);
+        double y = 0.0;
+        for (int k = dt.sph_start[row]; k < dt.sph_start[row + 1]; ++k)
+          y = fma(dt.sph_val[k], s.R0[cidx_sum(it, offP + dt.sph_col[k], offQ + sg)], y);
+        s.Y[idx] = y;
+      }
+      __syncwarp();
+      for (int idx = lane; idx < nsP * nsQ; idx += 32) {
+        const int m = idx / nsQ, mq = idx - m * nsQ;
+        const int row = sph_row(lQ, mq);
+        double v = 0.0;
+        for (int k = dt.sph_start[row]; k < dt.sph_start[row + 1]; ++k)
+          v = fma(dt.sph_val[k], s.Y[m * ncQ + dt.sph_col[k]], v);
+        s.out[idx] += v;
+      }
+      __syncwarp();
+    }
+}
+
+constexpr int kTwoCWarps = 4;
+constexpr int kTwoCScratch = 32 + 2 * ncum(2 * PA_LAUXMAX) + (2 * PA_LAUXMAX + 1) * ncart(PA_LAUXMAX) +
+                             (2 * PA_LAUXMAX + 1) * (2 * PA_LAUXMAX + 1);
+
+__device__ __forceinline__ TwoCScratch twoc_scratch(double* base) {
+  TwoCScratch s;
+  s.Rn = base;
+  s.R0 = s.Rn + 32;
+  s.R1 = s.R0 + ncum(2 * PA_LAUXMAX);
+  s.Y = s.R1 + ncum(2 * PA_LAUXMAX);
+  s.out = s.Y + (2 * PA_LAUXMAX + 1) * ncart(PA_LAUXMAX);
+  return s;
+}
+
+__global__ void __launch_bounds__(32 * kTwoCWarps) k_schwarz_aux(DevBasis X, DeviceTables dt,
+                                                                 int boys_mode,
+                                                                 double* __restrict__ Qc) {
+  __shared__ double scratch[kTwoCWarps][kTwoCScratch];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = blockIdx.x * kTwoCWarps + warp;
+  if (c >= X.nshells) return;
+  TwoCScratch s = twoc_scratch(scratch[warp]);
+  twoc_block_warp(X, c, c, dt, boys_mode, s, lane);
+  const int ns = 2 * X.shell[c].x + 1;
+  double s2 = 0.0;
+  for (int i = lane; i < ns * ns; i += 32) s2 += s.out[i] * s.out[i];
+  for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+  if (lane == 0) Qc[c] = sqrt(sqrt(s2));
+}
+
+__global__ void __launch_bounds__(32 * kTwoCWarps) k_metric(DevBasis X, DeviceTables dt,
+                                                            int boys_mode, long long npairs,
+                                                            double* __restrict__ M) {
+  __shared__ double scratch[kTwoCWarps][kTwoCScratch];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long pr = static_cast<long long>(blockIdx.x) * kTwoCWarps + warp;
+  if (pr >= npairs) return;
+  // pr = a (a + 1) / 2 + b, b <= a
+  long long a = static_cast<long long>((sqrt(8.0 * static_cast<double>(pr) + 1.0) - 1.0) * 0.5);
+  while (a * (a + 1) / 2 > pr) --a;
+  while ((a + 1) * (a + 2) / 2 <= pr) ++a;
+  const long long b = pr - a * (a + 1) / 2;
+  TwoCScratch s = twoc_scratch(scratch[warp]);
+  twoc_block_warp(X, static_cast<int>(a), static_cast<int>(b), dt, boys_mode, s, lane);
+  const int4 sA = X.shell[a], sB = X.shell[b];
+  const int nsA = 2 * sA.x + 1, nsB = 2 * sB.x + 1;
+  const long long N = X.nsph;
+  for (int i = lane; i < nsA * nsB; i += 32) {
+    const int ia = i / nsB, ib = i - ia * nsB;
+    const long long r = sA.w + ia, c = sB.w + ib;
+    const double v = s.out[i];
+    M[r + N * c] = v;
+    M[c + N * r] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+constexpr int kBraTChunk = 16;
+
+__global__ void __launch_bounds__(256) k_bra_prep(DevBasis B, const int2* __restrict__ pair_ab,
+                                                  UnitArrays U, BraPrepArgs a) {
+  extern __shared__ double smem[];
+  const int slot = a.slot0 + blockIdx.x;
+  if (slot >= a.slot_end) return;
+  const double q = a.slot_Q[slot];
+  if (q * (*a.qmax_aux) < a.thresh) return;  // never reached by any surviving triple
+  const int u = a.sorted_unit[slot];
+  const int2 ab = pair_ab[U.unit_pair[u]];
+  const int4 sa = B.shell[ab.x], sb = B.shell[ab.y];
+  const int la = sa.x, lb = sb.x;
+  const int nsb = 2 * lb + 1, nab = (2 * la + 1) * nsb;
+  const int NH = ncum(la + lb);
+  const int nd = a.nd;
+  double* Ds = smem;            // [nab][nd]
+  double* Es = Ds + nab * nd;   // [nab][kBraTChunk]
+  for (int idx = threadIdx.x; idx < nab * nd; idx += blockDim.x) {
+    const int r = idx / nd, d = idx - r * nd;
+    const int ma = r / nsb, mb = r - ma * nsb;
+    const long long i = sa.w + ma, j = sb.w + mb;
+    double v = a.dens[d * a.sd + i * a.si + j * a.sj];
+    if (ab.x != ab.y) v += a.dens[d * a.sd + j * a.si + i * a.sj];
+    Ds[idx] = v;
+  }
+  if (threadIdx.x == 0) a.slot_pP[slot] = U.unit_pP[u];
+  const double* E = U.esph + U.unit_esph[u];
+  double* G = a.G + a.g_base + static_cast<long long>(slot - a.slot0) * NH * nd;
+  for (int t0 = 0; t0 < NH; t0 += kBraTChunk) {
+    const int tn = min(kBraTChunk, NH - t0);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < nab * kBraTChunk; idx += blockDim.x) {
+      const int r = idx / kBraTChunk, tt = idx - r * kBraTChunk;
+      Es[idx] = tt < tn ? E[r * NH + t0 + tt] : 0.0;
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < tn * nd; idx += blockDim.x) {
+      const int tt = idx / nd, d = idx - tt * nd;
+      double v = 0.0;
+      for (int r = 0; r < nab; ++r) v = fma(Ds[r * nd + d], Es[r * kBraTChunk + tt], v);
+      G[(t0 + tt) * nd + d] = v;
+    }
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Launchers.
+
+int launch_unit_setup(const DevBasis& B, const int2* pair_ab, UnitArrays U, int nunits,
+                      const DeviceTables& dt, cudaStream_t s) {
+  if (nunits == 0) return 0;
+  k_unit_setup<<<nunits, 128, 0, s>>>(B, pair_ab, U, nunits, dt);
+  return 1;
+}
+
+size_t schwarz_bra_smem(int lab_max) {
+  const int NH = ncum(lab_max), NR = ncum(2 * lab_max);
+  const int nab = (2 * PA_LMAX + 1) * (2 * PA_LMAX + 1);
+  int nab_max = 1;
+  for (int la = 0; la <= PA_LMAX; ++la)
+    for (int lb = 0; lb <= la; ++lb)
+      if (la + lb <= lab_max) nab_max = max(nab_max, (2 * la + 1) * (2 * lb + 1));
+  (void)nab;
+  return sizeof(double) * (32 + 2 * NR + kSchwarzRowChunk * NH + nab_max * nab_max);
+}
+
+int launch_schwarz_bra(const DevBasis& B, const int2* pair_ab, const int* pair_unit0,
+                       UnitArrays U, int npairs, int lab_max, const DeviceTables& dt,
+                       int boys_mode, double* Qab, cudaStream_t s) {
+  if (npairs == 0) return 0;
+  const size_t smem = schwarz_bra_smem(lab_max);
+  cudaFuncSetAttribute(k_schwarz_bra, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(smem));
+  k_schwarz_bra<<<npairs, 256, smem, s>>>(B, pair_ab, pair_unit0, U, npairs, dt, boys_mode, Qab);
+  return 1;
+}
+
+int launch_schwarz_aux(const DevBasis& X, const DeviceTables& dt, int boys_mode, double* Qc,
+                       cudaStream_t s) {
+  if (X.nshells == 0) return 0;
+  const int blocks = (X.nshells + kTwoCWarps - 1) / kTwoCWarps;
+  k_schwarz_aux<<<blocks, 32 * kTwoCWarps, 0, s>>>(X, dt, boys_mode, Qc);
+  return 1;
+}
+
+int launch_metric(const DevBasis& X, const DeviceTables& dt, int boys_mode, double* M,
+                  cudaStream_t s) {
+  const long long npairs = static_cast<long long>(X.nshells) * (X.nshells + 1) / 2;
+  if (npairs == 0) return 0;
+  const long long blocks = (npairs + kTwoCWarps - 1) / kTwoCWarps;
+  k_metric<<<static_cast<unsigned>(blocks), 32 * kTwoCWarps, 0, s>>>(X, dt, boys_mode, npairs, M);
+  return 1;
+}
+
+int launch_bra_prep(const DevBasis& B, const int2* pair_ab, UnitArrays U, const BraPrepArgs& a,
+                    int lab, cudaStream_t s) {
+  const int n = a.slot_end - a.slot0;
+  if (n <= 0) return 0;
+  int nab_max = 1;
+  for (int la = 0; la <= PA_LMAX; ++la)
+    for (int lb = 0; lb <= la; ++lb)
+      if (la + lb == lab) nab_max = max(nab_max, (2 * la + 1) * (2 * lb + 1));
+  const size_t smem = sizeof(double) * nab_max * (a.nd + kBraTChunk);
+  cudaFuncSetAttribute(k_bra_prep, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(smem));
+  k_bra_prep<<<n, 256, smem, s>>>(B, pair_ab, U, a);
+  return 1;
+}
+
+}  // namespace pa

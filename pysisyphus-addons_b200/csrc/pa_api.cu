@@ -1,0 +1,1049 @@
+// Host orchestration and C-ABI of libpa_b200.so.
+//
+// The density-fitting path (diabatization/intor.f90:28-270) runs entirely on
+// the current CUDA device:
+//   Schwarz vectors (k_schwarz_bra / k_schwarz_aux)  -> screening
+//   class-wise sort of bra units and auxiliary shells by Schwarz value (CUB)
+//   density folding of the bra units (k_bra_prep)
+//   metric (P|Q) (k_metric) -> Cholesky (k_linalg)
+//   screened 3c2e contraction (k_df3c<LAB,LC>) -> ordered reduction
+//   B = L^-1 df (blocked forward substitution) [-> Coulomb tensor]
+#include <cub/device/device_reduce.cuh>
+#include <cub/device/device_segmented_radix_sort.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "boys.cuh"
+#include "k_df3c.cuh"
+#include "k_integrals.cuh"
+#include "k_linalg.cuh"
+#include "pa_b200.h"
+#include "pa_internal.h"
+
+namespace pa {
+
+namespace {
+
+thread_local std::string tl_err;
+
+int fail(int code, const std::string& msg) {
+  tl_err = msg;
+  return code;
+}
+
+std::mutex g_opt_mu;
+Options g_opts;
+pa_stats g_stats{};
+
+Options options() {
+  std::lock_guard<std::mutex> lk(g_opt_mu);
+  return g_opts;
+}
+
+#define PA_CUDA(call)                                                                  \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return fail(PA_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));   \
+  } while (0)
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Basis unpacking: common/shells.f90:97-187 and common/normalization.f90:10-38.
+int unpack_basis(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
+                 const double* bas_data, int lmax_allowed, HostBasis* out, std::string* err) {
+  if (nshells < 0 || ndata < 0) {
+    *err = "negative basis sizes";
+    return PA_ERR_ARG;
+  }
+  if (nshells > 0 && (!bas_centers || !bas_spec || !bas_data)) {
+    *err = "null basis array";
+    return PA_ERR_ARG;
+  }
+  HostBasis b;
+  b.shells.resize(nshells);
+  int sph = 0;
+  for (int i = 0; i < nshells; ++i) {
+    HostShell& s = b.shells[i];
+    const long long cptr = bas_centers[i + 2LL * nshells];
+    const int L = bas_spec[i + 1LL * nshells];
+    const int nprim = bas_spec[i + 2LL * nshells];
+    const long long ptr = bas_spec[i + 4LL * nshells];
+    if (L < 0) {
+      *err = "shell " + std::to_string(i) + ": L must be >= 0";
+      return PA_ERR_ARG;
+    }
+    if (L > lmax_allowed) {
+      *err = "shell " + std::to_string(i) + ": L = " + std::to_string(L) +
+             " exceeds the compiled maximum " + std::to_string(lmax_allowed);
+      return PA_ERR_LMAX;
+    }
+    if (nprim < 1) {
+      *err = "shell " + std::to_string(i) + ": needs at least one primitive";
+      return PA_ERR_ARG;
+    }
+    if (cptr < 1 || cptr + 2 > ndata || ptr < 1 || ptr + 2LL * nprim - 1 > ndata) {
+      *err = "shell " + std::to_string(i) + ": pointer outside bas_data (truncated basis?)";
+      return PA_ERR_ARG;
+    }
+    for (int d = 0; d < 3; ++d) s.A[d] = bas_data[cptr - 1 + d];
+    s.L = L;
+    s.nprim = nprim;
+    s.prim_off = static_cast<int>(b.exps.size());
+    s.sph_off = sph;
+    sph += 2 * L + 1;
+    std::vector<double> c(bas_data + ptr - 1, bas_data + ptr - 1 + nprim);
+    std::vector<double> e(bas_data + ptr - 1 + nprim, bas_data + ptr - 1 + 2 * nprim);
+    bool finite = std::isfinite(s.A[0]) && std::isfinite(s.A[1]) && std::isfinite(s.A[2]);
+    for (int k = 0; k < nprim; ++k) finite = finite && std::isfinite(c[k]) && std::isfinite(e[k]) && e[k] > 0.0;
+    if (!finite) {
+      *err = "shell " + std::to_string(i) + ": non-finite center, coefficient or non-positive exponent";
+      return PA_ERR_ARG;
+    }
+    double N = 0.0;
+    const double lp = L + 1.5;
+    for (int p = 0; p < nprim; ++p)
+      for (int q = 0; q < nprim; ++q)
+        N += c[p] * c[q] / std::pow(e[p] + e[q], lp) * std::pow(std::sqrt(e[p] * e[q]), lp);
+    for (int p = 0; p < nprim; ++p)
+      c[p] *= std::sqrt(std::pow(e[p], lp) / (std::pow(kPi, 1.5) / std::pow(2.0, L) * N));
+    b.exps.insert(b.exps.end(), e.begin(), e.end());
+    b.coefs.insert(b.coefs.end(), c.begin(), c.end());
+    b.lmax = std::max(b.lmax, L);
+  }
+  b.nsph = sph;
+  *out = std::move(b);
+  return PA_OK;
+}
+
+void build_pair_lists(const HostBasis& b, PairLists* out) {
+  PairLists p;
+  const int n = static_cast<int>(b.shells.size());
+  p.npairs = n * (n + 1) / 2;
+  p.lab_max = std::max(0, 2 * b.lmax);
+  p.pair_ab.reserve(p.npairs);
+  p.pair_unit0.reserve(p.npairs);
+  for (int a = 0; a < n; ++a)
+    for (int c = 0; c <= a; ++c) {
+      const HostShell& sa = b.shells[a];
+      const HostShell& sc = b.shells[c];
+      const int pair = static_cast<int>(p.pair_ab.size());
+      p.pair_ab.push_back(make_int2(a, c));
+      p.pair_unit0.push_back(static_cast<int>(p.unit_pair.size()));
+      const long long blk = static_cast<long long>(2 * sa.L + 1) * (2 * sc.L + 1) * ncum(sa.L + sc.L);
+      for (int i = 0; i < sa.nprim; ++i)
+        for (int j = 0; j < sc.nprim; ++j) {
+          p.unit_pair.push_back(pair);
+          p.unit_prims.push_back(make_int2(sa.prim_off + i, sc.prim_off + j));
+          p.unit_esph.push_back(p.esph_total);
+          p.esph_total += blk;
+        }
+    }
+  p.nunits = static_cast<int>(p.unit_pair.size());
+  p.class_off.assign(p.lab_max + 2, 0);
+  std::vector<int> lab(p.nunits);
+  for (int u = 0; u < p.nunits; ++u) {
+    const int2 ab = p.pair_ab[p.unit_pair[u]];
+    lab[u] = b.shells[ab.x].L + b.shells[ab.y].L;
+    p.class_off[lab[u] + 1]++;
+  }
+  for (int c = 0; c <= p.lab_max; ++c) p.class_off[c + 1] += p.class_off[c];
+  p.class_unit.assign(p.nunits, 0);
+  std::vector<int> fill(p.class_off.begin(), p.class_off.end() - 1);
+  for (int u = 0; u < p.nunits; ++u) p.class_unit[fill[lab[u]]++] = u;
+  *out = std::move(p);
+}
+
+void build_aux_lists(const HostBasis& b, AuxLists* out) {
+  AuxLists x;
+  x.lc_max = std::max(0, b.lmax);
+  x.class_off.assign(x.lc_max + 2, 0);
+  for (const HostShell& s : b.shells) x.class_off[s.L + 1]++;
+  for (int c = 0; c <= x.lc_max; ++c) x.class_off[c + 1] += x.class_off[c];
+  x.class_shell.assign(b.shells.size(), 0);
+  std::vector<int> fill(x.class_off.begin(), x.class_off.end() - 1);
+  for (int i = 0; i < static_cast<int>(b.shells.size()); ++i)
+    x.class_shell[fill[b.shells[i].L]++] = i;
+  *out = std::move(x);
+}
+
+cudaError_t Arena::reserve(size_t bytes) {
+  if (bytes <= cap) return cudaSuccess;
+  if (base) {
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return e;
+    cudaFree(base);
+    base = nullptr;
+    cap = 0;
+  }
+  const size_t want = bytes + bytes / 4 + (64 << 20);
+  cudaError_t e = cudaMalloc(&base, want);
+  if (e != cudaSuccess) {
+    base = nullptr;
+    return e;
+  }
+  cap = want;
+  return cudaSuccess;
+}
+
+}  // namespace pa
+
+// ---------------------------------------------------------------------------
+// Opaque basis handle.
+struct pa_basis_s {
+  int device = 0;
+  pa::HostBasis host;
+  pa::PairLists pairs;
+  pa::AuxLists aux;
+  char* dmem = nullptr;
+  pa::DevBasis dev;
+  int2* d_pair_ab = nullptr;
+  int* d_pair_unit0 = nullptr;
+  int* d_unit_pair = nullptr;
+  int2* d_unit_prims = nullptr;
+  long long* d_unit_esph = nullptr;
+  int* d_class_unit = nullptr;   // units grouped by Lab
+  int* d_class_off = nullptr;    // [lab_max + 2]
+  int* d_aux_shell = nullptr;    // aux shells grouped by L
+  int* d_aux_off = nullptr;      // [lc_max + 2]
+};
+
+namespace pa {
+namespace {
+
+struct Ctx {
+  std::mutex mu;
+  Arena arena;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ph[5] = {};  // phase boundaries: screen | bra | metric | 3c | solve
+  int* h_info = nullptr;  // pinned
+};
+
+std::mutex g_ctx_mu;
+std::vector<Ctx*> g_ctx;
+
+int current_ctx(Ctx** out, DeviceTables* dt) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(PA_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  std::string err;
+  const int st = get_device_tables(dt, &err);
+  if (st != PA_OK) return fail(st, err);
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  if (static_cast<int>(g_ctx.size()) <= dev) g_ctx.resize(dev + 1, nullptr);
+  if (!g_ctx[dev]) {
+    Ctx* c = new Ctx();
+    PA_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    PA_CUDA(cudaEventCreate(&c->ev0));
+    PA_CUDA(cudaEventCreate(&c->ev1));
+    for (auto& e : c->ph) PA_CUDA(cudaEventCreate(&e));
+    PA_CUDA(cudaMallocHost(&c->h_info, sizeof(int) * 4));
+    g_ctx[dev] = c;
+  }
+  *out = g_ctx[dev];
+  return PA_OK;
+}
+
+// Arena carving that can also just count bytes.
+struct Carver {
+  char* base = nullptr;
+  size_t used = 0;
+  template <class T>
+  T* take(size_t count) {
+    const size_t bytes = ((count * sizeof(T)) + 255) & ~size_t(255);
+    T* p = base ? reinterpret_cast<T*>(base + used) : nullptr;
+    used += bytes;
+    return p;
+  }
+};
+
+__global__ void k_gather_unit_keys(int n, const int* __restrict__ class_unit,
+                                   const int* __restrict__ unit_pair, const double* __restrict__ Qab,
+                                   double* keys, int* vals) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int u = class_unit[i];
+  keys[i] = Qab[unit_pair[u]];
+  vals[i] = u;
+}
+
+__global__ void k_gather_aux_keys(int n, const int* __restrict__ shells, const double* __restrict__ Qc,
+                                  double* keys, int* vals) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int s = shells[i];
+  keys[i] = Qc[s];
+  vals[i] = s;
+}
+
+__global__ void k_boys_eval(DeviceTables dt, int mode, int nmax, int n, const double* T, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n * (nmax + 1)) return;
+  const int k = i / (nmax + 1), m = i - k * (nmax + 1);
+  out[i] = boys_n(dt, mode, m, T[k]);
+}
+
+// Buffers of one density-fitting run.
+struct DfBuffers {
+  double *Qab, *Qc, *qmax, *esph, *ukeys, *slot_Q, *akeys, *aux_Q, *G, *M, *partial;
+  double4 *unit_pP, *slot_pP;
+  int *uvals, *sorted_unit, *avals, *sorted_aux, *info;
+  void* cub_tmp;
+  size_t cub_bytes;
+  std::vector<long long> g_off;      // per Lab class
+  struct ClassRun {
+    int lab, lc, ny, upc;
+    double* partial;
+  };
+  std::vector<ClassRun> runs;
+};
+
+size_t cub_temp_bytes(const pa_basis_s* orb, const pa_basis_s* aux) {
+  size_t b1 = 0, b2 = 0, b3 = 0;
+  const int nu = orb->pairs.nunits, nx = static_cast<int>(aux->host.shells.size());
+  cub::DeviceSegmentedRadixSort::SortPairsDescending(nullptr, b1, (const double*)nullptr, (double*)nullptr,
+                                                     (const int*)nullptr, (int*)nullptr, nu,
+                                                     orb->pairs.lab_max + 1, (const int*)nullptr,
+                                                     (const int*)nullptr);
+  cub::DeviceSegmentedRadixSort::SortPairsDescending(nullptr, b2, (const double*)nullptr, (double*)nullptr,
+                                                     (const int*)nullptr, (int*)nullptr, nx,
+                                                     aux->aux.lc_max + 1, (const int*)nullptr,
+                                                     (const int*)nullptr);
+  cub::DeviceReduce::Max(nullptr, b3, (const double*)nullptr, (double*)nullptr, nx);
+  return std::max(b1, std::max(b2, b3));
+}
+
+// Lays out all buffers of a run (counting when c.base == nullptr).
+void layout_df(Carver& c, const pa_basis_s* orb, const pa_basis_s* aux, int nd, DfBuffers* b) {
+  const PairLists& P = orb->pairs;
+  const int nx = static_cast<int>(aux->host.shells.size());
+  const long long naux = aux->host.nsph;
+  b->Qab = c.take<double>(P.npairs);
+  b->Qc = c.take<double>(nx);
+  b->qmax = c.take<double>(1);
+  b->unit_pP = c.take<double4>(P.nunits);
+  b->esph = c.take<double>(P.esph_total);
+  b->ukeys = c.take<double>(P.nunits);
+  b->uvals = c.take<int>(P.nunits);
+  b->slot_Q = c.take<double>(P.nunits);
+  b->sorted_unit = c.take<int>(P.nunits);
+  b->slot_pP = c.take<double4>(P.nunits);
+  b->akeys = c.take<double>(nx);
+  b->avals = c.take<int>(nx);
+  b->aux_Q = c.take<double>(nx);
+  b->sorted_aux = c.take<int>(nx);
+  b->info = c.take<int>(4);
+  b->g_off.assign(P.lab_max + 2, 0);
+  for (int lab = 0; lab <= P.lab_max; ++lab) {
+    const long long nu = P.class_off[lab + 1] - P.class_off[lab];
+    b->g_off[lab + 1] = b->g_off[lab] + nu * ncum(lab) * nd;
+  }
+  b->G = c.take<double>(b->g_off[P.lab_max + 1]);
+  b->M = c.take<double>(naux * naux);
+  b->cub_bytes = cub_temp_bytes(orb, aux);
+  b->cub_tmp = c.take<char>(b->cub_bytes);
+  // partial slabs
+  b->runs.clear();
+  size_t part_total = 0;
+  const AuxLists& X = aux->aux;
+  for (int lab = 0; lab <= P.lab_max; ++lab) {
+    const int nu = P.class_off[lab + 1] - P.class_off[lab];
+    if (nu == 0) continue;
+    for (int lc = 0; lc <= X.lc_max; ++lc) {
+      const int nxc = X.class_off[lc + 1] - X.class_off[lc];
+      if (nxc == 0) continue;
+      Df3cClassInfo ci;
+      df3c_class_info(lab, lc, &ci);
+      const int bx = (nxc + ci.tc - 1) / ci.tc;
+      const int bz = (nd + ci.ndc - 1) / ci.ndc;
+      const int target = 4 * 148;
+      int ny = std::max(1, (target + bx * bz - 1) / (bx * bz));
+      const int max_ny = (nu + ci.ub - 1) / ci.ub;
+      ny = std::min(ny, max_ny);
+      int upc = (nu + ny - 1) / ny;
+      upc = ((upc + ci.ub - 1) / ci.ub) * ci.ub;
+      ny = (nu + upc - 1) / upc;
+      DfBuffers::ClassRun r{lab, lc, ny, upc, nullptr};
+      b->runs.push_back(r);
+      part_total += static_cast<size_t>(ny) * nxc * (2 * lc + 1) * nd;
+    }
+  }
+  double* part = c.take<double>(part_total);
+  size_t off = 0;
+  for (auto& r : b->runs) {
+    const int nxc = X.class_off[r.lc + 1] - X.class_off[r.lc];
+    r.partial = part ? part + off : nullptr;
+    off += static_cast<size_t>(r.ny) * nxc * (2 * r.lc + 1) * nd;
+  }
+}
+
+UnitArrays unit_arrays(const pa_basis_s* orb, const DfBuffers& b) {
+  UnitArrays U;
+  U.unit_pair = orb->d_unit_pair;
+  U.unit_prims = orb->d_unit_prims;
+  U.unit_esph = orb->d_unit_esph;
+  U.unit_pP = b.unit_pP;
+  U.esph = b.esph;
+  return U;
+}
+
+// Schwarz vectors of both bases and the sorted class lists.
+int run_screening(const pa_basis_s* orb, const pa_basis_s* aux, const DeviceTables& dt,
+                  const Options& o, DfBuffers& b, cudaStream_t s, int* launches) {
+  const PairLists& P = orb->pairs;
+  const int nx = static_cast<int>(aux->host.shells.size());
+  UnitArrays U = unit_arrays(orb, b);
+  *launches += launch_unit_setup(orb->dev, orb->d_pair_ab, U, P.nunits, dt, s);
+  *launches += launch_schwarz_bra(orb->dev, orb->d_pair_ab, orb->d_pair_unit0, U, P.npairs,
+                                  P.lab_max, dt, o.boys_mode, b.Qab, s);
+  *launches += launch_schwarz_aux(aux->dev, dt, o.boys_mode, b.Qc, s);
+  if (nx > 0) {
+    size_t bytes = b.cub_bytes;
+    PA_CUDA(cub::DeviceReduce::Max(b.cub_tmp, bytes, b.Qc, b.qmax, nx, s));
+    ++*launches;
+  }
+  if (P.nunits > 0) {
+    k_gather_unit_keys<<<(P.nunits + 255) / 256, 256, 0, s>>>(P.nunits, orb->d_class_unit,
+                                                              orb->d_unit_pair, b.Qab, b.ukeys, b.uvals);
+    ++*launches;
+    size_t bytes = b.cub_bytes;
+    PA_CUDA(cub::DeviceSegmentedRadixSort::SortPairsDescending(
+        b.cub_tmp, bytes, b.ukeys, b.slot_Q, b.uvals, b.sorted_unit, P.nunits, P.lab_max + 1,
+        orb->d_class_off, orb->d_class_off + 1, 0, 64, s));
+    *launches += 2;
+  }
+  if (nx > 0) {
+    k_gather_aux_keys<<<(nx + 255) / 256, 256, 0, s>>>(nx, aux->d_aux_shell, b.Qc, b.akeys, b.avals);
+    ++*launches;
+    size_t bytes = b.cub_bytes;
+    PA_CUDA(cub::DeviceSegmentedRadixSort::SortPairsDescending(
+        b.cub_tmp, bytes, b.akeys, b.aux_Q, b.avals, b.sorted_aux, nx, aux->aux.lc_max + 1,
+        aux->d_aux_off, aux->d_aux_off + 1, 0, 64, s));
+    *launches += 2;
+  }
+  return PA_OK;
+}
+
+// df[naux, nd] (column-major) = L^-1 sum (ab|P) Dsym, into d_df.
+int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d_dens,
+           long long sd, long long si, long long sj, double* d_df, DfBuffers& b,
+           const DeviceTables& dt, const Options& o, cudaStream_t s, int* launches,
+           cudaEvent_t* ph, int* launches_3c) {
+  const PairLists& P = orb->pairs;
+  const AuxLists& X = aux->aux;
+  const int naux = aux->host.nsph;
+  int st = run_screening(orb, aux, dt, o, b, s, launches);
+  if (st != PA_OK) return st;
+  cudaEventRecord(ph[0], s);
+  UnitArrays U = unit_arrays(orb, b);
+  // density folding per bra class
+  for (int lab = 0; lab <= P.lab_max; ++lab) {
+    BraPrepArgs a;
+    a.slot0 = P.class_off[lab];
+    a.slot_end = P.class_off[lab + 1];
+    if (a.slot_end <= a.slot0 || nd == 0 || aux->host.shells.empty()) continue;
+    a.slot_Q = b.slot_Q;
+    a.qmax_aux = b.qmax;
+    a.thresh = o.screen_thresh;
+    a.sorted_unit = b.sorted_unit;
+    a.nd = nd;
+    a.dens = d_dens;
+    a.sd = sd;
+    a.si = si;
+    a.sj = sj;
+    a.slot_pP = b.slot_pP;
+    a.G = b.G;
+    a.g_base = b.g_off[lab];
+    *launches += launch_bra_prep(orb->dev, orb->d_pair_ab, U, a, lab, s);
+  }
+  cudaEventRecord(ph[1], s);
+  // metric and its Cholesky factor
+  *launches += launch_metric(aux->dev, dt, o.boys_mode, b.M, s);
+  *launches += cholesky_lower(b.M, naux, b.info, s);
+  cudaEventRecord(ph[2], s);
+  // three-center contraction
+  const int before3c = *launches;
+  if (nd > 0) {
+    for (const auto& r : b.runs) {
+      Df3cArgs a;
+      a.X = aux->dev;
+      a.dt = dt;
+      a.boys_mode = o.boys_mode;
+      a.thresh = o.screen_thresh;
+      a.unit_slot0 = P.class_off[r.lab];
+      a.n_units = P.class_off[r.lab + 1] - P.class_off[r.lab];
+      a.unit_Q = b.slot_Q;
+      a.slot_pP = b.slot_pP;
+      a.G = b.G + b.g_off[r.lab];
+      a.units_per_chunk = r.upc;
+      a.aux_slot0 = X.class_off[r.lc];
+      a.n_aux = X.class_off[r.lc + 1] - X.class_off[r.lc];
+      a.sorted_aux = b.sorted_aux;
+      a.aux_Q = b.aux_Q;
+      a.nd = nd;
+      a.partial = r.partial;
+      *launches += launch_df3c_class(r.lab, r.lc, a, r.ny, s);
+    }
+    for (int lc = 0; lc <= X.lc_max; ++lc) {
+      Df3cReduceArgs ra;
+      ra.X = aux->dev;
+      ra.aux_slot0 = X.class_off[lc];
+      ra.n_aux = X.class_off[lc + 1] - X.class_off[lc];
+      if (ra.n_aux == 0) continue;
+      ra.nc = 2 * lc + 1;
+      ra.nd = nd;
+      ra.naux = naux;
+      ra.sorted_aux = b.sorted_aux;
+      ra.nclasses = 0;
+      for (const auto& r : b.runs)
+        if (r.lc == lc) {
+          ra.part[ra.nclasses] = r.partial;
+          ra.ny[ra.nclasses] = r.ny;
+          ++ra.nclasses;
+        }
+      ra.df = d_df;
+      *launches += launch_df3c_reduce(ra, s);
+    }
+  }
+  *launches_3c = *launches - before3c;
+  cudaEventRecord(ph[3], s);
+  if (nd > 0) *launches += trsm_lower_left(b.M, naux, d_df, naux, nd, s);
+  return PA_OK;
+}
+
+int finish(Ctx* c, const DfBuffers& b, cudaStream_t s, int launches, float* ms) {
+  PA_CUDA(cudaGetLastError());
+  PA_CUDA(cudaEventRecord(c->ev1, s));
+  PA_CUDA(cudaMemcpyAsync(c->h_info, b.info, sizeof(int), cudaMemcpyDeviceToHost, s));
+  PA_CUDA(cudaStreamSynchronize(s));
+  PA_CUDA(cudaEventElapsedTime(ms, c->ev0, c->ev1));
+  float t[5];
+  PA_CUDA(cudaEventElapsedTime(&t[0], c->ev0, c->ph[0]));
+  for (int i = 1; i < 4; ++i) PA_CUDA(cudaEventElapsedTime(&t[i], c->ph[i - 1], c->ph[i]));
+  PA_CUDA(cudaEventElapsedTime(&t[4], c->ph[3], c->ev1));
+  g_stats.ms_screen = t[0];
+  g_stats.ms_bra = t[1];
+  g_stats.ms_metric = t[2];
+  g_stats.ms_3c = t[3];
+  g_stats.ms_solve = t[4];
+  g_stats.kernel_launches = launches;
+  g_stats.ms_total = *ms;
+  if (*c->h_info != 0)
+    return fail(PA_ERR_NOT_SPD, "metric (P|Q) is not positive definite (Cholesky pivot " +
+                                    std::to_string(*c->h_info) + ")");
+  return PA_OK;
+}
+
+int check_pair(pa_basis orb, pa_basis aux) {
+  if (!orb || !aux) return fail(PA_ERR_ARG, "null basis handle");
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (orb->device != dev || aux->device != dev)
+    return fail(PA_ERR_ARG, "basis handle belongs to another device");
+  return PA_OK;
+}
+
+int df_device(pa_basis orb, pa_basis aux, int ndens, int nbf, const double* d_dens, int layout,
+              double* d_df, int nstates, double* d_R, cudaStream_t user_stream) {
+  int st = check_pair(orb, aux);
+  if (st != PA_OK) return st;
+  if (ndens < 0 || nbf != orb->host.nsph)
+    return fail(PA_ERR_ARG, "nbf (" + std::to_string(nbf) + ") does not match the orbital basis (" +
+                                std::to_string(orb->host.nsph) + ")");
+  if (layout != PA_LAYOUT_FORTRAN && layout != PA_LAYOUT_C) return fail(PA_ERR_ARG, "unknown layout");
+  if (ndens > 0 && (!d_dens || !d_df)) return fail(PA_ERR_ARG, "null density or output pointer");
+  Ctx* c = nullptr;
+  DeviceTables dt;
+  st = current_ctx(&c, &dt);
+  if (st != PA_OK) return st;
+  std::lock_guard<std::mutex> lk(c->mu);
+  const Options o = options();
+  cudaStream_t s = user_stream;
+  DfBuffers b;
+  Carver cnt;
+  layout_df(cnt, orb, aux, ndens, &b);
+  if (d_R) cnt.take<double>(static_cast<size_t>(ndens) * ndens);
+  PA_CUDA(c->arena.reserve(cnt.used));
+  Carver real;
+  real.base = c->arena.base;
+  layout_df(real, orb, aux, ndens, &b);
+  double* gram = d_R ? real.take<double>(static_cast<size_t>(ndens) * ndens) : nullptr;
+  const long long n = nbf;
+  long long sd, si, sj;
+  if (layout == PA_LAYOUT_FORTRAN) {
+    sd = 1;
+    si = ndens;
+    sj = static_cast<long long>(ndens) * n;
+  } else {
+    sd = n * n;
+    si = n;
+    sj = 1;
+  }
+  PA_CUDA(cudaEventRecord(c->ev0, s));
+  int launches = 0, launches_3c = 0;
+  st = run_df(orb, aux, ndens, d_dens, sd, si, sj, d_df, b, dt, o, s, &launches, c->ph, &launches_3c);
+  if (st != PA_OK) return st;
+  g_stats.launches_3c = launches_3c;
+  if (d_R) launches += coulomb_4d(d_df, aux->host.nsph, ndens, nstates, gram, d_R, s);
+  float ms = 0.f;
+  g_stats.ntriplets = static_cast<long long>(orb->pairs.npairs) * aux->host.shells.size();
+  g_stats.nskipped = -1;
+  g_stats.nints = -1;
+  return finish(c, b, s, launches, &ms);
+}
+
+int nstates_of(int ndens) {
+  const int ns = static_cast<int>(std::lround((std::sqrt(8.0 * ndens + 1.0) - 1.0) / 2.0));
+  return ns * (ns + 1) / 2 == ndens ? ns : -1;
+}
+
+// Host-buffer path: copies in, runs on the library stream, copies out.
+int df_host(pa_basis orb, pa_basis aux, int ndens, int nbf, const double* dens, int layout,
+            double* out, int nstates) {
+  int st = check_pair(orb, aux);
+  if (st != PA_OK) return st;
+  Ctx* c = nullptr;
+  DeviceTables dt;
+  st = current_ctx(&c, &dt);
+  if (st != PA_OK) return st;
+  const size_t nd_bytes = sizeof(double) * static_cast<size_t>(ndens) * nbf * nbf;
+  const size_t df_count = static_cast<size_t>(aux->host.nsph) * ndens;
+  const size_t out_count = nstates > 0 ? static_cast<size_t>(nstates) * nstates * nstates * nstates : df_count;
+  double *d_dens = nullptr, *d_df = nullptr, *d_R = nullptr;
+  PA_CUDA(cudaMallocAsync(&d_dens, std::max<size_t>(nd_bytes, 8), c->stream));
+  PA_CUDA(cudaMallocAsync(&d_df, sizeof(double) * std::max<size_t>(df_count, 1), c->stream));
+  if (nstates > 0) PA_CUDA(cudaMallocAsync(&d_R, sizeof(double) * out_count, c->stream));
+  if (nd_bytes) PA_CUDA(cudaMemcpyAsync(d_dens, dens, nd_bytes, cudaMemcpyHostToDevice, c->stream));
+  st = df_device(orb, aux, ndens, nbf, d_dens, layout, d_df, nstates, d_R, c->stream);
+  if (st == PA_OK) {
+    cudaMemcpyAsync(out, nstates > 0 ? d_R : d_df, sizeof(double) * out_count, cudaMemcpyDeviceToHost,
+                    c->stream);
+  }
+  cudaFreeAsync(d_dens, c->stream);
+  cudaFreeAsync(d_df, c->stream);
+  if (d_R) cudaFreeAsync(d_R, c->stream);
+  const cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (st != PA_OK) return st;
+  if (e != cudaSuccess) return fail(PA_ERR_CUDA, std::string("download: ") + cudaGetErrorString(e));
+  return PA_OK;
+}
+
+struct BasisGuard {
+  pa_basis b = nullptr;
+  ~BasisGuard() {
+    if (b) pa_basis_destroy(b);
+  }
+};
+
+}  // namespace
+}  // namespace pa
+
+// ---------------------------------------------------------------------------
+// C-ABI
+using namespace pa;
+
+extern "C" {
+
+const char* pa_last_error(void) { return tl_err.c_str(); }
+
+int pa_set_boys_mode(int mode) {
+  if (mode != PA_BOYS_EXACT && mode != PA_BOYS_REFERENCE) return fail(PA_ERR_ARG, "unknown Boys mode");
+  std::lock_guard<std::mutex> lk(g_opt_mu);
+  g_opts.boys_mode = mode;
+  return PA_OK;
+}
+
+int pa_get_boys_mode(void) {
+  std::lock_guard<std::mutex> lk(g_opt_mu);
+  return g_opts.boys_mode;
+}
+
+int pa_set_screen_threshold(double thresh) {
+  if (!(thresh >= 0.0)) return fail(PA_ERR_ARG, "threshold must be >= 0");
+  std::lock_guard<std::mutex> lk(g_opt_mu);
+  g_opts.screen_thresh = thresh;
+  return PA_OK;
+}
+
+int pa_get_stats(pa_stats* out) {
+  if (!out) return fail(PA_ERR_ARG, "null stats pointer");
+  *out = g_stats;
+  return PA_OK;
+}
+
+int f_init(void) {
+  Ctx* c = nullptr;
+  DeviceTables dt;
+  return current_ctx(&c, &dt);
+}
+
+int pa_basis_create(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
+                    const double* bas_data, int lmax_allowed, pa_basis* out) {
+  if (!out) return fail(PA_ERR_ARG, "null output handle");
+  *out = nullptr;
+  if (lmax_allowed < 0 || lmax_allowed > std::max(PA_LMAX, PA_LAUXMAX))
+    lmax_allowed = std::max(PA_LMAX, PA_LAUXMAX);
+  Ctx* c = nullptr;
+  DeviceTables dt;
+  int st = current_ctx(&c, &dt);
+  if (st != PA_OK) return st;
+  pa_basis b = new pa_basis_s();
+  cudaGetDevice(&b->device);
+  std::string err;
+  st = unpack_basis(nshells, ndata, bas_centers, bas_spec, bas_data, lmax_allowed, &b->host, &err);
+  if (st != PA_OK) {
+    delete b;
+    return fail(st, err);
+  }
+  if (b->host.lmax <= PA_LMAX) build_pair_lists(b->host, &b->pairs);
+  build_aux_lists(b->host, &b->aux);
+  const HostBasis& h = b->host;
+  const PairLists& P = b->pairs;
+  const int ns = static_cast<int>(h.shells.size());
+  Carver cnt;
+  for (int pass = 0; pass < 2; ++pass) {
+    Carver& cv = cnt;
+    if (pass == 1) {
+      if (cudaMalloc(&b->dmem, std::max<size_t>(cnt.used, 256)) != cudaSuccess) {
+        delete b;
+        return fail(PA_ERR_CUDA, "cudaMalloc(basis) failed");
+      }
+      cv = Carver();
+      cv.base = b->dmem;
+    }
+    b->dev.shell = cv.take<int4>(ns);
+    b->dev.center = cv.take<double4>(ns);
+    b->dev.prim = cv.take<double2>(h.exps.size());
+    b->d_pair_ab = cv.take<int2>(P.pair_ab.size());
+    b->d_pair_unit0 = cv.take<int>(P.pair_unit0.size());
+    b->d_unit_pair = cv.take<int>(P.unit_pair.size());
+    b->d_unit_prims = cv.take<int2>(P.unit_prims.size());
+    b->d_unit_esph = cv.take<long long>(P.unit_esph.size());
+    b->d_class_unit = cv.take<int>(P.class_unit.size());
+    b->d_class_off = cv.take<int>(P.class_off.size());
+    b->d_aux_shell = cv.take<int>(b->aux.class_shell.size());
+    b->d_aux_off = cv.take<int>(b->aux.class_off.size());
+  }
+  std::vector<int4> shell(ns);
+  std::vector<double4> center(ns);
+  for (int i = 0; i < ns; ++i) {
+    const HostShell& s = h.shells[i];
+    shell[i] = make_int4(s.L, s.nprim, s.prim_off, s.sph_off);
+    center[i] = make_double4(s.A[0], s.A[1], s.A[2], 0.0);
+  }
+  std::vector<double2> prim(h.exps.size());
+  for (size_t k = 0; k < prim.size(); ++k) prim[k] = make_double2(h.exps[k], h.coefs[k]);
+  auto up = [&](void* dst, const void* src, size_t bytes) {
+    return bytes ? cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
+  };
+  cudaError_t e = cudaSuccess;
+  if (e == cudaSuccess) e = up(b->dev.shell, shell.data(), sizeof(int4) * ns);
+  if (e == cudaSuccess) e = up(b->dev.center, center.data(), sizeof(double4) * ns);
+  if (e == cudaSuccess) e = up(b->dev.prim, prim.data(), sizeof(double2) * prim.size());
+  if (e == cudaSuccess) e = up(b->d_pair_ab, P.pair_ab.data(), sizeof(int2) * P.pair_ab.size());
+  if (e == cudaSuccess) e = up(b->d_pair_unit0, P.pair_unit0.data(), sizeof(int) * P.pair_unit0.size());
+  if (e == cudaSuccess) e = up(b->d_unit_pair, P.unit_pair.data(), sizeof(int) * P.unit_pair.size());
+  if (e == cudaSuccess) e = up(b->d_unit_prims, P.unit_prims.data(), sizeof(int2) * P.unit_prims.size());
+  if (e == cudaSuccess) e = up(b->d_unit_esph, P.unit_esph.data(), sizeof(long long) * P.unit_esph.size());
+  if (e == cudaSuccess) e = up(b->d_class_unit, P.class_unit.data(), sizeof(int) * P.class_unit.size());
+  if (e == cudaSuccess) e = up(b->d_class_off, P.class_off.data(), sizeof(int) * P.class_off.size());
+  if (e == cudaSuccess) e = up(b->d_aux_shell, b->aux.class_shell.data(), sizeof(int) * b->aux.class_shell.size());
+  if (e == cudaSuccess) e = up(b->d_aux_off, b->aux.class_off.data(), sizeof(int) * b->aux.class_off.size());
+  if (e != cudaSuccess) {
+    cudaFree(b->dmem);
+    delete b;
+    return fail(PA_ERR_CUDA, std::string("basis upload: ") + cudaGetErrorString(e));
+  }
+  b->dev.nshells = ns;
+  b->dev.nprims = static_cast<int>(h.exps.size());
+  b->dev.nsph = h.nsph;
+  b->dev.lmax = h.lmax;
+  *out = b;
+  return PA_OK;
+}
+
+int pa_basis_destroy(pa_basis basis) {
+  if (!basis) return PA_OK;
+  if (basis->dmem) cudaFree(basis->dmem);
+  delete basis;
+  return PA_OK;
+}
+
+int pa_basis_info(pa_basis basis, int* nshells, int* nsph, int* lmax) {
+  if (!basis) return fail(PA_ERR_ARG, "null basis handle");
+  if (nshells) *nshells = static_cast<int>(basis->host.shells.size());
+  if (nsph) *nsph = basis->host.nsph;
+  if (lmax) *lmax = basis->host.lmax;
+  return PA_OK;
+}
+
+int pa_df_2d(pa_basis orbital, pa_basis aux, int ndens, int nbf, const double* d_densities,
+             int layout, double* d_df, void* stream) {
+  if (orbital && orbital->host.lmax > PA_LMAX)
+    return fail(PA_ERR_LMAX, "orbital basis L above the compiled maximum");
+  return df_device(orbital, aux, ndens, nbf, d_densities, layout, d_df, 0, nullptr,
+                   static_cast<cudaStream_t>(stream));
+}
+
+int pa_df_4d(pa_basis orbital, pa_basis aux, int ndens, int nbf, const double* d_densities,
+             int layout, int nstates, double* d_coulomb, void* stream) {
+  if (nstates < 0 || nstates * (nstates + 1) / 2 != ndens)
+    return fail(PA_ERR_ARG, "ndens must equal nstates (nstates + 1) / 2");
+  if (!d_coulomb) return fail(PA_ERR_ARG, "null output pointer");
+  Ctx* c = nullptr;
+  DeviceTables dt;
+  int st = current_ctx(&c, &dt);
+  if (st != PA_OK) return st;
+  double* d_df = nullptr;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  PA_CUDA(cudaMallocAsync(&d_df, sizeof(double) * std::max<size_t>(1, static_cast<size_t>(aux ? aux->host.nsph : 0) * ndens), s));
+  st = df_device(orbital, aux, ndens, nbf, d_densities, layout, d_df, nstates, d_coulomb, s);
+  cudaFreeAsync(d_df, s);
+  return st;
+}
+
+int pa_contract_coulomb_densities_2d(pa_basis orbital, pa_basis aux, int ndens, int nbf,
+                                     const double* densities, int layout, double* df_tensor) {
+  return df_host(orbital, aux, ndens, nbf, densities, layout, df_tensor, 0);
+}
+
+int pa_contract_coulomb_densities_4d(pa_basis orbital, pa_basis aux, int ndens, int nbf,
+                                     const double* densities, int layout, int nstates,
+                                     double* coulomb_tensor) {
+  if (nstates <= 0 || nstates * (nstates + 1) / 2 != ndens)
+    return fail(PA_ERR_ARG, "ndens must equal nstates (nstates + 1) / 2");
+  return df_host(orbital, aux, ndens, nbf, densities, layout, coulomb_tensor, nstates);
+}
+
+int f_contract_coulomb_densities_2d(int nshells, int ndata, const int* bas_centers,
+                                    const int* bas_spec, const double* bas_data, int nshells_aux,
+                                    int ndata_aux, const int* bas_centers_aux,
+                                    const int* bas_spec_aux, const double* bas_data_aux,
+                                    int ndens, int nbfs, const double* densities, int naux,
+                                    double* df_tensor) {
+  BasisGuard orb, aux;
+  int st = pa_basis_create(nshells, ndata, bas_centers, bas_spec, bas_data, PA_LMAX, &orb.b);
+  if (st != PA_OK) return st;
+  st = pa_basis_create(nshells_aux, ndata_aux, bas_centers_aux, bas_spec_aux, bas_data_aux,
+                       PA_LAUXMAX, &aux.b);
+  if (st != PA_OK) return st;
+  if (naux != aux.b->host.nsph)
+    return fail(PA_ERR_ARG, "naux (" + std::to_string(naux) + ") does not match the auxiliary basis (" +
+                                std::to_string(aux.b->host.nsph) + ")");
+  return df_host(orb.b, aux.b, ndens, nbfs, densities, PA_LAYOUT_FORTRAN, df_tensor, 0);
+}
+
+int f_contract_coulomb_densities_4d(int nshells, int ndata, const int* bas_centers,
+                                    const int* bas_spec, const double* bas_data, int nshells_aux,
+                                    int ndata_aux, const int* bas_centers_aux,
+                                    const int* bas_spec_aux, const double* bas_data_aux,
+                                    int ndens, int nbfs, const double* densities, int nstates,
+                                    double* coulomb_tensor) {
+  if (nstates <= 0 || nstates * (nstates + 1) / 2 != ndens)
+    return fail(PA_ERR_ARG, "ndens must equal nstates (nstates + 1) / 2");
+  BasisGuard orb, aux;
+  int st = pa_basis_create(nshells, ndata, bas_centers, bas_spec, bas_data, PA_LMAX, &orb.b);
+  if (st != PA_OK) return st;
+  st = pa_basis_create(nshells_aux, ndata_aux, bas_centers_aux, bas_spec_aux, bas_data_aux,
+                       PA_LAUXMAX, &aux.b);
+  if (st != PA_OK) return st;
+  return df_host(orb.b, aux.b, ndens, nbfs, densities, PA_LAYOUT_FORTRAN, coulomb_tensor, nstates);
+}
+
+// Schwarz vectors through the screening stage of the pipeline.
+static int schwarz_impl(pa_basis orb, pa_basis aux, double* q_bra, double* q_aux) {
+  Ctx* c = nullptr;
+  DeviceTables dt;
+  int st = current_ctx(&c, &dt);
+  if (st != PA_OK) return st;
+  std::lock_guard<std::mutex> lk(c->mu);
+  const Options o = options();
+  cudaStream_t s = c->stream;
+  int launches = 0;
+  if (orb) {
+    const PairLists& P = orb->pairs;
+    Carver cnt;
+    double* Qab = cnt.take<double>(P.npairs);
+    double4* pP = cnt.take<double4>(P.nunits);
+    double* esph = cnt.take<double>(P.esph_total);
+    PA_CUDA(c->arena.reserve(cnt.used));
+    Carver r;
+    r.base = c->arena.base;
+    Qab = r.take<double>(P.npairs);
+    pP = r.take<double4>(P.nunits);
+    esph = r.take<double>(P.esph_total);
+    UnitArrays U;
+    U.unit_pair = orb->d_unit_pair;
+    U.unit_prims = orb->d_unit_prims;
+    U.unit_esph = orb->d_unit_esph;
+    U.unit_pP = pP;
+    U.esph = esph;
+    launches += launch_unit_setup(orb->dev, orb->d_pair_ab, U, P.nunits, dt, s);
+    launches += launch_schwarz_bra(orb->dev, orb->d_pair_ab, orb->d_pair_unit0, U, P.npairs,
+                                   P.lab_max, dt, o.boys_mode, Qab, s);
+    if (P.npairs) PA_CUDA(cudaMemcpyAsync(q_bra, Qab, sizeof(double) * P.npairs, cudaMemcpyDeviceToHost, s));
+    PA_CUDA(cudaStreamSynchronize(s));
+  }
+  if (aux) {
+    const int nx = static_cast<int>(aux->host.shells.size());
+    PA_CUDA(c->arena.reserve(sizeof(double) * nx + 256));
+    double* Qc = reinterpret_cast<double*>(c->arena.base);
+    launches += launch_schwarz_aux(aux->dev, dt, o.boys_mode, Qc, s);
+    if (nx) PA_CUDA(cudaMemcpyAsync(q_aux, Qc, sizeof(double) * nx, cudaMemcpyDeviceToHost, s));
+    PA_CUDA(cudaStreamSynchronize(s));
+  }
+  PA_CUDA(cudaGetLastError());
+  g_stats.kernel_launches = launches;
+  return PA_OK;
+}
+
+int f_int_schwarz_aux(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
+                      const double* bas_data, double* integrals) {
+  BasisGuard b;
+  int st = pa_basis_create(nshells, ndata, bas_centers, bas_spec, bas_data, PA_LAUXMAX, &b.b);
+  if (st != PA_OK) return st;
+  if (nshells > 0 && !integrals) return fail(PA_ERR_ARG, "null output pointer");
+  return schwarz_impl(nullptr, b.b, nullptr, integrals);
+}
+
+int f_int_schwarz_bra(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
+                      const double* bas_data, double* integrals) {
+  BasisGuard b;
+  int st = pa_basis_create(nshells, ndata, bas_centers, bas_spec, bas_data, PA_LMAX, &b.b);
+  if (st != PA_OK) return st;
+  if (nshells > 0 && !integrals) return fail(PA_ERR_ARG, "null output pointer");
+  return schwarz_impl(b.b, nullptr, integrals, nullptr);
+}
+
+int pa_count_triplets(pa_basis orbital, pa_basis aux, long long* ntriplets, long long* ncomputed,
+                      long long* nints) {
+  int st = check_pair(orbital, aux);
+  if (st != PA_OK) return st;
+  std::vector<double> qb(orbital->pairs.npairs), qc(aux->host.shells.size());
+  st = schwarz_impl(orbital, aux, qb.data(), qc.data());
+  if (st != PA_OK) return st;
+  const double thr = options().screen_thresh;
+  std::vector<std::pair<double, int>> sc;
+  for (size_t i = 0; i < qc.size(); ++i) sc.push_back({qc[i], 2 * aux->host.shells[i].L + 1});
+  std::sort(sc.begin(), sc.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+  std::vector<long long> pre(sc.size() + 1, 0);
+  for (size_t i = 0; i < sc.size(); ++i) pre[i + 1] = pre[i] + sc[i].second;
+  long long ncomp = 0, ni = 0;
+  for (int p = 0; p < orbital->pairs.npairs; ++p) {
+    const double q = qb[p];
+    size_t lo = 0, hi = sc.size();  // count of leading entries with q * qc >= thr
+    while (lo < hi) {
+      const size_t mid = (lo + hi) / 2;
+      if (q * sc[mid].first >= thr)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    const int2 ab = orbital->pairs.pair_ab[p];
+    const long long nab = static_cast<long long>(2 * orbital->host.shells[ab.x].L + 1) *
+                          (2 * orbital->host.shells[ab.y].L + 1);
+    ncomp += static_cast<long long>(lo);
+    ni += nab * pre[lo];
+  }
+  if (ntriplets) *ntriplets = static_cast<long long>(orbital->pairs.npairs) * qc.size();
+  if (ncomputed) *ncomputed = ncomp;
+  if (nints) *nints = ni;
+  g_stats.ntriplets = static_cast<long long>(orbital->pairs.npairs) * qc.size();
+  g_stats.nskipped = g_stats.ntriplets - ncomp;
+  g_stats.nints = ni;
+  return PA_OK;
+}
+
+int pa_boys_eval(int mode, int nmax, int n, const double* T, double* out) {
+  if (nmax < 0 || nmax > PA_BOYS_NMAX || n < 0 || (n > 0 && (!T || !out)))
+    return fail(PA_ERR_ARG, "invalid Boys evaluation request");
+  if (mode != PA_BOYS_EXACT && mode != PA_BOYS_REFERENCE) return fail(PA_ERR_ARG, "unknown Boys mode");
+  for (int i = 0; i < n; ++i)
+    if (!(T[i] >= 0.0) || !std::isfinite(T[i])) return fail(PA_ERR_ARG, "Boys argument must be finite and >= 0");
+  Ctx* c = nullptr;
+  DeviceTables dt;
+  int st = current_ctx(&c, &dt);
+  if (st != PA_OK) return st;
+  std::lock_guard<std::mutex> lk(c->mu);
+  const size_t nout = static_cast<size_t>(n) * (nmax + 1);
+  PA_CUDA(c->arena.reserve(sizeof(double) * (n + nout) + 512));
+  double* dT = reinterpret_cast<double*>(c->arena.base);
+  double* dO = dT + ((n + 31) / 32) * 32;
+  if (n == 0) return PA_OK;
+  PA_CUDA(cudaMemcpyAsync(dT, T, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+  k_boys_eval<<<static_cast<int>((nout + 255) / 256), 256, 0, c->stream>>>(dt, mode, nmax, n, dT, dO);
+  PA_CUDA(cudaGetLastError());
+  PA_CUDA(cudaMemcpyAsync(out, dO, sizeof(double) * nout, cudaMemcpyDeviceToHost, c->stream));
+  PA_CUDA(cudaStreamSynchronize(c->stream));
+  return PA_OK;
+}
+
+int pa_metric(pa_basis aux, double* metric) {
+  if (!aux || !metric) return fail(PA_ERR_ARG, "null argument");
+  Ctx* c = nullptr;
+  DeviceTables dt;
+  int st = current_ctx(&c, &dt);
+  if (st != PA_OK) return st;
+  std::lock_guard<std::mutex> lk(c->mu);
+  const size_t n = aux->host.nsph;
+  PA_CUDA(c->arena.reserve(sizeof(double) * n * n + 256));
+  double* M = reinterpret_cast<double*>(c->arena.base);
+  launch_metric(aux->dev, dt, options().boys_mode, M, c->stream);
+  PA_CUDA(cudaGetLastError());
+  PA_CUDA(cudaMemcpyAsync(metric, M, sizeof(double) * n * n, cudaMemcpyDeviceToHost, c->stream));
+  PA_CUDA(cudaStreamSynchronize(c->stream));
+  return PA_OK;
+}
+
+int pa_cholesky_solve(int n, double* A, int nrhs, double* B) {
+  if (n < 0 || nrhs < 0 || (n > 0 && !A) || (n > 0 && nrhs > 0 && !B))
+    return fail(PA_ERR_ARG, "invalid Cholesky arguments");
+  Ctx* c = nullptr;
+  DeviceTables dt;
+  int st = current_ctx(&c, &dt);
+  if (st != PA_OK) return st;
+  std::lock_guard<std::mutex> lk(c->mu);
+  const size_t nn = static_cast<size_t>(n) * n, nb = static_cast<size_t>(n) * nrhs;
+  PA_CUDA(c->arena.reserve(sizeof(double) * (nn + nb) + 1024));
+  Carver cv;
+  cv.base = c->arena.base;
+  double* dA = cv.take<double>(nn);
+  double* dB = cv.take<double>(nb);
+  int* info = cv.take<int>(1);
+  if (n == 0) return PA_OK;
+  PA_CUDA(cudaMemcpyAsync(dA, A, sizeof(double) * nn, cudaMemcpyHostToDevice, c->stream));
+  if (nb) PA_CUDA(cudaMemcpyAsync(dB, B, sizeof(double) * nb, cudaMemcpyHostToDevice, c->stream));
+  cholesky_lower(dA, n, info, c->stream);
+  if (nb) trsm_lower_left(dA, n, dB, n, nrhs, c->stream);
+  PA_CUDA(cudaGetLastError());
+  PA_CUDA(cudaMemcpyAsync(A, dA, sizeof(double) * nn, cudaMemcpyDeviceToHost, c->stream));
+  if (nb) PA_CUDA(cudaMemcpyAsync(B, dB, sizeof(double) * nb, cudaMemcpyDeviceToHost, c->stream));
+  PA_CUDA(cudaMemcpyAsync(c->h_info, info, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  PA_CUDA(cudaStreamSynchronize(c->stream));
+  if (*c->h_info != 0)
+    return fail(PA_ERR_NOT_SPD, "matrix is not positive definite (Cholesky pivot " +
+                                    std::to_string(*c->h_info) + ")");
+  return PA_OK;
+}
+
+int f_intor_eri2c(int, int, const int*, const int*, const double*, int, int, const int*, const int*,
+                  const double*, int, double*) {
+  return fail(PA_ERR_ARG, "f_intor_eri2c: not available in this build");
+}
+int f_intor_df1c(int, int, const int*, const int*, const double*, int, int, const int*, const int*,
+                 const double*, int, int, double*) {
+  return fail(PA_ERR_ARG, "f_intor_df1c: not available in this build");
+}
+int f_intor_df2c_mo(int, int, const int*, const int*, const double*, int, int, const int*,
+                    const int*, const double*, int, int, const double*, int, double*) {
+  return fail(PA_ERR_ARG, "f_intor_df2c_mo: not available in this build");
+}
+
+}  // extern "C"

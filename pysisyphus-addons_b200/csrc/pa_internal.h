@@ -1,0 +1,145 @@
+// Host-side structures and kernel launchers of libpa_b200.so (internal).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "pa_common.cuh"
+
+namespace pa {
+
+// ---------------------------------------------------------------------------
+// Basis on the host, unpacked like common/shells.f90:97-187 and normalized like
+// common/normalization.f90:10-38.
+struct HostShell {
+  int L = 0, nprim = 0, prim_off = 0, sph_off = 0;
+  double A[3] = {0, 0, 0};
+};
+
+struct HostBasis {
+  std::vector<HostShell> shells;
+  std::vector<double> exps, coefs;  // coefs renormalized
+  int nsph = 0;
+  int lmax = -1;
+};
+
+// Returns PA_OK or an error code (message in *err).
+int unpack_basis(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
+                 const double* bas_data, int lmax_allowed, HostBasis* out, std::string* err);
+
+// ---------------------------------------------------------------------------
+// Device copy of a basis (structure of arrays).
+struct DevBasis {
+  int nshells = 0, nprims = 0, nsph = 0, lmax = -1;
+  int4* shell = nullptr;      // (L, nprim, prim_off, sph_off)
+  double4* center = nullptr;  // (x, y, z, 0)
+  double2* prim = nullptr;    // (exponent, normalized coefficient)
+};
+
+// Orbital shell pairs a >= b and their primitive pairs ("bra units"), grouped
+// by Lab = la + lb. Built on the host from the basis alone.
+struct PairLists {
+  int npairs = 0;
+  int nunits = 0;
+  int lab_max = 0;
+  std::vector<int2> pair_ab;          // pair -> (a, b)
+  std::vector<int> pair_unit0;        // pair -> first unit (units of a pair are contiguous)
+  std::vector<int> unit_pair;         // unit -> pair
+  std::vector<int2> unit_prims;       // unit -> (prim index in a, prim index in b), global
+  std::vector<long long> unit_esph;   // unit -> offset of its E_sph block (doubles)
+  long long esph_total = 0;
+  // units sorted by class: class_units[c] = list of units with Lab = c (host order)
+  std::vector<int> class_off;         // [lab_max + 2] offsets into class_unit
+  std::vector<int> class_unit;        // units grouped by class
+};
+
+struct AuxLists {
+  int lc_max = 0;
+  std::vector<int> class_off;   // [lc_max + 2]
+  std::vector<int> class_shell; // aux shells grouped by L
+};
+
+void build_pair_lists(const HostBasis& b, PairLists* out);
+void build_aux_lists(const HostBasis& b, AuxLists* out);
+
+// ---------------------------------------------------------------------------
+// Options and statistics.
+struct Options {
+  int boys_mode = 1;          // 1 = reference-compatible (default), 0 = exact
+  double screen_thresh = static_cast<double>(1e-10f);
+  int verbose = 0;
+};
+
+struct Stats {
+  long long ntriplets = 0, nskipped = 0, nints = 0;
+  long long n3c_flops_model = 0;
+  double ms_screen = 0, ms_metric = 0, ms_chol = 0, ms_bra = 0, ms_3c = 0, ms_trsm = 0,
+         ms_total = 0;
+  int kernel_launches = 0;
+};
+
+// ---------------------------------------------------------------------------
+// Device tables (built once per device).
+int get_device_tables(DeviceTables* out, std::string* err);
+
+// ---------------------------------------------------------------------------
+// Stream-ordered scratch arena (grow-only, one per device).
+struct Arena {
+  char* base = nullptr;
+  size_t cap = 0, used = 0;
+  cudaError_t reserve(size_t bytes);
+  void reset() { used = 0; }
+  template <class T>
+  T* take(size_t count) {
+    const size_t bytes = ((count * sizeof(T)) + 255) & ~size_t(255);
+    T* p = reinterpret_cast<T*>(base + used);
+    used += bytes;
+    return p;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Kernel launchers (return the number of kernel launches issued).
+struct UnitArrays {
+  // per unit (host order)
+  const int* unit_pair;
+  const int2* unit_prims;
+  const long long* unit_esph;
+  double4* unit_pP;   // (p, Px, Py, Pz)
+  double* esph;       // E_sph blocks
+};
+
+int launch_unit_setup(const DevBasis& B, const int2* pair_ab, UnitArrays U, int nunits,
+                      const DeviceTables& dt, cudaStream_t s);
+int launch_schwarz_bra(const DevBasis& B, const int2* pair_ab, const int* pair_unit0,
+                       UnitArrays U, int npairs, int lab_max, const DeviceTables& dt,
+                       int boys_mode, double* Qab, cudaStream_t s);
+int launch_schwarz_aux(const DevBasis& X, const DeviceTables& dt, int boys_mode, double* Qc,
+                       cudaStream_t s);
+int launch_metric(const DevBasis& X, const DeviceTables& dt, int boys_mode, double* M,
+                  cudaStream_t s);
+
+// 3c2e contraction with densities for all classes.
+struct Df3cPlan {
+  // sorted (by Q desc within class) unit slots
+  int lab_max = 0, lc_max = 0;
+  std::vector<int> unit_class_off;  // [lab_max + 2]
+  std::vector<int> aux_class_off;   // [lc_max + 2]
+  int nd = 0;
+};
+
+struct Df3cDev {
+  const int* sorted_unit;    // slot -> unit (host order id)
+  const double* unit_Q;      // slot -> Q (sorted)
+  double4* slot_pP;          // slot -> (p, P)
+  double* G;                 // G blocks per slot: class offsets g_off[c]
+  const long long* g_off;    // host array copy is in plan
+  const int* sorted_aux;     // aux slot -> shell
+  const double* aux_Q;       // aux slot -> Q (sorted)
+  double* partial;
+};
+
+}  // namespace pa

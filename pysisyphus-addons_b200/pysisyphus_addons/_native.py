@@ -1,0 +1,224 @@
+"""ctypes binding of libpa_b200.so (the C-ABI declared in include/pa_b200.h).
+
+This replaces the Cython modules (``*/_intor.pyx``) of the reference: the
+argument lists are the ones of the reference's ``bind(c)`` wrappers, arrays are
+column-major, basis pointers 1-based. There is no CPU fallback -- if the CUDA
+library has not been built, importing this module raises.
+"""
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(os.environ.get("PA_B200_LIB", Path(__file__).resolve().parent / "_lib" / "libpa_b200.so"))
+
+PA_OK = 0
+PA_ERR_ARG = 1
+PA_ERR_LMAX = 2
+PA_ERR_NOT_SPD = 3
+PA_ERR_CUDA = 4
+PA_ERR_TIMEOUT = 5
+PA_ERR_NO_DEVICE = 6
+PA_ERR_SCRATCH = 7
+
+PA_BOYS_EXACT = 0
+PA_BOYS_REFERENCE = 1
+PA_LAYOUT_FORTRAN = 0
+PA_LAYOUT_C = 1
+PA_LMAX_ORBITAL = 4
+PA_LMAX_AUX = 5
+
+_ERRNAMES = {
+    PA_ERR_ARG: "invalid argument",
+    PA_ERR_LMAX: "angular momentum above the compiled maximum",
+    PA_ERR_NOT_SPD: "metric not positive definite",
+    PA_ERR_CUDA: "CUDA error",
+    PA_ERR_TIMEOUT: "device timeout",
+    PA_ERR_NO_DEVICE: "no CUDA device",
+    PA_ERR_SCRATCH: "scratch capacity exceeded",
+}
+
+
+class PaError(RuntimeError):
+    def __init__(self, code, message):
+        self.code = code
+        super().__init__(f"{_ERRNAMES.get(code, 'error')} ({code}): {message}")
+
+
+class PaStats(ctypes.Structure):
+    _fields_ = [
+        ("ntriplets", ctypes.c_longlong),
+        ("nskipped", ctypes.c_longlong),
+        ("nints", ctypes.c_longlong),
+        ("ms_total", ctypes.c_double),
+        ("ms_screen", ctypes.c_double),
+        ("ms_bra", ctypes.c_double),
+        ("ms_metric", ctypes.c_double),
+        ("ms_3c", ctypes.c_double),
+        ("ms_solve", ctypes.c_double),
+        ("kernel_launches", ctypes.c_int),
+        ("launches_3c", ctypes.c_int),
+    ]
+
+
+_i = ctypes.c_int
+_d = ctypes.c_double
+_pi = ctypes.POINTER(ctypes.c_int)
+_pd = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+_BASIS = [_i, _i, _pi, _pi, _pd]
+
+# Symbols declared in include/pa_b200.h with their argument types.
+SIGNATURES = {
+    "f_init": [],
+    "f_int_schwarz_aux": _BASIS + [_pd],
+    "f_int_schwarz_bra": _BASIS + [_pd],
+    "f_contract_coulomb_densities_2d": _BASIS + _BASIS + [_i, _i, _pd, _i, _pd],
+    "f_contract_coulomb_densities_4d": _BASIS + _BASIS + [_i, _i, _pd, _i, _pd],
+    "f_intor_eri2c": _BASIS + _BASIS + [_i, _pd],
+    "f_intor_df1c": _BASIS + _BASIS + [_i, _i, _pd],
+    "f_intor_df2c_mo": _BASIS + _BASIS + [_i, _i, _pd, _i, _pd],
+    "pa_last_error": [],
+    "pa_set_boys_mode": [_i],
+    "pa_get_boys_mode": [],
+    "pa_set_screen_threshold": [_d],
+    "pa_get_stats": [ctypes.POINTER(PaStats)],
+    "pa_basis_create": [_i, _i, _pi, _pi, _pd, _i, ctypes.POINTER(_vp)],
+    "pa_basis_destroy": [_vp],
+    "pa_basis_info": [_vp, _pi, _pi, _pi],
+    "pa_df_2d": [_vp, _vp, _i, _i, _vp, _i, _vp, _vp],
+    "pa_df_4d": [_vp, _vp, _i, _i, _vp, _i, _i, _vp, _vp],
+    "pa_contract_coulomb_densities_2d": [_vp, _vp, _i, _i, _pd, _i, _pd],
+    "pa_contract_coulomb_densities_4d": [_vp, _vp, _i, _i, _pd, _i, _i, _pd],
+    "pa_count_triplets": [_vp, _vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
+                          ctypes.POINTER(ctypes.c_longlong)],
+    "pa_boys_eval": [_i, _i, _i, _pd, _pd],
+    "pa_metric": [_vp, _pd],
+    "pa_cholesky_solve": [_i, _pd, _i, _pd],
+}
+
+_lib = None
+
+
+def load():
+    """Load libpa_b200.so (raises if it is missing: there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"{LIB_PATH} not found: build the CUDA library first "
+            "(make -C pysisyphus-addons_b200, or __graft_entry__.build())"
+        )
+    lib = ctypes.CDLL(str(LIB_PATH))
+    for name, args in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = ctypes.c_char_p if name == "pa_last_error" else ctypes.c_int
+    _lib = lib
+    return lib
+
+
+def check(rc):
+    if rc != PA_OK:
+        msg = load().pa_last_error().decode(errors="replace")
+        raise PaError(rc, msg)
+
+
+def ptr(arr, ctype=ctypes.c_double):
+    return arr.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def basis_args(shells):
+    """(keep-alive arrays, ctypes argument list) of a shells object."""
+    bc, bs, bd = shells.as_arrays(fortran=True)
+    bc = np.asfortranarray(bc, dtype=np.int32)
+    bs = np.asfortranarray(bs, dtype=np.int32)
+    bd = np.ascontiguousarray(bd, dtype=np.float64)
+    return (bc, bs, bd), [len(bc), len(bd), ptr(bc, ctypes.c_int), ptr(bs, ctypes.c_int), ptr(bd)]
+
+
+def nsph(shells):
+    _, bs, _ = shells.as_arrays(fortran=True)
+    return int(np.sum(2 * np.asarray(bs)[:, 1] + 1))
+
+
+def set_boys_mode(mode):
+    """'reference' (default; the reference's interpolation) or 'exact'."""
+    code = {"exact": PA_BOYS_EXACT, "reference": PA_BOYS_REFERENCE}.get(mode, mode)
+    check(load().pa_set_boys_mode(int(code)))
+
+
+def get_boys_mode():
+    return {PA_BOYS_EXACT: "exact", PA_BOYS_REFERENCE: "reference"}[load().pa_get_boys_mode()]
+
+
+def set_screen_threshold(thresh):
+    check(load().pa_set_screen_threshold(float(thresh)))
+
+
+def get_stats():
+    st = PaStats()
+    check(load().pa_get_stats(ctypes.byref(st)))
+    return {name: getattr(st, name) for name, _ in PaStats._fields_}
+
+
+def boys(nmax, T, mode="reference"):
+    """F_0..F_nmax at the points T, evaluated on the device; shape (len(T), nmax+1)."""
+    T = np.ascontiguousarray(np.atleast_1d(T), dtype=np.float64)
+    out = np.zeros((len(T), nmax + 1))
+    code = {"exact": PA_BOYS_EXACT, "reference": PA_BOYS_REFERENCE}.get(mode, mode)
+    check(load().pa_boys_eval(int(code), int(nmax), len(T), ptr(T), ptr(out)))
+    return out
+
+
+class Basis:
+    """A basis unpacked, normalized and resident in device memory (pa_basis)."""
+
+    def __init__(self, shells, role="orbital"):
+        lib = load()
+        keep, args = basis_args(shells)
+        lmax = PA_LMAX_ORBITAL if role == "orbital" else PA_LMAX_AUX
+        handle = _vp()
+        check(lib.pa_basis_create(*args, lmax, ctypes.byref(handle)))
+        self.handle = handle
+        n, ns, lm = _i(), _i(), _i()
+        check(lib.pa_basis_info(handle, ctypes.byref(n), ctypes.byref(ns), ctypes.byref(lm)))
+        self.nshells, self.nsph, self.lmax = n.value, ns.value, lm.value
+        self.role = role
+
+    def close(self):
+        if getattr(self, "handle", None):
+            load().pa_basis_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def count_triplets(orbital, aux):
+    """(ntriplets, ncomputed, nints) of the Schwarz screening for two Basis objects."""
+    a, b, c = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+    check(load().pa_count_triplets(orbital.handle, aux.handle, ctypes.byref(a), ctypes.byref(b),
+                                   ctypes.byref(c)))
+    return a.value, b.value, c.value
+
+
+def metric(aux):
+    out = np.zeros((aux.nsph, aux.nsph), order="F")
+    check(load().pa_metric(aux.handle, ptr(out)))
+    return out
+
+
+def cholesky_solve(A, B):
+    """(L, L^-1 B) computed on the device (lower Cholesky factor of A)."""
+    A = np.array(A, dtype=np.float64, order="F", copy=True)
+    B = np.array(B, dtype=np.float64, order="F", copy=True)
+    n = A.shape[0]
+    check(load().pa_cholesky_solve(n, ptr(A), B.shape[1] if B.ndim == 2 else 1, ptr(B)))
+    return A, B

@@ -1,0 +1,186 @@
+"""GPU (libpa_b200.so through its C-ABI) against the oracle and the golden
+vectors. Tolerances: the reference asserts the Coulomb tensor at atol 1e-12
+(tests/test_coulomb_tensor/test_coulomb_tensor.py:32); two FP64
+implementations with different summation orders agree to a few ulp of the
+largest element, so tensors are compared at atol 1e-12 + 1e-13 * max|ref|
+(about 1e-11 on the ~345 golden diagonal)."""
+
+import json
+
+import numpy as np
+import pytest
+
+import oracle
+from pysisyphus_addons import _native as nat
+from pysisyphus_addons.common.shells import Shell, Shells
+from pysisyphus_addons.common.synthetic import config_workload
+from pysisyphus_addons.diabatization import intor as dia
+from pysisyphus_addons.intor import intor as sch
+
+pytestmark = pytest.mark.gpu
+
+MODES = ["reference", "exact"]
+
+
+def assert_tensor_close(x, ref, atol=1e-12, rel_of_max=1e-13):
+    tol = atol + rel_of_max * np.abs(ref).max()
+    err = np.abs(x - ref).max()
+    assert err <= tol, f"max abs err {err:.3e} > {tol:.3e}"
+
+
+@pytest.fixture(params=MODES)
+def mode(request):
+    nat.set_boys_mode(request.param)
+    oracle.set_boys_mode(request.param)
+    yield request.param
+    nat.set_boys_mode("reference")
+
+
+def bena2(golden_dir):
+    basis = json.loads((golden_dir / "bena2_basis.json").read_text())
+    shells = Shells([Shell(b["L"], b["center"], b["coeffs"], b["exps"], b["center_ind"], b["atomic_num"])
+                     for b in basis])
+    return shells, np.load(golden_dir / "bena2_densities.npy"), json.loads(
+        (golden_dir / "bena2_coulomb_ref.json").read_text())
+
+
+def test_boys_device_vs_oracle(mode):
+    T = np.array([0.0, 1e-12, 1e-3, 0.049, 0.05, 0.5, 1.0, 3.3, 7.77, 14.2, 26.98, 26.999, 27.0,
+                  27.5, 35.0, 39.99, 40.0, 41.0, 77.7, 400.0])
+    F = nat.boys(16, T, mode)
+    for i, t in enumerate(T):
+        ref = oracle.boys(16, t)
+        np.testing.assert_allclose(F[i], ref, rtol=2e-14, atol=0, err_msg=f"T={t}")
+
+
+def test_golden_coulomb_tensor_gpu(golden_dir, mode):
+    shells, D, ref = bena2(golden_dir)
+    R = dia.contract_coulomb_densities_4d(shells, shells, D)
+    np.testing.assert_allclose(R, np.array(ref["tensor"]), atol=ref["atol"], rtol=ref["rtol"])
+    Ro = oracle.contract_coulomb_densities_4d(shells, shells, D)
+    assert_tensor_close(R, Ro)
+
+
+def test_schwarz_vs_oracle(mode):
+    w = config_workload("cfg1")
+    np.testing.assert_allclose(sch.int_schwarz_aux(w.shells_aux), oracle.int_schwarz_aux(w.shells_aux),
+                               rtol=1e-12, atol=1e-300)
+    np.testing.assert_allclose(sch.int_schwarz_bra(w.shells), oracle.int_schwarz_bra(w.shells),
+                               rtol=1e-12, atol=1e-300)
+
+
+def test_metric_vs_oracle(mode):
+    w = config_workload("cfg1")
+    M = nat.metric(nat.Basis(w.shells_aux, "aux"))
+    Mo = oracle.int2c2e(w.shells_aux)
+    assert_tensor_close(M, Mo, atol=1e-12, rel_of_max=1e-14)
+
+
+def test_df2d_vs_oracle_cfg1(mode):
+    w = config_workload("cfg1")
+    df = dia.contract_coulomb_densities_2d(w.shells, w.shells_aux, w.densities)
+    ref = oracle.contract_coulomb_densities_2d(w.shells, w.shells_aux, w.densities)
+    assert df.shape == ref.shape and df.flags.f_contiguous
+    assert_tensor_close(df, ref, atol=1e-11)
+
+
+def test_coulomb4d_vs_oracle_cfg1(mode):
+    w = config_workload("cfg1")
+    R = dia.contract_coulomb_densities_4d(w.shells, w.shells_aux, w.densities)
+    Ro = oracle.contract_coulomb_densities_4d(w.shells, w.shells_aux, w.densities)
+    assert_tensor_close(R, Ro)
+
+
+def test_coulomb4d_vs_fixture_cfg2(golden_dir, mode):
+    """40 atoms, lmax 3 / lauxmax 4, 8 states: the plain FP64 path vs the oracle."""
+    w = config_workload("cfg2")
+    R = dia.contract_coulomb_densities_4d(w.shells, w.shells_aux, w.densities)
+    fx = np.load(golden_dir / f"oracle_cfg2_{mode}.npz")
+    assert_tensor_close(R, fx["R"])
+    df = dia.contract_coulomb_densities_2d(w.shells, w.shells_aux, w.densities)
+    assert_tensor_close(df, fx["df"], atol=1e-11)
+
+
+def test_density_layouts_agree():
+    w = config_workload("cfg1")
+    a = dia.contract_coulomb_densities_2d(w.shells, w.shells_aux, np.ascontiguousarray(w.densities))
+    b = dia.contract_coulomb_densities_2d(w.shells, w.shells_aux, np.asfortranarray(w.densities))
+    np.testing.assert_array_equal(a, b)
+
+
+def test_deterministic():
+    w = config_workload("cfg1")
+    a = dia.contract_coulomb_densities_4d(w.shells, w.shells_aux, w.densities)
+    b = dia.contract_coulomb_densities_4d(w.shells, w.shells_aux, w.densities)
+    np.testing.assert_array_equal(a, b)
+
+
+def test_screening_counts_match_oracle():
+    w = config_workload("cfg1")
+    oracle.set_boys_mode("reference")
+    oracle.contract_coulomb_densities_2d(w.shells, w.shells_aux, w.densities)
+    st = oracle.last_stats()
+    ntrip, ncomp, nints = nat.count_triplets(nat.Basis(w.shells, "orbital"), nat.Basis(w.shells_aux, "aux"))
+    assert ntrip == st["ntriplets"]
+    assert ntrip - ncomp == st["nskipped"]
+    assert nints == st["nints"]
+
+
+def test_single_state_and_empty_densities():
+    w = config_workload("cfg1")
+    D1 = w.densities[:1]
+    R = dia.contract_coulomb_densities_4d(w.shells, w.shells_aux, D1)
+    oracle.set_boys_mode("reference")
+    Ro = oracle.contract_coulomb_densities_4d(w.shells, w.shells_aux, D1)
+    assert R.shape == (1, 1, 1, 1)
+    assert_tensor_close(R, Ro)
+    df = dia.contract_coulomb_densities_2d(w.shells, w.shells_aux, w.densities[:0])
+    assert df.shape == (w.shells_aux.sph_size, 0)
+
+
+def test_error_lmax():
+    sh = Shells([Shell(5, [0, 0, 0], [1.0], [1.0])])
+    aux = Shells([Shell(0, [0, 0, 0], [1.0], [1.0])])
+    with pytest.raises(nat.PaError) as e:
+        dia.contract_coulomb_densities_2d(sh, aux, np.zeros((1, 11, 11)))
+    assert e.value.code == nat.PA_ERR_LMAX
+
+
+def test_error_truncated_basis():
+    lib = nat.load()
+    sh = Shells([Shell(1, [0, 0, 0], [1.0, 0.5], [1.0, 0.3])])
+    keep, args = nat.basis_args(sh)
+    args[1] = args[1] - 2  # ndata too small: pointer runs past bas_data
+    out = np.zeros(1)
+    rc = lib.f_int_schwarz_aux(*args, nat.ptr(out))
+    assert rc == nat.PA_ERR_ARG
+    assert "pointer" in lib.pa_last_error().decode()
+
+
+def test_error_nan_coordinates():
+    sh = Shells([Shell(0, [np.nan, 0, 0], [1.0], [1.0])])
+    with pytest.raises(nat.PaError) as e:
+        sch.int_schwarz_aux(sh)
+    assert e.value.code == nat.PA_ERR_ARG
+
+
+def test_cholesky_solve_vs_numpy():
+    rng = np.random.default_rng(7)
+    for n in (1, 63, 64, 65, 200):
+        X = rng.normal(size=(n, n))
+        A = X @ X.T + n * np.eye(n)
+        B = rng.normal(size=(n, 5))
+        L, Y = nat.cholesky_solve(A, B)
+        Lref = np.linalg.cholesky(A)
+        np.testing.assert_allclose(np.tril(L), Lref, atol=1e-12 * np.abs(Lref).max())
+        np.testing.assert_allclose(Y, np.linalg.solve(Lref, B), atol=1e-11)
+
+
+def test_error_non_spd_metric():
+    """An indefinite matrix gives PA_ERR_NOT_SPD with the failing column (the
+    reference ignores dpotrf's info, common/linalg.f90:78)."""
+    A = np.diag([4.0, 1.0, -2.0, 3.0])
+    with pytest.raises(nat.PaError) as e:
+        nat.cholesky_solve(A, np.ones((4, 1)))
+    assert e.value.code == nat.PA_ERR_NOT_SPD
+    assert "3" in str(e.value)
