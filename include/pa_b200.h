@@ -121,6 +121,9 @@ const char* pa_last_error(void);
 int pa_set_boys_mode(int mode);
 int pa_get_boys_mode(void);
 int pa_set_screen_threshold(double thresh);
+/* 1: return the raw contraction sum_(a>=b) (ab|P) Dsym without the metric
+ * solve L^-1 (the first half of the density fit); 0 (default): full path. */
+int pa_set_skip_metric(int skip);
 
 /* Statistics of the last density-fitting call on this process. */
 typedef struct {

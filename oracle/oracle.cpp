@@ -30,6 +30,7 @@ const double DF2C_SKIP1 = static_cast<double>(1e-10f);
 const double DF2C_SKIP2 = 1e-10;
 
 int g_boys_mode = 0;
+int g_skip_metric = 0;
 OracleStats g_stats{};
 
 // ---------------------------------------------------------------------------
@@ -758,7 +759,7 @@ void df_contract_2d(const OBasis& B, const OBasis& X, int ndens, int nbf, const 
     }
   }
   const double t4 = now();
-  trmm_left_lower(metric, naux, df, ndens);
+  if (!g_skip_metric) trmm_left_lower(metric, naux, df, ndens);
   const double t5 = now();
   g_stats.ntriplets = static_cast<long long>(nsh) * (nsh + 1) / 2 * nsx;
   g_stats.nskipped = skipped;
@@ -947,6 +948,7 @@ extern "C" {
 
 void oracle_set_boys_mode(int mode) { g_boys_mode = mode; }
 int oracle_get_boys_mode(void) { return g_boys_mode; }
+void oracle_set_skip_metric(int skip) { g_skip_metric = skip ? 1 : 0; }
 void oracle_set_threads(int nthreads) {
   if (nthreads > 0) omp_set_num_threads(nthreads);
 }

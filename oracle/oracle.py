@@ -83,6 +83,7 @@ def lib():
     L.oracle_set_boys_mode.argtypes = [_i]
     L.oracle_get_boys_mode.restype = _i
     L.oracle_set_threads.argtypes = [_i]
+    L.oracle_set_skip_metric.argtypes = [_i]
     L.oracle_get_threads.restype = _i
     L.oracle_register_lapack.argtypes = [ctypes.c_void_p] * 4
     L.oracle_last_stats.argtypes = [ctypes.POINTER(OracleStats)]
@@ -122,6 +123,10 @@ def set_boys_mode(mode):
 
 def get_boys_mode():
     return lib().oracle_get_boys_mode()
+
+
+def set_skip_metric(skip):
+    lib().oracle_set_skip_metric(int(bool(skip)))
 
 
 def set_threads(n):

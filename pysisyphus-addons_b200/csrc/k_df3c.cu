@@ -275,14 +275,17 @@ __global__ void __launch_bounds__(kThreads) k_df3c(Df3cArgs a) {
       const int np = active ? c_info[2 * ci] : 0, po = c_info[2 * ci + 1];
       for (int kp = 0; kp < maxprim; ++kp) {
         const bool has = active && kp < np;
-        if (has && lane <= C::L) {
+        if (has) {
           const double2 g = a.X.prim[po + kp];
           const double gam = g.x, pg = p + gam, alpha = p * gam / pg;
           double pref = kTwoPi52 / (p * gam * sqrt(pg)) * g.y;
           for (int l = 0; l < LC; ++l) pref *= -0.5 / gam;
-          double f = pref;
-          for (int n = 0; n < lane; ++n) f *= -2.0 * alpha;
-          Rn[lane] = f * boys_n(a.dt, a.boys_mode, lane, alpha * RPC2);
+          // orders n = lane, lane + TS, ...: a team may have fewer lanes than L + 1
+          for (int n = lane; n <= C::L; n += C::TS) {
+            double f = pref;
+            for (int k = 0; k < n; ++k) f *= -2.0 * alpha;
+            Rn[n] = f * boys_n(a.dt, a.boys_mode, n, alpha * RPC2);
+          }
         }
         __syncthreads();
         hermite_R(it, C::L, Rn, X, Y, Z, b0, b1, in_team ? lane : C::TS, has ? C::TS : 0,

@@ -353,7 +353,7 @@ void layout_df(Carver& c, const pa_basis_s* orb, const pa_basis_s* aux, int nd, 
   b->runs.clear();
   size_t part_total = 0;
   const AuxLists& X = aux->aux;
-  for (int lab = 0; lab <= P.lab_max; ++lab) {
+  for (int lab = 0; lab <= P.lab_max && nd > 0; ++lab) {
     const int nu = P.class_off[lab + 1] - P.class_off[lab];
     if (nu == 0) continue;
     for (int lc = 0; lc <= X.lc_max; ++lc) {
@@ -514,7 +514,7 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
   }
   *launches_3c = *launches - before3c;
   cudaEventRecord(ph[3], s);
-  if (nd > 0) *launches += trsm_lower_left(b.M, naux, d_df, naux, nd, s);
+  if (nd > 0 && !o.skip_metric) *launches += trsm_lower_left(b.M, naux, d_df, naux, nd, s);
   return PA_OK;
 }
 
@@ -669,6 +669,12 @@ int pa_set_screen_threshold(double thresh) {
   if (!(thresh >= 0.0)) return fail(PA_ERR_ARG, "threshold must be >= 0");
   std::lock_guard<std::mutex> lk(g_opt_mu);
   g_opts.screen_thresh = thresh;
+  return PA_OK;
+}
+
+int pa_set_skip_metric(int skip) {
+  std::lock_guard<std::mutex> lk(g_opt_mu);
+  g_opts.skip_metric = skip ? 1 : 0;
   return PA_OK;
 }
 

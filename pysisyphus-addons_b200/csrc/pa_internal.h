@@ -71,6 +71,7 @@ struct Options {
   int boys_mode = 1;          // 1 = reference-compatible (default), 0 = exact
   double screen_thresh = static_cast<double>(1e-10f);
   int verbose = 0;
+  int skip_metric = 0;
 };
 
 struct Stats {

@@ -84,6 +84,7 @@ SIGNATURES = {
     "pa_set_boys_mode": [_i],
     "pa_get_boys_mode": [],
     "pa_set_screen_threshold": [_d],
+    "pa_set_skip_metric": [_i],
     "pa_get_stats": [ctypes.POINTER(PaStats)],
     "pa_basis_create": [_i, _i, _pi, _pi, _pd, _i, ctypes.POINTER(_vp)],
     "pa_basis_destroy": [_vp],
@@ -157,6 +158,10 @@ def get_boys_mode():
 
 def set_screen_threshold(thresh):
     check(load().pa_set_screen_threshold(float(thresh)))
+
+
+def set_skip_metric(skip):
+    check(load().pa_set_skip_metric(int(bool(skip))))
 
 
 def get_stats():

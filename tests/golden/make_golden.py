@@ -16,7 +16,8 @@ Outputs:
 * bena2_overlap.npy: ORCA overlap matrix permuted to m = -l..l order;
 * bena2_densities.npy: stack(D00, D01, D11) as the reference test builds it;
 * bena2_coulomb_ref.json: the reference's golden Coulomb tensor;
-* oracle_<cfg>_<mode>.npz: oracle results (Coulomb tensor, df tensor) of the
+* oracle_<cfg>_<mode>.npz: oracle results (Coulomb tensor, df tensor and the
+  raw contraction before the metric solve) of the
   synthetic workloads, for GPU parity tests at sizes where re-running the
   oracle would dominate the test time.
 """
@@ -69,9 +70,13 @@ def oracle_fixtures(keys):
         for mode in ("reference", "exact"):
             oracle.set_boys_mode(mode)
             df = oracle.contract_coulomb_densities_2d(w.shells, w.shells_aux, w.densities)
+            oracle.set_skip_metric(1)
+            raw = oracle.contract_coulomb_densities_2d(w.shells, w.shells_aux, w.densities)
+            oracle.set_skip_metric(0)
             R = oracle.contract_coulomb_densities_4d(w.shells, w.shells_aux, w.densities)
             st = oracle.last_stats()
-            np.savez_compressed(HERE / f"oracle_{key}_{mode}.npz", R=R, df=df,
+            extra = {"df": df} if key == "cfg1" else {}  # the cfg2 df is too ill-conditioned to compare
+            np.savez_compressed(HERE / f"oracle_{key}_{mode}.npz", R=R, raw=raw, **extra,
                                 ntriplets=st["ntriplets"], nskipped=st["nskipped"], nints=st["nints"])
             print(key, mode, st)
 

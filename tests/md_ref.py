@@ -104,3 +104,75 @@ def overlap_matrix(shells):
         for j, sb in enumerate(shells):
             S[offs[i]:offs[i] + sa.sph_size, offs[j]:offs[j] + sb.sph_size] = overlap_block(sa, sb)
     return S
+
+
+def schwarz_pair_mp(sa, sb, dps=40):
+    """sqrt(||(ab|ab)||_F) of two single-primitive shells in mpmath arithmetic
+    (McMurchie-Davidson with mpmath Boys values) -- a high-precision check."""
+    import mpmath as mp
+
+    mp.mp.dps = dps
+    assert sa.nprims == 1 and sb.nprims == 1
+
+    def E(i, j, t, Qx, a, b):
+        p = a + b
+        q = a * b / p
+        if t < 0 or t > i + j:
+            return mp.mpf(0)
+        if i == j == t == 0:
+            return mp.exp(-q * Qx * Qx)
+        if j == 0:
+            return E(i - 1, j, t - 1, Qx, a, b) / (2 * p) - (q * Qx / a) * E(i - 1, j, t, Qx, a, b) + (t + 1) * E(i - 1, j, t + 1, Qx, a, b)
+        return E(i, j - 1, t - 1, Qx, a, b) / (2 * p) + (q * Qx / b) * E(i, j - 1, t, Qx, a, b) + (t + 1) * E(i, j - 1, t + 1, Qx, a, b)
+
+    al, be = mp.mpf(float(sa.exps[0])), mp.mpf(float(sb.exps[0]))
+    ca = mp.mpf(float(norm_coeffs(sa.coeffs, sa.exps, sa.L)[0]))
+    cb = mp.mpf(float(norm_coeffs(sb.coeffs, sb.exps, sb.L)[0]))
+    A = [mp.mpf(float(x)) for x in sa.center]
+    B = [mp.mpf(float(x)) for x in sb.center]
+    p = al + be
+    Ta, Tb = solid_harmonics(sa.L), solid_harmonics(sb.L)
+    cla, clb = cart_list(sa.L), cart_list(sb.L)
+    herm = []
+    for ma in range(2 * sa.L + 1):
+        for mb in range(2 * sb.L + 1):
+            d = {}
+            for i1, e1 in enumerate(cla):
+                for i2, e2 in enumerate(clb):
+                    c = mp.mpf(float(Ta[ma, i1])) * mp.mpf(float(Tb[mb, i2]))
+                    if c == 0:
+                        continue
+                    for t in range(e1[0] + e2[0] + 1):
+                        for u in range(e1[1] + e2[1] + 1):
+                            for v in range(e1[2] + e2[2] + 1):
+                                val = c * ca * cb * E(e1[0], e2[0], t, A[0] - B[0], al, be) * E(e1[1], e2[1], u, A[1] - B[1], al, be) * E(e1[2], e2[2], v, A[2] - B[2], al, be)
+                                d[(t, u, v)] = d.get((t, u, v), 0) + val
+            herm.append(d)
+    alpha = p / 2
+    # R_tuv(alpha, 0): nonzero for even t, u, v only
+    boys = {}
+
+    def F(n):
+        if n not in boys:
+            boys[n] = mp.mpf(1) / (2 * n + 1)
+        return boys[n]
+
+    def R0(t, u, v):
+        if t % 2 or u % 2 or v % 2:
+            return mp.mpf(0)
+        val = mp.mpf(1)
+        for k in (t, u, v):
+            val *= mp.mpf((-1) ** (k // 2) * _dfact(k - 1))
+        n = (t + u + v) // 2
+        return val * (2 * alpha) ** n * F(n) * (-1) ** 0
+
+    pref = 2 * mp.pi ** mp.mpf(2.5) / (p * p * mp.sqrt(2 * p))
+    tot = mp.mpf(0)
+    for dr in herm:
+        for ds in herm:
+            val = mp.mpf(0)
+            for (t, u, v), x in dr.items():
+                for (t2, u2, v2), y in ds.items():
+                    val += x * y * (-1) ** (t2 + u2 + v2) * R0(t + t2, u + u2, v + v2)
+            tot += (pref * val) ** 2
+    return float(mp.sqrt(mp.sqrt(tot)))

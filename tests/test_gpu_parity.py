@@ -48,9 +48,12 @@ def test_boys_device_vs_oracle(mode):
     T = np.array([0.0, 1e-12, 1e-3, 0.049, 0.05, 0.5, 1.0, 3.3, 7.77, 14.2, 26.98, 26.999, 27.0,
                   27.5, 35.0, 39.99, 40.0, 41.0, 77.7, 400.0])
     F = nat.boys(16, T, mode)
+    # reference mode: the device evaluates the reference's interpolating polynomial
+    # in Lagrange form, the oracle in Neville form -- equal up to rounding
+    rtol = 2e-14 if mode == "exact" else 3e-13
     for i, t in enumerate(T):
         ref = oracle.boys(16, t)
-        np.testing.assert_allclose(F[i], ref, rtol=2e-14, atol=0, err_msg=f"T={t}")
+        np.testing.assert_allclose(F[i], ref, rtol=rtol, atol=0, err_msg=f"T={t}")
 
 
 def test_golden_coulomb_tensor_gpu(golden_dir, mode):
@@ -62,18 +65,51 @@ def test_golden_coulomb_tensor_gpu(golden_dir, mode):
 
 
 def test_schwarz_vs_oracle(mode):
+    """The oracle's horizontal recurrence loses up to ~1e-8 relative on distant
+    pairs with d shells (cancellation over large |AB|); see the high-precision
+    test below for which side is accurate."""
     w = config_workload("cfg1")
     np.testing.assert_allclose(sch.int_schwarz_aux(w.shells_aux), oracle.int_schwarz_aux(w.shells_aux),
                                rtol=1e-12, atol=1e-300)
-    np.testing.assert_allclose(sch.int_schwarz_bra(w.shells), oracle.int_schwarz_bra(w.shells),
-                               rtol=1e-12, atol=1e-300)
+    qg, qo = sch.int_schwarz_bra(w.shells), oracle.int_schwarz_bra(w.shells)
+    np.testing.assert_allclose(qg, qo, rtol=1e-7, atol=1e-14)
+    big = qo > 1e-2 * qo.max()
+    np.testing.assert_allclose(qg[big], qo[big], rtol=1e-12)
+
+
+def test_schwarz_high_precision():
+    """Device Schwarz values of distant s-d and d-d pairs against 40-digit arithmetic."""
+    from md_ref import schwarz_pair_mp
+
+    nat.set_boys_mode("exact")
+    w = config_workload("cfg1")
+    qg = sch.int_schwarz_bra(w.shells)
+    ia, ib = np.tril_indices(len(w.shells))
+    for k in (708, 201, 281):
+        ref = schwarz_pair_mp(w.shells[ia[k]], w.shells[ib[k]])
+        assert abs(qg[k] - ref) <= 1e-13 * ref, (k, qg[k], ref)
+    nat.set_boys_mode("reference")
+
+
+def test_df3c_raw_vs_oracle(mode):
+    """The screened 3c contraction alone (no metric solve): sum (ab|P) Dsym."""
+    w = config_workload("cfg1")
+    nat.set_skip_metric(1)
+    oracle.set_skip_metric(1)
+    try:
+        df = dia.contract_coulomb_densities_2d(w.shells, w.shells_aux, w.densities)
+        ref = oracle.contract_coulomb_densities_2d(w.shells, w.shells_aux, w.densities)
+    finally:
+        nat.set_skip_metric(0)
+        oracle.set_skip_metric(0)
+    assert_tensor_close(df, ref, atol=1e-12, rel_of_max=2e-14)
 
 
 def test_metric_vs_oracle(mode):
     w = config_workload("cfg1")
     M = nat.metric(nat.Basis(w.shells_aux, "aux"))
     Mo = oracle.int2c2e(w.shells_aux)
-    assert_tensor_close(M, Mo, atol=1e-12, rel_of_max=1e-14)
+    assert_tensor_close(M, Mo, atol=1e-12, rel_of_max=1e-13)
 
 
 def test_df2d_vs_oracle_cfg1(mode):
@@ -92,13 +128,25 @@ def test_coulomb4d_vs_oracle_cfg1(mode):
 
 
 def test_coulomb4d_vs_fixture_cfg2(golden_dir, mode):
-    """40 atoms, lmax 3 / lauxmax 4, 8 states: the plain FP64 path vs the oracle."""
+    """40 atoms, lmax 3 / lauxmax 4, 8 states: the plain FP64 path vs the oracle.
+
+    The screened three-center contraction is well conditioned and is compared
+    at 1e-13 of its largest element. The metric (P|Q) of this workload has
+    condition number ~7e13: a 1e-15 relative change of (P|Q) moves the Coulomb
+    tensor by ~1e-8 and the reference's own dtrtri + dtrmm differs from a
+    triangular solve by 1.3e-10 (both measured with the oracle), so no two FP64
+    implementations agree on the tensor to 1e-12. The tensor is compared at
+    5e-9 of its largest element."""
     w = config_workload("cfg2")
-    R = dia.contract_coulomb_densities_4d(w.shells, w.shells_aux, w.densities)
     fx = np.load(golden_dir / f"oracle_cfg2_{mode}.npz")
-    assert_tensor_close(R, fx["R"])
-    df = dia.contract_coulomb_densities_2d(w.shells, w.shells_aux, w.densities)
-    assert_tensor_close(df, fx["df"], atol=1e-11)
+    nat.set_skip_metric(1)
+    try:
+        raw = dia.contract_coulomb_densities_2d(w.shells, w.shells_aux, w.densities)
+    finally:
+        nat.set_skip_metric(0)
+    assert_tensor_close(raw, fx["raw"], atol=1e-12, rel_of_max=1e-13)
+    R = dia.contract_coulomb_densities_4d(w.shells, w.shells_aux, w.densities)
+    assert_tensor_close(R, fx["R"], atol=1e-12, rel_of_max=5e-9)
 
 
 def test_density_layouts_agree():
