@@ -23,9 +23,7 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
 import time
 from pathlib import Path
 
@@ -50,6 +48,8 @@ def parse():
     ap.add_argument("--boys", default="reference", choices=["reference", "exact"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="device steps only (for ncu): no e2e, CPU baseline, FP64 probe or clocks")
     return ap.parse_args()
 
 
@@ -74,46 +74,70 @@ def workload_config(key, w, nd):
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clock and clock-event reasons sampled every 20 ms by a thread while
+    the timed region runs (NVML reads only; nvidia-smi reports the same
+    counters). Nothing here changes a GPU setting."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
 
     def __init__(self, index):
         self.index = index
-        self.proc = None
-        self.path = None
+        self.nvml = None
+        self.thread = None
+        self.samples = []
+        self.reasons = set()
+        self.sm_max = None
+        self.error = None
 
     def start(self):
-        fd, self.path = tempfile.mkstemp(suffix=".csv")
-        os.close(fd)
+        import threading
+
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
+            import pynvml
+
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.sm_max = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            self.nvml = pynvml
+        except Exception as exc:  # no NVML: report that instead of clocks
+            self.error = f"NVML unavailable: {exc}"
+            return
+        self.stop_flag = threading.Event()
+
+        def loop():
+            nv = self.nvml
+            while not self.stop_flag.is_set():
+                try:
+                    self.samples.append(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                    active = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    for name, attr in self.REASONS:
+                        if active & getattr(nv, attr):
+                            self.reasons.add(name)
+                except Exception as exc:
+                    self.error = str(exc)
+                    return
+                self.stop_flag.wait(0.02)
+
+        self.thread = threading.Thread(target=loop, daemon=True)
+        self.thread.start()
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        self.proc.wait(timeout=10)
-        rows = [r.split(",") for r in Path(self.path).read_text().splitlines() if r.strip()]
-        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
-        smax = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = set()
-        for r in rows:
-            if len(r) < 9:
-                continue
-            for name, v in zip(names, r[5:9]):
-                if v.strip().lower() == "active":
-                    reasons.add(name)
-        os.unlink(self.path)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        if self.thread is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [self.error or "not sampled"], "samples": 0}
+        self.stop_flag.set()
+        self.thread.join(timeout=5)
+        try:
+            self.nvml.nvmlShutdown()
+        except Exception:
+            pass
+        out = {"sm_mhz": statistics.median(self.samples) if self.samples else None, "sm_max_mhz": self.sm_max,
+               "reasons": sorted(self.reasons), "samples": len(self.samples)}
+        if self.error:
+            out["error"] = self.error
+        return out
 
 
 def fp64_peak_tflops(torch):
@@ -235,6 +259,11 @@ def main():
         nat.check(lib.pa_df_4d(orb.handle, aux.handle, nd, nbf, dens.data_ptr(), nat.PA_LAYOUT_C, ns,
                                out.data_ptr(), stream.cuda_stream))
 
+    if args.profile:
+        for _ in range(args.warmup + args.steps):
+            step()
+        torch.cuda.synchronize()
+        return
     for _ in range(max(3, args.warmup)):
         step()
     torch.cuda.synchronize()
@@ -277,9 +306,12 @@ def main():
             R = dia.contract_coulomb_densities_4d(w.shells, w.shells_aux, pinned)
         torch.cuda.synchronize()
         barrier()
+        iters = []
         t0 = time.perf_counter()
         for _ in range(args.steps):
+            ti = time.perf_counter()
             R = dia.contract_coulomb_densities_4d(w.shells, w.shells_aux, pinned)
+            iters.append((time.perf_counter() - ti) * 1e3)
         torch.cuda.synchronize()
         e2e_s = (time.perf_counter() - t0) / args.steps
         if world > 1:
@@ -289,7 +321,8 @@ def main():
         keep = [a for a in w.shells.as_arrays(fortran=True)] + [a for a in w.shells_aux.as_arrays(fortran=True)]
         h2d = int(pinned.nbytes + sum(a.nbytes for a in keep))
         e2e = {"value": total_ints / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": int(R.nbytes), "ms_per_step": e2e_s * 1e3}
+               "d2h_bytes_per_step": int(R.nbytes), "ms_per_step": e2e_s * 1e3,
+               "ms_per_call": [round(x, 3) for x in iters]}
 
     if rank != 0:
         if world > 1:

@@ -175,9 +175,11 @@ int pa_count_triplets(pa_basis orbital, pa_basis aux, long long* ntriplets, long
  * arguments on the device (results copied to host), and the metric (P|Q). */
 int pa_boys_eval(int mode, int nmax, int n, const double* T, double* out);
 int pa_metric(pa_basis aux, double* metric);
-/* Host-buffer Cholesky and forward substitution on the device: A (n x n,
- * column-major) is replaced by its lower factor L, B (n x nrhs) by L^-1 B.
- * PA_ERR_NOT_SPD when A is not positive definite. */
+/* Host-buffer Cholesky solve on the device, the linear algebra of
+ * inv_chol + dtrmm (common/linalg.f90:60-82, diabatization/intor.f90:198):
+ * the lower triangle of A (n x n, column-major) is replaced by L with
+ * A = L L^T (entries above the diagonal are left as they were), and B
+ * (n x nrhs) by L^-1 B. PA_ERR_NOT_SPD when A is not positive definite. */
 int pa_cholesky_solve(int n, double* A, int nrhs, double* B);
 
 #ifdef __cplusplus

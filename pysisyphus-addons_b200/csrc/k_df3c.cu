@@ -3,31 +3,38 @@
 // contract_coulomb_densities_2d (diabatization/intor.f90:108-183).
 //
 // Formulation (McMurchie-Davidson with the density folded into the bra):
-//   df[P,m][d] += sum_tuv G_u[tuv][d] * X_(u,P)[tuv][m]
+//   df[P,m][d] += sum_tuv X_(u,P)[tuv][m] G_u[tuv][d]
 //   X_(u,P)[tuv][m] = pref(u,P) sum_(|tau|=lc) S_lc,m[tau] R_(tuv+tau)(alpha, P_u - C_P)
-// where u is a primitive pair ("bra unit") of a surviving shell pair, G_u the
-// density-folded Hermite expansion of the pair (k_bra_prep) and S the solid
-// harmonic coefficients of the auxiliary shell (Hobson's theorem: only Hermite
+// where u is a primitive pair ("bra unit") of a surviving shell pair, G_u its
+// density-folded Hermite expansion (k_bra_prep) and S the solid harmonic
+// coefficients of the auxiliary shell (Hobson's theorem: only Hermite
 // components of degree exactly lc appear on the auxiliary side).
 //
 // One kernel instance per class (LAB = la + lb, LC = l_aux). Bra units and
 // auxiliary shells are sorted by Schwarz value (descending) within their class,
-// so the surviving triples Q_ab * Q_c >= threshold form a staircase: a block
+// so the surviving triplets Q_ab * Q_c >= threshold form a staircase: a block
 // stops at the first unit failing against the largest auxiliary shell of its
-// tile, and individual triples below the threshold are skipped exactly as in
-// the reference (schwarz_estimate < 1e-10 -> cycle).
+// tile, and individual triplets below the threshold contribute exactly zero, as
+// the reference skips them (schwarz_estimate < 1e-10 -> cycle).
 //
-// A block owns a tile of TC auxiliary shells x (density chunk) and loops over a
-// chunk of bra units, UB units per step:
-//   1. stage G of the UB units into shared memory;
-//   2. build X for the UB x TC triples (Boys function, Hermite R recurrence,
-//      solid-harmonic contraction) into shared memory;
-//   3. register-tiled FP64 update acc[aux fn][d] += X^T G.
-// Each block writes its partial sums to a per-chunk slab; k_df3c_reduce sums
-// the slabs in a fixed order (deterministic results, no atomics).
+// A block (8 warps) owns a tile of TC auxiliary shells and a density chunk of
+// up to 40 columns, and walks a range of bra units, UB units per step:
+//   1. cp.async stages G of the UB units (one contiguous range) into shared
+//      memory while
+//   2. X of the UB x TC triplets is built into shared memory: the Boys function,
+//      the Hermite recurrence for R and the solid-harmonic contraction --
+//      per thread with R in registers and compile-time indices for L <= 5, by
+//      thread teams with R in shared memory above;
+//   3. the update acc[aux fn][d] += X^T G runs on the FP64 tensor cores
+//      (mma.sync m8n8k4 f64), accumulators in registers.
+// Each block writes its partial sums to a per-chunk slab; k_df3c_reduce sums the
+// slabs in a fixed order (deterministic results, no atomics).
 #include "boys.cuh"
 #include "k_df3c.cuh"
 #include "md.cuh"
+#include "sph_raw.cuh"
+
+#include <utility>
 
 namespace pa {
 
@@ -38,7 +45,17 @@ struct BlockSync {
 };
 
 constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
 constexpr int kSmemBudget = 200 * 1024 / 8;  // doubles
+constexpr int kGStride = 44;                 // shared-memory row stride of G (>= 40, = 4 mod 16)
+
+__constant__ double c_sph_dense[1024];  // solid harmonics, row (l, m) at c_sph_off[l] + m * ncart(l)
+__constant__ int c_sph_off[PA_LAUXMAX + 2];
+__constant__ double c_sph_rownorm[(PA_LAUXMAX + 1) * (PA_LAUXMAX + 1)];  // [l*l + m + l]
+
+constexpr int round_up(int x, int m) { return (x + m - 1) / m * m; }
+// row stride = 4 (mod 16) doubles: conflict-free m8n8k4 fragment loads
+constexpr int pad_stride(int mp) { return mp + ((20 - mp % 16) % 16); }
 
 template <int LAB, int LC>
 struct Cfg {
@@ -47,38 +64,73 @@ struct Cfg {
   static constexpr int NCC = ncart(LC);
   static constexpr int L = LAB + LC;
   static constexpr int NR = ncum(L);
-  static constexpr bool kPerThread = (L <= 3);
-  static constexpr int UB = NH >= 32 ? 1 : (32 / NH < 16 ? 32 / NH : 16);
-  static constexpr int smem_for(int tc, int ndc) {
-    const int mp = ((tc * NC + 15) / 16) * 16;
-    const int k = UB * NH;
-    const int ntrip = UB * tc;
-    const int team = kPerThread ? 0 : ntrip * (2 * NR + 16);
-    return k * mp + k * ndc + team + ((NC * NCC + 3) / 4) * 4 + 8 * 64;
+  static constexpr bool kPerThread = (L <= 5);
+  static constexpr int pick_ub(int tc) {
+    if (kPerThread) {
+      int ub = 64 / NH;
+      if (ub < 1) ub = 1;
+      if (ub * tc > 512) ub = 512 / tc;
+      return ub < 1 ? 1 : ub;
+    }
+    int ub = 40 / NH;
+    if (ub < 1) ub = 1;
+    if (ub * tc > 64) ub = 64 / tc;
+    return ub < 1 ? 1 : ub;
+  }
+  static constexpr int smem_for(int tc) {
+    const int ub = pick_ub(tc);
+    const int kp = round_up(ub * NH, 4);
+    const int mpad = pad_stride(round_up(tc * NC, 8));
+    const int team = kPerThread ? 0 : ub * tc * (2 * NR + 16) + 2 * NR;
+    return kp * mpad + kp * kGStride + team + 1024;
   }
   static constexpr int pick_tc() {
     int tc = 128 / NC;
-    if (tc > 64) tc = 64;
-    if (!kPerThread && UB * tc > kThreads) tc = kThreads / UB;
-    while (tc > 1 && smem_for(tc, 32) > kSmemBudget) --tc;
+    if (tc > 128) tc = 128;
+    if (!kPerThread && tc > 32) tc = 32;
+    while (tc > 1 && smem_for(tc) > kSmemBudget) --tc;
     return tc;
   }
   static constexpr int TC = pick_tc();
+  static constexpr int UB = pick_ub(TC);
   static constexpr int M = TC * NC;
-  static constexpr int MP = ((M + 15) / 16) * 16;
-  static constexpr int RM = MP / 16;
-  static constexpr int pick_ndc() {
-    int ndc = 64;
-    while (ndc > 16 && smem_for(TC, ndc) > kSmemBudget) ndc -= 16;
-    return ndc;
-  }
-  static constexpr int NDC = pick_ndc();  // max densities per block
-  static constexpr int RN = NDC / 16;
+  static constexpr int MP = round_up(M, 8);
+  static constexpr int MPAD = pad_stride(MP);
+  static constexpr int MT = MP / 8;                 // m8n8k4 row tiles
+  static constexpr int MTW = (MT + kWarps - 1) / kWarps;
   static constexpr int K = UB * NH;
+  static constexpr int KP = round_up(K, 4);
   static constexpr int NTRIP = UB * TC;
-  static constexpr int TS = kPerThread ? 1 : (kThreads / NTRIP >= 32 ? 32 : kThreads / NTRIP);
-  static constexpr int SMEM = smem_for(TC, NDC);
+  // per-thread mode: threads per triplet (power of two, warp-uniform split of t)
+  static constexpr int pick_tpt() {
+    int t = 1;
+    while (t < 8 && 2 * t * NTRIP <= kThreads) t *= 2;
+    return t;
+  }
+  static constexpr int TPT = kPerThread ? pick_tpt() : 1;
+  // team mode: team size is a power of two <= 32, so teams never straddle warps
+  static constexpr int pick_ts() {
+    int t = 1;
+    while (t < 32 && 2 * t * NTRIP <= kThreads) t *= 2;
+    return t;
+  }
+  static constexpr int TS = kPerThread ? 1 : pick_ts();
+  static constexpr int SMEM = smem_for(TC);
 };
+
+__device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src));
+}
+__device__ __forceinline__ void cp_async_commit_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::);
+}
 
 // Per-thread Hermite R (small L): in-place level recursion in registers.
 template <int L>
@@ -97,13 +149,13 @@ __device__ __forceinline__ void hermite_R_thread(const double* Rn, double X, dou
           double val;
           if (t > 0) {
             val = X * R[cidx(t - 1, u, v)];
-            if (t > 1) val += (t - 1) * R[cidx(t - 2, u, v)];
+            if (t > 1) val = fma(static_cast<double>(t - 1), R[cidx(t - 2, u, v)], val);
           } else if (u > 0) {
             val = Y * R[cidx(0, u - 1, v)];
-            if (u > 1) val += (u - 1) * R[cidx(0, u - 2, v)];
+            if (u > 1) val = fma(static_cast<double>(u - 1), R[cidx(0, u - 2, v)], val);
           } else {
             val = Z * R[cidx(0, 0, v - 1)];
-            if (v > 1) val += (v - 1) * R[cidx(0, 0, v - 2)];
+            if (v > 1) val = fma(static_cast<double>(v - 1), R[cidx(0, 0, v - 2)], val);
           }
           R[cidx(t, u, v)] = val;
         }
@@ -113,33 +165,90 @@ __device__ __forceinline__ void hermite_R_thread(const double* Rn, double X, dou
   }
 }
 
-__constant__ double c_sph_dense[1024];  // dense solid harmonics, row (l, m) at c_sph_off[l] + m * ncart(l)
-__constant__ int c_sph_off[PA_LAUXMAX + 2];
+// Decoded local Cartesian index c of degree l (x^l, x^(l-1) y, ...), compile time.
+__host__ __device__ constexpr int cart_x(int l, int c) {
+  int i = l, k = c;
+  while (k > l - i) {
+    k -= l - i + 1;
+    --i;
+  }
+  return i;
+}
+__host__ __device__ constexpr int cart_y(int l, int c) {
+  int i = l, k = c;
+  while (k > l - i) {
+    k -= l - i + 1;
+    --i;
+  }
+  return l - i - k;
+}
+
+// One solid-harmonic term w * R[t + tau] with w a compile-time constant (the
+// term vanishes at compile time when w == 0).
+template <int LC, int M, int C>
+__device__ __forceinline__ double sph_term(const double* R, int tx, int ty, int tz) {
+  constexpr int ax = cart_x(LC, C), ay = cart_y(LC, C), az = LC - ax - ay;
+  constexpr double w = sph_raw(LC, M - LC, ax, ay, az);
+  if constexpr (w != 0.0)
+    return w * R[cidx(tx + ax, ty + ay, tz + az)];
+  else
+    return -0.0;  // x + (-0.0) == x exactly, so the compiler drops the term
+}
+
+template <int LC, int M, int... Cs>
+__device__ __forceinline__ double sph_row(const double* R, int tx, int ty, int tz,
+                                          std::integer_sequence<int, Cs...>) {
+  return (-0.0 + ... + sph_term<LC, M, Cs>(R, tx, ty, tz));
+}
+
+template <int LC, int... Ms>
+__device__ __forceinline__ void sph_rows(const double* R, int tx, int ty, int tz, double* xr,
+                                         std::integer_sequence<int, Ms...>) {
+  ((xr[Ms] = fma(c_sph_rownorm[LC * LC + Ms],
+                 sph_row<LC, Ms>(R, tx, ty, tz, std::make_integer_sequence<int, ncart(LC)>{}),
+                 xr[Ms])),
+   ...);
+}
+
+// X rows of one triplet, per thread: rows t with t % TPT == part.
+template <int LAB, int LC, int TPT>
+__device__ __forceinline__ void x_rows_thread(const double* R, double* xrow0, int mpad, int part) {
+#pragma unroll
+  for (int tl = 0; tl <= LAB; ++tl)
+#pragma unroll
+    for (int tx = tl; tx >= 0; --tx)
+#pragma unroll
+      for (int ty = tl - tx; ty >= 0; --ty) {
+        const int tz = tl - tx - ty;
+        const int th = cidx(tx, ty, tz);
+        if (th % TPT != part) continue;
+        sph_rows<LC>(R, tx, ty, tz, xrow0 + th * mpad, std::make_integer_sequence<int, 2 * LC + 1>{});
+      }
+}
 
 template <int LAB, int LC>
-__global__ void __launch_bounds__(kThreads) k_df3c(Df3cArgs a) {
+__global__ void __launch_bounds__(kThreads, 1) k_df3c(Df3cArgs a) {
   using C = Cfg<LAB, LC>;
-  extern __shared__ double smem[];
-  double* Xs = smem;                    // [K][MP]
-  double* Gs = Xs + C::K * C::MP;       // [K][NDC]
-  double* Ts = Gs + C::K * C::NDC;      // [NC][NCC] solid harmonics
-  double* misc = Ts + ((C::NC * C::NCC + 3) / 4) * 4;  // unit / aux parameters (32-byte aligned)
-  double* Rteam = misc + 8 * 64;        // team scratch
-  double4* u_pP = reinterpret_cast<double4*>(misc);         // [UB]      (4 doubles each)
-  double* u_Q = misc + 4 * 16;                              // [UB]
-  double4* c_C = reinterpret_cast<double4*>(misc + 4 * 16 + 16);  // [TC] center (x,y,z,Q)
-  int* c_info = reinterpret_cast<int*>(misc + 4 * 16 + 16 + 4 * 64);  // [TC] (nprim, prim_off)
+  extern __shared__ __align__(16) double smem[];
+  double* Xs = smem;                               // [KP][MPAD]
+  double* Gs = Xs + C::KP * C::MPAD;               // [KP][kGStride]
+  double* misc = Gs + C::KP * kGStride;            // unit / aux parameters
+  double* Rteam = misc + 1024;                     // team scratch
+  double4* u_pP = reinterpret_cast<double4*>(misc);                   // [UB <= 64]
+  double* u_Q = misc + 256;                                           // [UB]
+  double4* c_C = reinterpret_cast<double4*>(misc + 320);              // [TC <= 128] (x, y, z, Q)
+  int* c_info = reinterpret_cast<int*>(misc + 320 + 512);             // [TC] (nprim, prim_off)
 
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int c0 = blockIdx.x * C::TC;
   const int tile_n = min(C::TC, a.n_aux - c0);
-  const int d0 = blockIdx.z * C::NDC;
-  const int ndc = min(C::NDC, a.nd - d0);
+  const int z = blockIdx.z;
+  const int d0 = z * a.dw;
+  const int ndc = min(a.dw, a.nd - d0);
+  const int nt_rt = a.dw / 8;  // n-tiles of this launch (dw multiple of 8, <= 40)
   const int ub = blockIdx.y * a.units_per_chunk;
   const int ue = min(a.n_units, ub + a.units_per_chunk);
 
-  // auxiliary tile
-  int maxprim = 0;
   if (tid < C::TC) {
     if (tid < tile_n) {
       const int sh = a.sorted_aux[a.aux_slot0 + c0 + tid];
@@ -154,26 +263,32 @@ __global__ void __launch_bounds__(kThreads) k_df3c(Df3cArgs a) {
       c_info[2 * tid + 1] = 0;
     }
   }
-  for (int i = tid; i < C::NC * C::NCC; i += kThreads) Ts[i] = c_sph_dense[c_sph_off[LC] + i];
   __syncthreads();
+  int maxprim = 0;
   for (int i = 0; i < tile_n; ++i) maxprim = max(maxprim, c_info[2 * i]);
   const double qc_max = tile_n > 0 ? c_C[0].w : 0.0;
-
-  double acc[C::RM][C::RN];
-#pragma unroll
-  for (int i = 0; i < C::RM; ++i)
-#pragma unroll
-    for (int j = 0; j < C::RN; ++j) acc[i][j] = 0.0;
-  const int tx = tid & 15, ty = tid >> 4;
   const double thr = a.thresh;
   const IndexTables* it = a.dt.idx;
+  const int g = lane >> 2, t4 = lane & 3;
+
+  double acc[C::MTW][5][2];
+#pragma unroll
+  for (int j = 0; j < C::MTW; ++j)
+#pragma unroll
+    for (int n = 0; n < 5; ++n) acc[j][n][0] = acc[j][n][1] = 0.0;
 
   for (int u0 = ub; u0 < ue && tile_n > 0; u0 += C::UB) {
     if (a.unit_Q[a.unit_slot0 + u0] * qc_max < thr) break;  // sorted: nothing below survives
-    __syncthreads();
+    __syncthreads();  // previous step's GEMM is done with Xs / Gs / unit data
+    // units of this step that can meet the tile (a prefix, units are sorted)
+    int nvalid = 0;
+    for (int i = 0; i < C::UB; ++i) {
+      const int s = u0 + i;
+      if (s < ue && a.unit_Q[a.unit_slot0 + s] * qc_max >= thr) nvalid = i + 1;
+    }
     if (tid < C::UB) {
       const int s = u0 + tid;
-      if (s < ue) {
+      if (tid < nvalid) {
         u_pP[tid] = a.slot_pP[a.unit_slot0 + s];
         u_Q[tid] = a.unit_Q[a.unit_slot0 + s];
       } else {
@@ -181,42 +296,46 @@ __global__ void __launch_bounds__(kThreads) k_df3c(Df3cArgs a) {
         u_Q[tid] = 0.0;
       }
     }
-    // stage G
-    for (int idx = tid; idx < C::K * C::NDC; idx += kThreads) {
-      const int k = idx / C::NDC, col = idx - k * C::NDC;
-      const int ui = k / C::NH, t = k - ui * C::NH;
-      const int s = u0 + ui;
-      double v = 0.0;
-      // Units failing against the tile's largest auxiliary shell were skipped by
-      // k_bra_prep (their G is not written) and contribute nothing here.
-      if (s < ue && col < ndc && a.unit_Q[a.unit_slot0 + s] * qc_max >= thr)
-        v = a.G[static_cast<long long>(s) * C::NH * a.nd + t * a.nd + d0 + col];
-      Gs[idx] = v;
+    // 1. G of the valid units: rows k = ui * NH + t, dw doubles each (16-byte chunks)
+    {
+      const double* gsrc = a.G + (static_cast<long long>(z) * a.n_units + u0) * C::NH * a.dw;
+      const int rows = nvalid * C::NH;
+      const int chunks_per_row = a.dw / 2;
+      for (int i = tid; i < rows * chunks_per_row; i += kThreads) {
+        const int r = i / chunks_per_row, c = i - r * chunks_per_row;
+        cp_async16(Gs + r * kGStride + 2 * c, gsrc + static_cast<long long>(r) * a.dw + 2 * c);
+      }
+      for (int i = tid; i < (C::KP - rows) * 40; i += kThreads) {
+        const int r = rows + i / 40, c = i % 40;
+        Gs[r * kGStride + c] = 0.0;
+      }
+      for (int i = tid; i < rows * (40 - a.dw); i += kThreads) {
+        const int r = i / (40 - a.dw), c = a.dw + i % (40 - a.dw);
+        Gs[r * kGStride + c] = 0.0;
+      }
     }
-    for (int idx = tid; idx < C::K * C::MP; idx += kThreads) Xs[idx] = 0.0;
+    // zero X
+    for (int i = tid; i < C::KP * C::MPAD; i += kThreads) Xs[i] = 0.0;
     __syncthreads();
 
-    // build X
+    // 2. X
     if constexpr (C::kPerThread) {
-      for (int trip = tid; trip < C::NTRIP; trip += kThreads) {
-        const int ui = trip / C::TC, ci = trip - ui * C::TC;
-        if (ci >= tile_n || u0 + ui >= ue) continue;
+      const int part = warp % C::TPT;
+      for (int tr = lane + 32 * (warp / C::TPT); tr < C::NTRIP; tr += 32 * (kWarps / C::TPT)) {
+        const int ui = tr / C::TC, ci = tr - ui * C::TC;
+        if (ci >= tile_n || ui >= nvalid) continue;
         const double4 cc = c_C[ci];
         if (u_Q[ui] * cc.w < thr) continue;
         const double4 up = u_pP[ui];
         const double p = up.x;
         const double X = up.y - cc.x, Y = up.z - cc.y, Z = up.w - cc.z;
         const double RPC2 = X * X + Y * Y + Z * Z;
-        double xacc[C::NH][C::NC];
-#pragma unroll
-        for (int t = 0; t < C::NH; ++t)
-#pragma unroll
-          for (int m = 0; m < C::NC; ++m) xacc[t][m] = 0.0;
         const int np = c_info[2 * ci], po = c_info[2 * ci + 1];
+        double* xrow0 = Xs + (ui * C::NH) * C::MPAD + ci * C::NC;
         for (int kp = 0; kp < np; ++kp) {
-          const double2 g = a.X.prim[po + kp];
-          const double gam = g.x, pg = p + gam, alpha = p * gam / pg;
-          double pref = kTwoPi52 / (p * gam * sqrt(pg)) * g.y;
+          const double2 gp = a.X.prim[po + kp];
+          const double gam = gp.x, pg = p + gam, alpha = p * gam / pg;
+          double pref = kTwoPi52 / (p * gam * sqrt(pg)) * gp.y;
 #pragma unroll
           for (int l = 0; l < LC; ++l) pref *= -0.5 / gam;  // (-1)^LC (2 gam)^-LC
           double F[C::L + 1];
@@ -230,114 +349,132 @@ __global__ void __launch_bounds__(kThreads) k_df3c(Df3cArgs a) {
           }
           double R[C::NR];
           hermite_R_thread<C::L>(Rn, X, Y, Z, R);
-#pragma unroll
-          for (int t = 0; t <= LAB; ++t)
-#pragma unroll
-            for (int tt = t; tt >= 0; --tt)
-#pragma unroll
-              for (int uu = t - tt; uu >= 0; --uu) {
-                const int vv = t - tt - uu;
-                const int th = cidx(tt, uu, vv);
-#pragma unroll
-                for (int m = 0; m < C::NC; ++m) {
-                  double s = 0.0;
-#pragma unroll
-                  for (int ta = LC; ta >= 0; --ta)
-#pragma unroll
-                    for (int ua = LC - ta; ua >= 0; --ua) {
-                      const int va = LC - ta - ua;
-                      const int cl = cidx(ta, ua, va) - ncum(LC - 1);
-                      s += Ts[m * C::NCC + cl] * R[cidx(tt + ta, uu + ua, vv + va)];
-                    }
-                  xacc[th][m] += s;
-                }
-              }
+          x_rows_thread<LAB, LC, C::TPT>(R, xrow0, C::MPAD, part);
         }
-#pragma unroll
-        for (int t = 0; t < C::NH; ++t)
-#pragma unroll
-          for (int m = 0; m < C::NC; ++m) Xs[(ui * C::NH + t) * C::MP + ci * C::NC + m] = xacc[t][m];
       }
     } else {
-      const int team = tid / C::TS, lane = tid - team * C::TS;
+      // team index tables (shared memory copies of the decoded multi-indices)
+      uchar4* txyz = reinterpret_cast<uchar4*>(Rteam + C::NTRIP * (2 * C::NR + 16));
+      // short4 needs 8-byte alignment: start after an even number of uchar4 entries
+      short4* tminus = reinterpret_cast<short4*>(txyz + round_up(C::NR, 2));
+      if (u0 == ub) {
+        for (int i = tid; i < C::NR; i += kThreads) {
+          txyz[i] = *reinterpret_cast<const uchar4*>(it->xyz[i]);
+          tminus[i] = make_short4(it->minus[i][0], it->minus[i][1], it->minus[i][2], 0);
+        }
+        __syncthreads();
+      }
+      const int team = tid / C::TS, tl = tid - team * C::TS;
       const bool in_team = team < C::NTRIP;
       const int ui = in_team ? team / C::TC : 0, ci = in_team ? team - ui * C::TC : 0;
       double* Rn = Rteam + (in_team ? team : 0) * (2 * C::NR + 16);
       double* b0 = Rn + 16;
       double* b1 = b0 + C::NR;
-      bool active = in_team && ci < tile_n && (u0 + ui) < ue;
-      double4 cc = c_C[ci];
-      active = active && (u_Q[ui] * cc.w >= thr);
+      const double4 cc = c_C[ci];
+      const bool active = in_team && ci < tile_n && ui < nvalid && (u_Q[ui] * cc.w >= thr);
       const double4 up = u_pP[ui];
       const double p = up.x;
       const double X = up.y - cc.x, Y = up.z - cc.y, Z = up.w - cc.z;
       const double RPC2 = X * X + Y * Y + Z * Z;
       const int np = active ? c_info[2 * ci] : 0, po = c_info[2 * ci + 1];
+      // Teams are warp-aligned (TS | 32): every barrier below is a warp barrier.
       for (int kp = 0; kp < maxprim; ++kp) {
         const bool has = active && kp < np;
         if (has) {
-          const double2 g = a.X.prim[po + kp];
-          const double gam = g.x, pg = p + gam, alpha = p * gam / pg;
-          double pref = kTwoPi52 / (p * gam * sqrt(pg)) * g.y;
+          const double2 gp = a.X.prim[po + kp];
+          const double gam = gp.x, pg = p + gam, alpha = p * gam / pg;
+          double pref = kTwoPi52 / (p * gam * sqrt(pg)) * gp.y;
           for (int l = 0; l < LC; ++l) pref *= -0.5 / gam;
-          // orders n = lane, lane + TS, ...: a team may have fewer lanes than L + 1
-          for (int n = lane; n <= C::L; n += C::TS) {
+          // orders n = tl, tl + TS, ...: a team may have fewer lanes than L + 1
+          for (int n = tl; n <= C::L; n += C::TS) {
             double f = pref;
             for (int k = 0; k < n; ++k) f *= -2.0 * alpha;
             Rn[n] = f * boys_n(a.dt, a.boys_mode, n, alpha * RPC2);
           }
         }
-        __syncthreads();
-        hermite_R(it, C::L, Rn, X, Y, Z, b0, b1, in_team ? lane : C::TS, has ? C::TS : 0,
-                  BlockSync());
-        if (has) {
-          for (int idx = lane; idx < C::NH * C::NC; idx += C::TS) {
-            const int t = idx / C::NC, m = idx - t * C::NC;
-            double s = 0.0;
-#pragma unroll
-            for (int cl = 0; cl < C::NCC; ++cl) {
-              const double w = Ts[m * C::NCC + cl];
-              if (w != 0.0) {
-                const uchar4 e = *reinterpret_cast<const uchar4*>(it->xyz[t]);
-                const uchar4 f = *reinterpret_cast<const uchar4*>(it->xyz[ncum(LC - 1) + cl]);
-                s = fma(w, b0[cidx(e.x + f.x, e.y + f.y, e.z + f.z)], s);
+        __syncwarp();
+        // Hermite R, level by level
+        {
+          double* top = (C::L & 1) ? b1 : b0;
+          if (has && tl == 0) top[0] = Rn[C::L];
+          __syncwarp();
+          for (int n = C::L - 1; n >= 0; --n) {
+            double* dst = (n & 1) ? b1 : b0;
+            const double* src = (n & 1) ? b0 : b1;
+            const int cnt = has ? ncum(C::L - n) : 0;
+            for (int idx = tl; idx < cnt; idx += C::TS) {
+              double v;
+              if (idx == 0) {
+                v = Rn[n];
+              } else {
+                const uchar4 e = txyz[idx];
+                const short4 mi = tminus[idx];
+                if (e.x) {
+                  v = X * src[mi.x];
+                  if (e.x > 1) v = fma(static_cast<double>(e.x - 1), src[tminus[mi.x].x], v);
+                } else if (e.y) {
+                  v = Y * src[mi.y];
+                  if (e.y > 1) v = fma(static_cast<double>(e.y - 1), src[tminus[mi.y].y], v);
+                } else {
+                  v = Z * src[mi.z];
+                  if (e.z > 1) v = fma(static_cast<double>(e.z - 1), src[tminus[mi.z].z], v);
+                }
               }
+              dst[idx] = v;
             }
-            Xs[(ui * C::NH + t) * C::MP + ci * C::NC + m] += s;
+            __syncwarp();
           }
         }
-        __syncthreads();
+        // X rows: lanes over the Hermite components t of the bra, compile-time
+        // solid-harmonic terms of the auxiliary shell
+        if (has) {
+          for (int t = tl; t < C::NH; t += C::TS) {
+            const uchar4 e = txyz[t];
+            sph_rows<LC>(b0, e.x, e.y, e.z, Xs + (ui * C::NH + t) * C::MPAD + ci * C::NC,
+                         std::make_integer_sequence<int, C::NC>{});
+          }
+        }
+        __syncwarp();
       }
     }
+    cp_async_commit_wait_all();
     __syncthreads();
 
-    // acc[row][col] += sum_k Xs[k][row] Gs[k][col]
-#pragma unroll 4
-    for (int k = 0; k < C::K; ++k) {
-      double xr[C::RM], gc[C::RN];
+    // 3. acc[aux fn][d] += X^T G on the FP64 tensor cores
+#pragma unroll 2
+    for (int k4 = 0; k4 < C::KP / 4; ++k4) {
+      const int kr = 4 * k4 + t4;
+      double bf[5];
 #pragma unroll
-      for (int i = 0; i < C::RM; ++i) xr[i] = Xs[k * C::MP + ty + 16 * i];
+      for (int n = 0; n < 5; ++n) bf[n] = n < nt_rt ? Gs[kr * kGStride + 8 * n + g] : 0.0;
 #pragma unroll
-      for (int j = 0; j < C::RN; ++j) gc[j] = Gs[k * C::NDC + tx + 16 * j];
+      for (int j = 0; j < C::MTW; ++j) {
+        const int mt = warp + kWarps * j;
+        if (mt < C::MT) {
+          const double av = Xs[kr * C::MPAD + 8 * mt + g];
 #pragma unroll
-      for (int i = 0; i < C::RM; ++i)
-#pragma unroll
-        for (int j = 0; j < C::RN; ++j) acc[i][j] = fma(xr[i], gc[j], acc[i][j]);
+          for (int n = 0; n < 5; ++n)
+            if (n < nt_rt) dmma_m8n8k4(acc[j][n][0], acc[j][n][1], av, bf[n]);
+        }
+      }
     }
   }
 
   // partial[y][fn][d]
   double* out = a.partial + static_cast<long long>(blockIdx.y) * a.n_aux * C::NC * a.nd;
 #pragma unroll
-  for (int i = 0; i < C::RM; ++i) {
-    const int row = ty + 16 * i;
-    if (row >= C::M || row / C::NC >= tile_n) continue;
+  for (int j = 0; j < C::MTW; ++j) {
+    const int mt = warp + kWarps * j;
+    const int row = 8 * mt + g;
+    if (mt >= C::MT || row >= C::M || row / C::NC >= tile_n) continue;
     const long long fn = static_cast<long long>(c0) * C::NC + row;
 #pragma unroll
-    for (int j = 0; j < C::RN; ++j) {
-      const int col = tx + 16 * j;
-      if (col < ndc) out[fn * a.nd + d0 + col] = acc[i][j];
-    }
+    for (int n = 0; n < 5; ++n)
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int col = 8 * n + 2 * t4 + i;
+        if (n < nt_rt && col < ndc) out[fn * a.nd + d0 + col] = acc[j][n][i];
+      }
   }
 }
 
@@ -369,7 +506,7 @@ int launch_class(const Df3cArgs& a, int ny, cudaStream_t s) {
   const size_t smem = sizeof(double) * C::SMEM;
   cudaFuncSetAttribute(k_df3c<LAB, LC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        static_cast<int>(smem));
-  dim3 grid((a.n_aux + C::TC - 1) / C::TC, ny, (a.nd + C::NDC - 1) / C::NDC);
+  dim3 grid((a.n_aux + C::TC - 1) / C::TC, ny, (a.nd + a.dw - 1) / a.dw);
   k_df3c<LAB, LC><<<grid, kThreads, smem, s>>>(a);
   return 1;
 }
@@ -379,25 +516,19 @@ void class_info(Df3cClassInfo* ci) {
   using C = Cfg<LAB, LC>;
   ci->tc = C::TC;
   ci->ub = C::UB;
-  ci->ndc = C::NDC;
+  ci->ndc = 40;
   ci->smem = sizeof(double) * C::SMEM;
 }
 
 using LaunchFn = int (*)(const Df3cArgs&, int, cudaStream_t);
 using InfoFn = void (*)(Df3cClassInfo*);
 
-template <int LAB, int LC>
-struct Entry {
-  static constexpr LaunchFn launch = &launch_class<LAB, LC>;
-  static constexpr InfoFn info = &class_info<LAB, LC>;
-};
-
 #define PA_ROW(LAB)                                                                    \
-  {Entry<LAB, 0>::launch, Entry<LAB, 1>::launch, Entry<LAB, 2>::launch, Entry<LAB, 3>::launch, \
-   Entry<LAB, 4>::launch, Entry<LAB, 5>::launch}
-#define PA_IROW(LAB)                                                                 \
-  {Entry<LAB, 0>::info, Entry<LAB, 1>::info, Entry<LAB, 2>::info, Entry<LAB, 3>::info, \
-   Entry<LAB, 4>::info, Entry<LAB, 5>::info}
+  {&launch_class<LAB, 0>, &launch_class<LAB, 1>, &launch_class<LAB, 2>, &launch_class<LAB, 3>, \
+   &launch_class<LAB, 4>, &launch_class<LAB, 5>}
+#define PA_IROW(LAB)                                                               \
+  {&class_info<LAB, 0>, &class_info<LAB, 1>, &class_info<LAB, 2>, &class_info<LAB, 3>, \
+   &class_info<LAB, 4>, &class_info<LAB, 5>}
 
 const LaunchFn kLaunch[2 * PA_LMAX + 1][PA_LAUXMAX + 1] = {
     PA_ROW(0), PA_ROW(1), PA_ROW(2), PA_ROW(3), PA_ROW(4), PA_ROW(5), PA_ROW(6), PA_ROW(7), PA_ROW(8)};
@@ -421,9 +552,14 @@ int launch_df3c_reduce(const Df3cReduceArgs& r, cudaStream_t s) {
   return 1;
 }
 
-cudaError_t upload_sph_dense(const double* vals, int n, const int* offs, cudaStream_t s) {
+cudaError_t upload_sph_dense(const double* vals, int n, const int* offs, const double* rownorm,
+                             cudaStream_t s) {
   cudaError_t e = cudaMemcpyToSymbolAsync(c_sph_dense, vals, sizeof(double) * n, 0,
                                           cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return e;
+  e = cudaMemcpyToSymbolAsync(c_sph_rownorm, rownorm,
+                              sizeof(double) * (PA_LAUXMAX + 1) * (PA_LAUXMAX + 1), 0,
+                              cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return e;
   return cudaMemcpyToSymbolAsync(c_sph_off, offs, sizeof(int) * (PA_LAUXMAX + 2), 0,
                                  cudaMemcpyHostToDevice, s);

@@ -16,7 +16,8 @@ struct Df3cArgs {
   int unit_slot0 = 0, n_units = 0;   // global slot offset, count
   const double* unit_Q = nullptr;    // [slot]
   const double4* slot_pP = nullptr;  // [slot] (p, P)
-  const double* G = nullptr;         // class base: [s][tuv][d]
+  const double* G = nullptr;         // class base: [z][s][tuv][dw]
+  int dw = 8;                        // density chunk width (multiple of 8, <= 40)
   int units_per_chunk = 1;
   // auxiliary shells of class LC, sorted by Schwarz value (descending)
   int aux_slot0 = 0, n_aux = 0;
@@ -44,6 +45,7 @@ struct Df3cClassInfo {
 void df3c_class_info(int lab, int lc, Df3cClassInfo* ci);
 int launch_df3c_class(int lab, int lc, const Df3cArgs& a, int ny, cudaStream_t s);
 int launch_df3c_reduce(const Df3cReduceArgs& r, cudaStream_t s);
-cudaError_t upload_sph_dense(const double* vals, int n, const int* offs, cudaStream_t s);
+cudaError_t upload_sph_dense(const double* vals, int n, const int* offs, const double* rownorm,
+                             cudaStream_t s);
 
 }  // namespace pa

@@ -318,7 +318,11 @@ __global__ void __launch_bounds__(256) k_bra_prep(DevBasis B, const int2* __rest
   }
   if (threadIdx.x == 0) a.slot_pP[slot] = U.unit_pP[u];
   const double* E = U.esph + U.unit_esph[u];
-  double* G = a.G + a.g_base + static_cast<long long>(slot - a.slot0) * NH * nd;
+  // G layout: [z][slot in class][t][dw], density d = z * dw + column, zero padded
+  const int dw = a.dw;
+  const int nz = (nd + dw - 1) / dw;
+  const long long zstride = static_cast<long long>(a.n_class) * NH * dw;
+  double* G = a.G + a.g_base + static_cast<long long>(slot - a.slot0) * NH * dw;
   for (int t0 = 0; t0 < NH; t0 += kBraTChunk) {
     const int tn = min(kBraTChunk, NH - t0);
     __syncthreads();
@@ -327,11 +331,13 @@ __global__ void __launch_bounds__(256) k_bra_prep(DevBasis B, const int2* __rest
       Es[idx] = tt < tn ? E[r * NH + t0 + tt] : 0.0;
     }
     __syncthreads();
-    for (int idx = threadIdx.x; idx < tn * nd; idx += blockDim.x) {
-      const int tt = idx / nd, d = idx - tt * nd;
+    for (int idx = threadIdx.x; idx < tn * nz * dw; idx += blockDim.x) {
+      const int tt = idx / (nz * dw), dd = idx - tt * (nz * dw);
+      const int z = dd / dw, c = dd - z * dw;
       double v = 0.0;
-      for (int r = 0; r < nab; ++r) v = fma(Ds[r * nd + d], Es[r * kBraTChunk + tt], v);
-      G[(t0 + tt) * nd + d] = v;
+      if (dd < nd)
+        for (int r = 0; r < nab; ++r) v = fma(Ds[r * nd + dd], Es[r * kBraTChunk + tt], v);
+      G[z * zstride + (t0 + tt) * dw + c] = v;
     }
   }
 }

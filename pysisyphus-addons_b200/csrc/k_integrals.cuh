@@ -16,8 +16,10 @@ struct BraPrepArgs {
   const double* dens = nullptr;           // density (d, i, j) at d*sd + i*si + j*sj
   long long sd = 0, si = 0, sj = 0;
   double4* slot_pP = nullptr;             // slot -> (p, P)
-  double* G = nullptr;                    // G blocks
+  double* G = nullptr;                    // G blocks: [z][slot in class][tuv][dw]
   long long g_base = 0;                   // offset of this class's first slot
+  int dw = 8;                             // density chunk width (multiple of 8, <= 40)
+  int n_class = 0;                        // slots in this class (stride of z)
 };
 
 size_t schwarz_bra_smem(int lab_max);

@@ -1,12 +1,15 @@
 // Dense FP64 linear algebra of the density-fitting path (column-major):
 //  * blocked right-looking Cholesky of the metric, lower triangle
-//    (replaces dpotrf("L"), common/linalg.f90:78);
-//  * blocked forward substitution B := L^-1 B, which replaces the reference's
-//    dtrtri("L","N") + dtrmm("L","L","N","N") pair (common/linalg.f90:81,
-//    diabatization/intor.f90:198) by the same product computed without
-//    forming L^-1;
-//  * a tiled FP64 GEMM C := beta C + alpha op(A) op(B) used by the trailing
-//    updates and by the Coulomb-tensor Gram matrix;
+//    (replaces dpotrf("L"), common/linalg.f90:78); each 64 x 64 diagonal block is
+//    factorized and inverted by one thread block, the panel below it is
+//    scaled in place and the trailing matrix updated by a lower GEMM;
+//  * L^-1 df as a blocked forward substitution on the density columns, using
+//    the inverted diagonal blocks (replaces dtrtri("L","N"), common/linalg.f90:81,
+//    followed by dtrmm("L","L","N","N"), diabatization/intor.f90:198: the
+//    explicit inverse is never formed);
+//  * a tiled FP64 GEMM C := beta C + alpha op(A) op(B) with optional lower
+//    triangular A, used by all of the above and by the Coulomb-tensor Gram
+//    matrix;
 //  * the 8-fold-symmetric scatter of the Coulomb tensor
 //    (diabatization/intor.f90:241-269).
 #include <algorithm>
@@ -19,112 +22,232 @@ namespace {
 
 constexpr int NB = 64;
 
-// Unblocked Cholesky of the nb x nb diagonal block at (j0, j0) in shared memory.
-__global__ void __launch_bounds__(256) k_potrf_diag(double* A, long long lda, int j0, int nb,
-                                                    int* info) {
-  __shared__ double S[NB][NB + 1];
-  for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
-    const int i = idx % nb, j = idx / nb;
-    S[i][j] = (i >= j) ? A[(j0 + i) + lda * (j0 + j)] : 0.0;
+// Factorize the nb x nb diagonal block at (j0, j0) in place (lower) and write
+// its inverse (lower, zeros above the diagonal, NB x NB) to dinv.
+// Thread (r, g) = (tid % 64, tid / 64) keeps row r, columns j = 4 q + g
+// (q = 0..15) in registers; each column / row step is two block barriers and
+// at most 16 FMAs per thread.
+__global__ void __launch_bounds__(256) k_potrf_diag_inv(double* A, long long lda, int j0, int nb,
+                                                        double* dinv, int* info) {
+  __shared__ double Ls[NB][NB + 1];  // the factor, filled column by column
+  __shared__ double diag[NB];
+  __shared__ double xrow[2][NB];
+  const int tid = threadIdx.x, r = tid & (NB - 1), g = tid >> 6;
+  double a[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const int j = 4 * q + g;
+    a[q] = (r < nb && j <= r) ? A[(j0 + r) + lda * (j0 + j)] : (r == j ? 1.0 : 0.0);
+  }
+  if (g == (r & 3)) {
+#pragma unroll
+    for (int q = 0; q < 16; ++q)
+      if (4 * q + g == r) diag[r] = a[q];
   }
   __syncthreads();
-  for (int k = 0; k < nb; ++k) {
-    if (threadIdx.x == 0) {
-      const double d = S[k][k];
-      if (!(d > 0.0)) {
-        if (*info == 0) *info = j0 + k + 1;
-        S[k][k] = 1.0;  // keep the factorization finite; the error is reported
-      } else {
-        S[k][k] = sqrt(d);
+  // Cholesky, right-looking over columns k
+  for (int k = 0; k < NB; ++k) {
+    double dkk = diag[k];
+    if (!(dkk > 0.0)) {
+      if (k < nb && tid == 0) atomicCAS(info, 0, j0 + k + 1);
+      dkk = 1.0;  // keep the factor finite; the error is reported through info
+    }
+    const double d = sqrt(dkk);
+    const int qk = k >> 2;
+    if (g == (k & 3) && r >= k) {
+      double v = 0.0;
+#pragma unroll
+      for (int q = 0; q < 16; ++q)
+        if (q == qk) v = a[q];
+      v = (r == k) ? d : v / d;
+#pragma unroll
+      for (int q = 0; q < 16; ++q)
+        if (q == qk) a[q] = v;
+      Ls[r][k] = v;
+    }
+    __syncthreads();
+    const double lik = r > k ? Ls[r][k] : 0.0;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int j = 4 * q + g;
+      if (j > k && j <= r) a[q] = fma(-lik, Ls[j][k], a[q]);
+    }
+    if (r == k + 1 && g == (r & 3)) {
+#pragma unroll
+      for (int q = 0; q < 16; ++q)
+        if (4 * q + g == r) diag[r] = a[q];
+    }
+    __syncthreads();
+  }
+  // write the factor back
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const int j = 4 * q + g;
+    if (r < nb && j <= r) A[(j0 + r) + lda * (j0 + j)] = a[q];
+  }
+  // inverse X = L^-1 by rows: X[k][:] /= L_kk, then X[i][:] -= L_ik X[k][:]
+#pragma unroll
+  for (int q = 0; q < 16; ++q) a[q] = (4 * q + g == r) ? 1.0 : 0.0;
+  for (int k = 0; k < NB; ++k) {
+    if (r == k) {
+      const double inv = 1.0 / Ls[k][k];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const int j = 4 * q + g;
+        if (j <= k) {
+          a[q] *= inv;
+          xrow[k & 1][j] = a[q];
+        }
       }
     }
     __syncthreads();
-    const double dkk = S[k][k];
-    for (int i = k + 1 + threadIdx.x; i < nb; i += blockDim.x) S[i][k] /= dkk;
-    __syncthreads();
-    const int m = nb - k - 1;
-    for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
-      const int i = k + 1 + idx % m, j = k + 1 + idx / m;
-      if (i >= j) S[i][j] -= S[i][k] * S[j][k];
+    if (r > k) {
+      const double lik = Ls[r][k];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const int j = 4 * q + g;
+        if (j <= k) a[q] = fma(-lik, xrow[k & 1][j], a[q]);
+      }
     }
-    __syncthreads();
   }
-  for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
-    const int i = idx % nb, j = idx / nb;
-    if (i >= j) A[(j0 + i) + lda * (j0 + j)] = S[i][j];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    const int j = 4 * q + g;
+    dinv[r + NB * j] = (r < nb && j <= r) ? a[q] : 0.0;
   }
 }
 
-// Panel solve: rows r in [r0, n) of columns j0..j0+nb: A[r, j0:] := A[r, j0:] L_kk^-T.
-constexpr int kPanelRows = 128;
-__global__ void __launch_bounds__(kPanelRows) k_trsm_panel(double* A, long long lda, int n, int j0,
-                                                           int nb) {
-  extern __shared__ double dsm[];
-  double(*Lk)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(dsm);
-  double(*X)[kPanelRows + 1] = reinterpret_cast<double(*)[kPanelRows + 1]>(dsm + NB * (NB + 1));
-  for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
-    const int i = idx % nb, j = idx / nb;
-    Lk[i][j] = (i >= j) ? A[(j0 + i) + lda * (j0 + j)] : 0.0;
+// Panel below the diagonal block (rows j0 + NB.., columns j0..j0 + nb):
+// P := P Dinv^T in place. One block per 64 rows; the whole row slice is read
+// into shared memory before it is overwritten.
+__global__ void __launch_bounds__(256) k_panel_inplace(double* A, long long lda, int j0, int nb,
+                                                       int rows, const double* __restrict__ dinv) {
+  extern __shared__ double psm[];
+  double(*P)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(psm);           // [row][p]
+  double(*D)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(psm + NB * (NB + 1));  // [j][p]
+  const int tid = threadIdx.x;
+  const int i0 = blockIdx.x * NB;
+  double* base = A + (j0 + nb) + lda * j0;
+#pragma unroll
+  for (int idx = tid; idx < NB * NB; idx += 256) {
+    const int i = idx & (NB - 1), p = idx >> 6;
+    P[i][p] = (i0 + i < rows && p < nb) ? base[(i0 + i) + lda * p] : 0.0;
+    D[i][p] = dinv[i + NB * p];
   }
-  const int r = j0 + nb + blockIdx.x * kPanelRows + threadIdx.x;
-  const bool ok = r < n;
-  for (int j = 0; j < nb; ++j) X[j][threadIdx.x] = ok ? A[r + lda * (j0 + j)] : 0.0;
   __syncthreads();
-  for (int j = 0; j < nb; ++j) {
-    double x = X[j][threadIdx.x];
-    for (int l = 0; l < j; ++l) x -= X[l][threadIdx.x] * Lk[j][l];
-    X[j][threadIdx.x] = x / Lk[j][j];
+  const int tx = tid & 15, ty = tid >> 4;
+  double acc[4][4] = {};
+  for (int p = 0; p < NB; ++p) {
+    double x[4], y[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      x[u] = P[tx + 16 * u][p];
+      y[u] = D[ty + 16 * u][p];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) acc[u][v] = fma(x[u], y[v], acc[u][v]);
   }
-  if (ok)
-    for (int j = 0; j < nb; ++j) A[r + lda * (j0 + j)] = X[j][threadIdx.x];
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int i = i0 + tx + 16 * u, j = ty + 16 * v;
+      if (i < rows && j < nb) base[i + lda * j] = acc[u][v];
+    }
 }
 
-// Diagonal-block forward substitution for a block of right-hand sides:
-// B[j0:j0+nb, c] := L_kk^-1 B[j0:j0+nb, c].
-constexpr int kRhsCols = 64;
-__global__ void __launch_bounds__(kRhsCols) k_trsm_diag(const double* L, long long ldl, double* B,
-                                                        long long ldb, int nrhs, int j0, int nb) {
-  extern __shared__ double dsm[];
-  double(*Lk)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(dsm);
-  double(*X)[kRhsCols + 1] = reinterpret_cast<double(*)[kRhsCols + 1]>(dsm + NB * (NB + 1));
-  for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
-    const int i = idx % nb, j = idx / nb;
-    Lk[i][j] = (i >= j) ? L[(j0 + i) + ldl * (j0 + j)] : 0.0;
+// One step k of the blocked forward substitution B := L^-1 B (right-looking).
+// Block (it, jt), it = k.., jt over 16-column tiles of B: Xk = Dinv_k B_k
+// (recomputed by every block; B_k is not written in this step); block it = k
+// stores Xk in C, the others update B_it -= L_(it,k) Xk. Thread (r, g) =
+// (tid % 64, tid / 64) owns row r, columns 4 g .. 4 g + 3 of the tile.
+constexpr int kTrsmCols = 16;
+__global__ void __launch_bounds__(256) k_trsm_step(const double* __restrict__ L, long long lda, int n,
+                                                   int k, const double* __restrict__ dinv_k,
+                                                   double* B, long long ldb, int nrhs, double* C,
+                                                   long long ldc) {
+  __shared__ double M[NB][NB + 1];            // Dinv_k, then L_(it,k)   [i][p]
+  __shared__ double Xs[NB][kTrsmCols + 1];    // B_k, then Xk            [p][c]
+  const int tid = threadIdx.x, r = tid & (NB - 1), g = tid >> 6;
+  const int it = k + blockIdx.x, c0 = blockIdx.y * kTrsmCols;
+  const int r0 = k * NB, nbk = min(NB, n - r0);
+#pragma unroll
+  for (int idx = tid; idx < NB * NB; idx += 256) {
+    const int i = idx & (NB - 1), p = idx >> 6;
+    M[i][p] = dinv_k[i + NB * p];
   }
-  const int c = blockIdx.x * kRhsCols + threadIdx.x;
-  const bool ok = c < nrhs;
-  for (int j = 0; j < nb; ++j) X[j][threadIdx.x] = ok ? B[(j0 + j) + ldb * c] : 0.0;
+#pragma unroll
+  for (int idx = tid; idx < NB * kTrsmCols; idx += 256) {
+    const int i = idx & (NB - 1), c = idx >> 6;
+    Xs[i][c] = (i < nbk && c0 + c < nrhs) ? B[(r0 + i) + ldb * (c0 + c)] : 0.0;
+  }
   __syncthreads();
-  for (int j = 0; j < nb; ++j) {
-    double x = X[j][threadIdx.x];
-    for (int l = 0; l < j; ++l) x -= Lk[j][l] * X[l][threadIdx.x];
-    X[j][threadIdx.x] = x / Lk[j][j];
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 8
+  for (int p = 0; p < NB; ++p) {
+    const double m = M[r][p];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[c] = fma(m, Xs[p][4 * g + c], acc[c]);
   }
-  if (ok)
-    for (int j = 0; j < nb; ++j) B[(j0 + j) + ldb * c] = X[j][threadIdx.x];
+  if (it == k) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int col = c0 + 4 * g + c;
+      if (r < nbk && col < nrhs) C[(r0 + r) + ldc * col] = acc[c];
+    }
+    return;
+  }
+  const int ri = it * NB, nbi = min(NB, n - ri);
+  __syncthreads();  // every thread is done with M and Xs
+#pragma unroll
+  for (int c = 0; c < 4; ++c) Xs[r][4 * g + c] = acc[c];
+#pragma unroll
+  for (int idx = tid; idx < NB * NB; idx += 256) {
+    const int i = idx & (NB - 1), p = idx >> 6;
+    M[i][p] = (i < nbi && p < nbk) ? L[(ri + i) + lda * (r0 + p)] : 0.0;
+  }
+  __syncthreads();
+  double upd[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 8
+  for (int p = 0; p < NB; ++p) {
+    const double m = M[r][p];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) upd[c] = fma(m, Xs[p][4 * g + c], upd[c]);
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const int col = c0 + 4 * g + c;
+    if (r < nbi && col < nrhs) B[(ri + r) + ldb * col] -= upd[c];
+  }
 }
 
 // C[m x n] := beta C + alpha op(A) op(B); op(A) is m x k, op(B) is k x n.
 // 64 x 64 tiles, k-steps of 16, 256 threads with 4 x 4 outputs each.
-// lower_only: skip tiles strictly above the diagonal (and entries above it).
+// lower_c: skip output tiles strictly above the diagonal (and entries above it).
+// lower_a: A (not transposed) is lower triangular; entries above its diagonal
+//          are treated as zero whatever the storage holds.
 constexpr int TM = 64, TN = 64, TK = 16;
 template <bool TA, bool TB>
 __global__ void __launch_bounds__(256) k_gemm(int m, int n, int k, double alpha,
                                               const double* __restrict__ A, long long lda,
                                               const double* __restrict__ B, long long ldb,
                                               double beta, double* C, long long ldc,
-                                              int lower_only) {
+                                              int lower_c, int lower_a) {
   const int bi = blockIdx.x, bj = blockIdx.y;
-  if (lower_only && bj > bi) return;
+  if (lower_c && bj > bi) return;
   __shared__ double As[TK][TM + 1];
   __shared__ double Bs[TK][TN + 1];
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const int i0 = bi * TM, j0 = bj * TN;
   double acc[4][4] = {};
-  for (int kk = 0; kk < k; kk += TK) {
+  // with a lower triangular A, columns k > i0 + TM - 1 contribute nothing
+  const int kend = (lower_a && !TA) ? min(k, i0 + TM) : k;
+  for (int kk = 0; kk < kend; kk += TK) {
     for (int idx = threadIdx.x; idx < TK * TM; idx += 256) {
       int r, c;  // r in tile rows (m), c in k
-      if (TA) {  // A stored k x m: op(A)(r, c) = A[c + lda * r]; read along c fastest
+      if (TA) {  // A stored k x m: op(A)(r, c) = A[c + lda * r]
         c = idx % TK;
         r = idx / TK;
       } else {
@@ -133,7 +256,7 @@ __global__ void __launch_bounds__(256) k_gemm(int m, int n, int k, double alpha,
       }
       const int gi = i0 + r, gk = kk + c;
       double v = 0.0;
-      if (gi < m && gk < k) v = TA ? A[gk + lda * gi] : A[gi + lda * gk];
+      if (gi < m && gk < k && (!lower_a || TA || gi >= gk)) v = TA ? A[gk + lda * gi] : A[gi + lda * gk];
       As[c][r] = v;
     }
     for (int idx = threadIdx.x; idx < TK * TN; idx += 256) {
@@ -170,7 +293,7 @@ __global__ void __launch_bounds__(256) k_gemm(int m, int n, int k, double alpha,
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int gi = i0 + tx + 16 * i, gj = j0 + ty + 16 * j;
-      if (gi < m && gj < n && (!lower_only || gi >= gj)) {
+      if (gi < m && gj < n && (!lower_c || gi >= gj)) {
         double* c = C + gi + ldc * gj;
         *c = (beta == 0.0 ? 0.0 : beta * *c) + alpha * acc[i][j];
       }
@@ -195,65 +318,70 @@ __global__ void k_coulomb4d(const double* __restrict__ gram, int ndens, int ns, 
   }
 }
 
+constexpr size_t kTileSmem = sizeof(double) * NB * (NB + 1);
+
+int gemm_impl(bool ta, bool tb, int m, int n, int k, double alpha, const double* A, long long lda,
+              const double* B, long long ldb, double beta, double* C, long long ldc, bool lower_c,
+              bool lower_a, cudaStream_t s) {
+  if (m <= 0 || n <= 0) return 0;
+  dim3 grid((m + TM - 1) / TM, (n + TN - 1) / TN);
+  const int lc = lower_c ? 1 : 0, la = lower_a ? 1 : 0;
+  if (!ta && !tb)
+    k_gemm<false, false><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, lc, la);
+  else if (!ta && tb)
+    k_gemm<false, true><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, lc, la);
+  else if (ta && !tb)
+    k_gemm<true, false><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, lc, la);
+  else
+    k_gemm<true, true><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, lc, la);
+  return 1;
+}
+
 }  // namespace
 
 int gemm(bool ta, bool tb, int m, int n, int k, double alpha, const double* A, long long lda,
          const double* B, long long ldb, double beta, double* C, long long ldc, bool lower_only,
          cudaStream_t s) {
-  if (m <= 0 || n <= 0) return 0;
-  dim3 grid((m + TM - 1) / TM, (n + TN - 1) / TN);
-  const int lo = lower_only ? 1 : 0;
-  if (!ta && !tb)
-    k_gemm<false, false><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, lo);
-  else if (!ta && tb)
-    k_gemm<false, true><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, lo);
-  else if (ta && !tb)
-    k_gemm<true, false><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, lo);
-  else
-    k_gemm<true, true><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, lo);
-  return 1;
+  return gemm_impl(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, lower_only, false, s);
 }
 
-constexpr size_t kPanelSmem = sizeof(double) * (NB * (NB + 1) + NB * (kPanelRows + 1));
-constexpr size_t kDiagSmem = sizeof(double) * (NB * (NB + 1) + NB * (kRhsCols + 1));
+size_t linalg_workspace_doubles(int n) {
+  const int nblk = (n + NB - 1) / NB;
+  return static_cast<size_t>(nblk) * NB * NB;
+}
 
-int cholesky_lower(double* A, int n, int* d_info, cudaStream_t s) {
+int cholesky_lower(double* A, int n, int* d_info, double* work, cudaStream_t s) {
   int launches = 0;
-  cudaFuncSetAttribute(k_trsm_panel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmem);
+  cudaFuncSetAttribute(k_panel_inplace, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(2 * kTileSmem));
   cudaMemsetAsync(d_info, 0, sizeof(int), s);
-  for (int j0 = 0; j0 < n; j0 += NB) {
-    const int nb = std::min(NB, n - j0);
-    k_potrf_diag<<<1, 256, 0, s>>>(A, n, j0, nb, d_info);
+  const int nblk = (n + NB - 1) / NB;
+  // per block column: diagonal factor + inverse, panel P := P L_kk^-T, A22 -= P P^T
+  for (int b = 0; b < nblk; ++b) {
+    const int j0 = b * NB, nb = std::min(NB, n - j0);
+    double* Db = work + static_cast<size_t>(b) * NB * NB;
+    k_potrf_diag_inv<<<1, 256, 0, s>>>(A, n, j0, nb, Db, d_info);
     ++launches;
     const int rest = n - j0 - nb;
     if (rest > 0) {
-      k_trsm_panel<<<(rest + kPanelRows - 1) / kPanelRows, kPanelRows, kPanelSmem, s>>>(A, n, n, j0, nb);
-      ++launches;
-      // trailing lower update: A22 -= P P^T
+      k_panel_inplace<<<(rest + NB - 1) / NB, 256, 2 * kTileSmem, s>>>(A, n, j0, nb, rest, Db);
       double* P = A + (j0 + nb) + static_cast<long long>(n) * j0;
       double* A22 = A + (j0 + nb) + static_cast<long long>(n) * (j0 + nb);
-      launches += gemm(false, true, rest, rest, nb, -1.0, P, n, P, n, 1.0, A22, n, true, s);
+      launches += 1 + gemm_impl(false, true, rest, rest, nb, -1.0, P, n, P, n, 1.0, A22, n, true,
+                                false, s);
     }
   }
   return launches;
 }
 
-int trsm_lower_left(const double* L, int n, double* B, long long ldb, int nrhs, cudaStream_t s) {
-  int launches = 0;
-  if (nrhs <= 0) return 0;
-  cudaFuncSetAttribute(k_trsm_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDiagSmem);
-  for (int j0 = 0; j0 < n; j0 += NB) {
-    const int nb = std::min(NB, n - j0);
-    k_trsm_diag<<<(nrhs + kRhsCols - 1) / kRhsCols, kRhsCols, kDiagSmem, s>>>(L, n, B, ldb, nrhs, j0, nb);
-    ++launches;
-    const int rest = n - j0 - nb;
-    if (rest > 0) {
-      const double* Lp = L + (j0 + nb) + static_cast<long long>(n) * j0;
-      launches += gemm(false, false, rest, nrhs, nb, -1.0, Lp, n, B + j0, ldb, 1.0,
-                       B + j0 + nb, ldb, false, s);
-    }
-  }
-  return launches;
+int trsm_lower_left(const double* L, int n, const double* dinv, double* B, long long ldb, int nrhs,
+                    double* C, long long ldc, cudaStream_t s) {
+  if (n <= 0 || nrhs <= 0) return 0;
+  const int nblk = (n + NB - 1) / NB, ct = (nrhs + kTrsmCols - 1) / kTrsmCols;
+  for (int k = 0; k < nblk; ++k)
+    k_trsm_step<<<dim3(nblk - k, ct), 256, 0, s>>>(L, n, n, k, dinv + static_cast<size_t>(k) * NB * NB, B,
+                                                   ldb, nrhs, C, ldc);
+  return nblk;
 }
 
 int coulomb_4d(const double* df, int naux, int ndens, int nstates, double* gram_scratch,

@@ -3,17 +3,25 @@
 
 #include <cuda_runtime.h>
 
+#include <cstddef>
+
 namespace pa {
 
 // Column-major C := beta C + alpha op(A) op(B). Returns the number of launches.
 int gemm(bool ta, bool tb, int m, int n, int k, double alpha, const double* A, long long lda,
          const double* B, long long ldb, double beta, double* C, long long ldc, bool lower_only,
          cudaStream_t s);
-// In-place lower Cholesky factor of the n x n matrix A (lda = n). *d_info
+// Doubles of scratch cholesky_lower needs for an n x n matrix (the inverted
+// 64 x 64 diagonal blocks, kept for trsm_lower_left).
+size_t linalg_workspace_doubles(int n);
+// In place: the lower triangle of A (n x n, lda = n) becomes L with A = L L^T
+// (dpotrf); work receives the inverses of L's diagonal blocks. *d_info
 // (device) receives 0 or the 1-based column of the first non-positive pivot.
-int cholesky_lower(double* A, int n, int* d_info, cudaStream_t s);
-// B := L^-1 B for the lower factor L (n x n, ldl = n) and nrhs columns of B.
-int trsm_lower_left(const double* L, int n, double* B, long long ldb, int nrhs, cudaStream_t s);
+int cholesky_lower(double* A, int n, int* d_info, double* work, cudaStream_t s);
+// C := L^-1 B (n x nrhs) for the factor and work of cholesky_lower. B is
+// overwritten (used as scratch).
+int trsm_lower_left(const double* L, int n, const double* dinv, double* B, long long ldb, int nrhs,
+                    double* C, long long ldc, cudaStream_t s);
 // Coulomb tensor R[ns,ns,ns,ns] (column-major) from df[naux, ndens].
 int coulomb_4d(const double* df, int naux, int ndens, int nstates, double* gram_scratch,
                double* R, cudaStream_t s);

@@ -203,6 +203,11 @@ struct pa_basis_s {
   pa::AuxLists aux;
   char* dmem = nullptr;
   pa::DevBasis dev;
+  // Shell-pair lists: built on the first use as an orbital basis (an
+  // auxiliary basis never needs them).
+  std::mutex pair_mu;
+  bool pairs_ready = false;
+  char* dpair = nullptr;
   int2* d_pair_ab = nullptr;
   int* d_pair_unit0 = nullptr;
   int* d_unit_pair = nullptr;
@@ -222,8 +227,15 @@ struct Ctx {
   Arena arena;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  cudaEvent_t ph[5] = {};  // phase boundaries: screen | bra | metric | 3c | solve
+  cudaEvent_t ph[5] = {};  // phase boundaries on the main stream: screen | bra | 3c | solve
+  cudaStream_t stream2 = nullptr;     // metric + Cholesky + inverse, overlapped with the 3c work
+  cudaEvent_t fork = nullptr, m0 = nullptr, m1 = nullptr;
   int* h_info = nullptr;  // pinned
+  // Stream-ordered pool of the host-buffer entry points (densities, df, R).
+  // Freed blocks stay mapped in this private pool, so repeated calls of the
+  // same size do not map device memory again; the device's default pool and
+  // other allocators in the process are untouched.
+  cudaMemPool_t pool = nullptr;
 };
 
 std::mutex g_ctx_mu;
@@ -244,7 +256,23 @@ int current_ctx(Ctx** out, DeviceTables* dt) {
     PA_CUDA(cudaEventCreate(&c->ev0));
     PA_CUDA(cudaEventCreate(&c->ev1));
     for (auto& e : c->ph) PA_CUDA(cudaEventCreate(&e));
+    // The metric + Cholesky chain is a long sequence of small dependent
+    // launches; at the highest priority each of its blocks takes the next SM
+    // that a 3c block frees instead of queueing behind the whole 3c grid.
+    int prio_lo = 0, prio_hi = 0;
+    PA_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    PA_CUDA(cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, prio_hi));
+    PA_CUDA(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
+    PA_CUDA(cudaEventCreate(&c->m0));
+    PA_CUDA(cudaEventCreate(&c->m1));
     PA_CUDA(cudaMallocHost(&c->h_info, sizeof(int) * 4));
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    PA_CUDA(cudaMemPoolCreate(&c->pool, &props));
+    unsigned long long keep = ~0ull;
+    PA_CUDA(cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep));
     g_ctx[dev] = c;
   }
   *out = g_ctx[dev];
@@ -292,12 +320,14 @@ __global__ void k_boys_eval(DeviceTables dt, int mode, int nmax, int n, const do
 
 // Buffers of one density-fitting run.
 struct DfBuffers {
-  double *Qab, *Qc, *qmax, *esph, *ukeys, *slot_Q, *akeys, *aux_Q, *G, *M, *partial;
+  double *Qab, *Qc, *qmax, *esph, *ukeys, *slot_Q, *akeys, *aux_Q, *G, *M, *partial, *lawork,
+      *df_raw;
   double4 *unit_pP, *slot_pP;
   int *uvals, *sorted_unit, *avals, *sorted_aux, *info;
   void* cub_tmp;
   size_t cub_bytes;
   std::vector<long long> g_off;      // per Lab class
+  int dw = 8;                        // density chunk width of G (multiple of 8, <= 40)
   struct ClassRun {
     int lab, lc, ny, upc;
     double* partial;
@@ -340,13 +370,17 @@ void layout_df(Carver& c, const pa_basis_s* orb, const pa_basis_s* aux, int nd, 
   b->aux_Q = c.take<double>(nx);
   b->sorted_aux = c.take<int>(nx);
   b->info = c.take<int>(4);
+  b->dw = std::min(40, std::max(8, (nd + 7) / 8 * 8));
+  const int nz = nd > 0 ? (nd + b->dw - 1) / b->dw : 0;
   b->g_off.assign(P.lab_max + 2, 0);
   for (int lab = 0; lab <= P.lab_max; ++lab) {
     const long long nu = P.class_off[lab + 1] - P.class_off[lab];
-    b->g_off[lab + 1] = b->g_off[lab] + nu * ncum(lab) * nd;
+    b->g_off[lab + 1] = b->g_off[lab] + nu * ncum(lab) * nz * b->dw;
   }
   b->G = c.take<double>(b->g_off[P.lab_max + 1]);
   b->M = c.take<double>(naux * naux);
+  b->lawork = c.take<double>(linalg_workspace_doubles(static_cast<int>(naux)));
+  b->df_raw = c.take<double>(static_cast<size_t>(naux) * nd);
   b->cub_bytes = cub_temp_bytes(orb, aux);
   b->cub_tmp = c.take<char>(b->cub_bytes);
   // partial slabs
@@ -362,8 +396,8 @@ void layout_df(Carver& c, const pa_basis_s* orb, const pa_basis_s* aux, int nd, 
       Df3cClassInfo ci;
       df3c_class_info(lab, lc, &ci);
       const int bx = (nxc + ci.tc - 1) / ci.tc;
-      const int bz = (nd + ci.ndc - 1) / ci.ndc;
-      const int target = 4 * 148;
+      const int bz = nz;
+      const int target = 2 * 148;
       int ny = std::max(1, (target + bx * bz - 1) / (bx * bz));
       const int max_ny = (nu + ci.ub - 1) / ci.ub;
       ny = std::min(ny, max_ny);
@@ -435,10 +469,20 @@ int run_screening(const pa_basis_s* orb, const pa_basis_s* aux, const DeviceTabl
 int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d_dens,
            long long sd, long long si, long long sj, double* d_df, DfBuffers& b,
            const DeviceTables& dt, const Options& o, cudaStream_t s, int* launches,
-           cudaEvent_t* ph, int* launches_3c) {
+           Ctx* ctx, int* launches_3c) {
   const PairLists& P = orb->pairs;
   const AuxLists& X = aux->aux;
   const int naux = aux->host.nsph;
+  cudaEvent_t* ph = ctx->ph;
+  // metric (P|Q), its Cholesky factor and L^-1 on the second stream: independent
+  // of everything until the final L^-1 df
+  cudaStream_t s2 = ctx->stream2;
+  cudaEventRecord(ctx->fork, s);
+  cudaStreamWaitEvent(s2, ctx->fork, 0);
+  cudaEventRecord(ctx->m0, s2);
+  *launches += launch_metric(aux->dev, dt, o.boys_mode, b.M, s2);
+  *launches += cholesky_lower(b.M, naux, b.info, b.lawork, s2);
+  cudaEventRecord(ctx->m1, s2);
   int st = run_screening(orb, aux, dt, o, b, s, launches);
   if (st != PA_OK) return st;
   cudaEventRecord(ph[0], s);
@@ -461,13 +505,11 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
     a.slot_pP = b.slot_pP;
     a.G = b.G;
     a.g_base = b.g_off[lab];
+    a.dw = b.dw;
+    a.n_class = a.slot_end - a.slot0;
     *launches += launch_bra_prep(orb->dev, orb->d_pair_ab, U, a, lab, s);
   }
   cudaEventRecord(ph[1], s);
-  // metric and its Cholesky factor
-  *launches += launch_metric(aux->dev, dt, o.boys_mode, b.M, s);
-  *launches += cholesky_lower(b.M, naux, b.info, s);
-  cudaEventRecord(ph[2], s);
   // three-center contraction
   const int before3c = *launches;
   if (nd > 0) {
@@ -482,6 +524,7 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
       a.unit_Q = b.slot_Q;
       a.slot_pP = b.slot_pP;
       a.G = b.G + b.g_off[r.lab];
+      a.dw = b.dw;
       a.units_per_chunk = r.upc;
       a.aux_slot0 = X.class_off[r.lc];
       a.n_aux = X.class_off[r.lc + 1] - X.class_off[r.lc];
@@ -508,13 +551,19 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
           ra.ny[ra.nclasses] = r.ny;
           ++ra.nclasses;
         }
-      ra.df = d_df;
+      ra.df = b.df_raw;
       *launches += launch_df3c_reduce(ra, s);
     }
   }
   *launches_3c = *launches - before3c;
-  cudaEventRecord(ph[3], s);
-  if (nd > 0 && !o.skip_metric) *launches += trsm_lower_left(b.M, naux, d_df, naux, nd, s);
+  cudaEventRecord(ph[2], s);
+  cudaStreamWaitEvent(s, ctx->m1, 0);  // join the metric stream
+  if (nd > 0) {
+    if (o.skip_metric)
+      cudaMemcpyAsync(d_df, b.df_raw, sizeof(double) * naux * nd, cudaMemcpyDeviceToDevice, s);
+    else
+      *launches += trsm_lower_left(b.M, naux, b.lawork, b.df_raw, naux, nd, d_df, naux, s);
+  }
   return PA_OK;
 }
 
@@ -526,8 +575,10 @@ int finish(Ctx* c, const DfBuffers& b, cudaStream_t s, int launches, float* ms) 
   PA_CUDA(cudaEventElapsedTime(ms, c->ev0, c->ev1));
   float t[5];
   PA_CUDA(cudaEventElapsedTime(&t[0], c->ev0, c->ph[0]));
-  for (int i = 1; i < 4; ++i) PA_CUDA(cudaEventElapsedTime(&t[i], c->ph[i - 1], c->ph[i]));
-  PA_CUDA(cudaEventElapsedTime(&t[4], c->ph[3], c->ev1));
+  PA_CUDA(cudaEventElapsedTime(&t[1], c->ph[0], c->ph[1]));
+  PA_CUDA(cudaEventElapsedTime(&t[2], c->m0, c->m1));  // concurrent with screening..3c
+  PA_CUDA(cudaEventElapsedTime(&t[3], c->ph[1], c->ph[2]));
+  PA_CUDA(cudaEventElapsedTime(&t[4], c->ph[2], c->ev1));
   g_stats.ms_screen = t[0];
   g_stats.ms_bra = t[1];
   g_stats.ms_metric = t[2];
@@ -541,13 +592,60 @@ int finish(Ctx* c, const DfBuffers& b, cudaStream_t s, int launches, float* ms) 
   return PA_OK;
 }
 
+// Builds and uploads the shell-pair / primitive-pair lists of an orbital basis
+// once; later calls return at once.
+int ensure_pairs(pa_basis b) {
+  std::lock_guard<std::mutex> lk(b->pair_mu);
+  if (b->pairs_ready) return PA_OK;
+  if (b->host.lmax > PA_LMAX) return fail(PA_ERR_LMAX, "orbital basis L above the compiled maximum");
+  PairLists P;
+  build_pair_lists(b->host, &P);
+  Carver cnt;
+  char* dpair = nullptr;
+  for (int pass = 0; pass < 2; ++pass) {
+    if (pass == 1) {
+      if (cudaMalloc(&dpair, std::max<size_t>(cnt.used, 256)) != cudaSuccess)
+        return fail(PA_ERR_CUDA, "cudaMalloc(pair lists) failed");
+      cnt = Carver();
+      cnt.base = dpair;
+    }
+    b->d_pair_ab = cnt.take<int2>(P.pair_ab.size());
+    b->d_pair_unit0 = cnt.take<int>(P.pair_unit0.size());
+    b->d_unit_pair = cnt.take<int>(P.unit_pair.size());
+    b->d_unit_prims = cnt.take<int2>(P.unit_prims.size());
+    b->d_unit_esph = cnt.take<long long>(P.unit_esph.size());
+    b->d_class_unit = cnt.take<int>(P.class_unit.size());
+    b->d_class_off = cnt.take<int>(P.class_off.size());
+  }
+  std::vector<char> stage(cnt.used);
+  auto put = [&](const void* dst, const void* src, size_t bytes) {
+    if (bytes) std::memcpy(stage.data() + (static_cast<const char*>(dst) - dpair), src, bytes);
+  };
+  put(b->d_pair_ab, P.pair_ab.data(), sizeof(int2) * P.pair_ab.size());
+  put(b->d_pair_unit0, P.pair_unit0.data(), sizeof(int) * P.pair_unit0.size());
+  put(b->d_unit_pair, P.unit_pair.data(), sizeof(int) * P.unit_pair.size());
+  put(b->d_unit_prims, P.unit_prims.data(), sizeof(int2) * P.unit_prims.size());
+  put(b->d_unit_esph, P.unit_esph.data(), sizeof(long long) * P.unit_esph.size());
+  put(b->d_class_unit, P.class_unit.data(), sizeof(int) * P.class_unit.size());
+  put(b->d_class_off, P.class_off.data(), sizeof(int) * P.class_off.size());
+  const cudaError_t e = cudaMemcpy(dpair, stage.data(), cnt.used, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(dpair);
+    return fail(PA_ERR_CUDA, std::string("pair-list upload: ") + cudaGetErrorString(e));
+  }
+  b->pairs = std::move(P);
+  b->dpair = dpair;
+  b->pairs_ready = true;
+  return PA_OK;
+}
+
 int check_pair(pa_basis orb, pa_basis aux) {
   if (!orb || !aux) return fail(PA_ERR_ARG, "null basis handle");
   int dev = 0;
   cudaGetDevice(&dev);
   if (orb->device != dev || aux->device != dev)
     return fail(PA_ERR_ARG, "basis handle belongs to another device");
-  return PA_OK;
+  return ensure_pairs(orb);
 }
 
 int df_device(pa_basis orb, pa_basis aux, int ndens, int nbf, const double* d_dens, int layout,
@@ -588,7 +686,7 @@ int df_device(pa_basis orb, pa_basis aux, int ndens, int nbf, const double* d_de
   }
   PA_CUDA(cudaEventRecord(c->ev0, s));
   int launches = 0, launches_3c = 0;
-  st = run_df(orb, aux, ndens, d_dens, sd, si, sj, d_df, b, dt, o, s, &launches, c->ph, &launches_3c);
+  st = run_df(orb, aux, ndens, d_dens, sd, si, sj, d_df, b, dt, o, s, &launches, c, &launches_3c);
   if (st != PA_OK) return st;
   g_stats.launches_3c = launches_3c;
   if (d_R) launches += coulomb_4d(d_df, aux->host.nsph, ndens, nstates, gram, d_R, s);
@@ -617,9 +715,9 @@ int df_host(pa_basis orb, pa_basis aux, int ndens, int nbf, const double* dens, 
   const size_t df_count = static_cast<size_t>(aux->host.nsph) * ndens;
   const size_t out_count = nstates > 0 ? static_cast<size_t>(nstates) * nstates * nstates * nstates : df_count;
   double *d_dens = nullptr, *d_df = nullptr, *d_R = nullptr;
-  PA_CUDA(cudaMallocAsync(&d_dens, std::max<size_t>(nd_bytes, 8), c->stream));
-  PA_CUDA(cudaMallocAsync(&d_df, sizeof(double) * std::max<size_t>(df_count, 1), c->stream));
-  if (nstates > 0) PA_CUDA(cudaMallocAsync(&d_R, sizeof(double) * out_count, c->stream));
+  PA_CUDA(cudaMallocFromPoolAsync(&d_dens, std::max<size_t>(nd_bytes, 8), c->pool, c->stream));
+  PA_CUDA(cudaMallocFromPoolAsync(&d_df, sizeof(double) * std::max<size_t>(df_count, 1), c->pool, c->stream));
+  if (nstates > 0) PA_CUDA(cudaMallocFromPoolAsync(&d_R, sizeof(double) * out_count, c->pool, c->stream));
   if (nd_bytes) PA_CUDA(cudaMemcpyAsync(d_dens, dens, nd_bytes, cudaMemcpyHostToDevice, c->stream));
   st = df_device(orb, aux, ndens, nbf, d_dens, layout, d_df, nstates, d_R, c->stream);
   if (st == PA_OK) {
@@ -708,10 +806,8 @@ int pa_basis_create(int nshells, int ndata, const int* bas_centers, const int* b
     delete b;
     return fail(st, err);
   }
-  if (b->host.lmax <= PA_LMAX) build_pair_lists(b->host, &b->pairs);
   build_aux_lists(b->host, &b->aux);
   const HostBasis& h = b->host;
-  const PairLists& P = b->pairs;
   const int ns = static_cast<int>(h.shells.size());
   Carver cnt;
   for (int pass = 0; pass < 2; ++pass) {
@@ -727,13 +823,6 @@ int pa_basis_create(int nshells, int ndata, const int* bas_centers, const int* b
     b->dev.shell = cv.take<int4>(ns);
     b->dev.center = cv.take<double4>(ns);
     b->dev.prim = cv.take<double2>(h.exps.size());
-    b->d_pair_ab = cv.take<int2>(P.pair_ab.size());
-    b->d_pair_unit0 = cv.take<int>(P.pair_unit0.size());
-    b->d_unit_pair = cv.take<int>(P.unit_pair.size());
-    b->d_unit_prims = cv.take<int2>(P.unit_prims.size());
-    b->d_unit_esph = cv.take<long long>(P.unit_esph.size());
-    b->d_class_unit = cv.take<int>(P.class_unit.size());
-    b->d_class_off = cv.take<int>(P.class_off.size());
     b->d_aux_shell = cv.take<int>(b->aux.class_shell.size());
     b->d_aux_off = cv.take<int>(b->aux.class_off.size());
   }
@@ -746,22 +835,17 @@ int pa_basis_create(int nshells, int ndata, const int* bas_centers, const int* b
   }
   std::vector<double2> prim(h.exps.size());
   for (size_t k = 0; k < prim.size(); ++k) prim[k] = make_double2(h.exps[k], h.coefs[k]);
-  auto up = [&](void* dst, const void* src, size_t bytes) {
-    return bytes ? cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
+  // one host image of the carved block, one copy
+  std::vector<char> stage(cnt.used);
+  auto put = [&](const void* dst, const void* src, size_t bytes) {
+    if (bytes) std::memcpy(stage.data() + (static_cast<const char*>(dst) - b->dmem), src, bytes);
   };
-  cudaError_t e = cudaSuccess;
-  if (e == cudaSuccess) e = up(b->dev.shell, shell.data(), sizeof(int4) * ns);
-  if (e == cudaSuccess) e = up(b->dev.center, center.data(), sizeof(double4) * ns);
-  if (e == cudaSuccess) e = up(b->dev.prim, prim.data(), sizeof(double2) * prim.size());
-  if (e == cudaSuccess) e = up(b->d_pair_ab, P.pair_ab.data(), sizeof(int2) * P.pair_ab.size());
-  if (e == cudaSuccess) e = up(b->d_pair_unit0, P.pair_unit0.data(), sizeof(int) * P.pair_unit0.size());
-  if (e == cudaSuccess) e = up(b->d_unit_pair, P.unit_pair.data(), sizeof(int) * P.unit_pair.size());
-  if (e == cudaSuccess) e = up(b->d_unit_prims, P.unit_prims.data(), sizeof(int2) * P.unit_prims.size());
-  if (e == cudaSuccess) e = up(b->d_unit_esph, P.unit_esph.data(), sizeof(long long) * P.unit_esph.size());
-  if (e == cudaSuccess) e = up(b->d_class_unit, P.class_unit.data(), sizeof(int) * P.class_unit.size());
-  if (e == cudaSuccess) e = up(b->d_class_off, P.class_off.data(), sizeof(int) * P.class_off.size());
-  if (e == cudaSuccess) e = up(b->d_aux_shell, b->aux.class_shell.data(), sizeof(int) * b->aux.class_shell.size());
-  if (e == cudaSuccess) e = up(b->d_aux_off, b->aux.class_off.data(), sizeof(int) * b->aux.class_off.size());
+  put(b->dev.shell, shell.data(), sizeof(int4) * ns);
+  put(b->dev.center, center.data(), sizeof(double4) * ns);
+  put(b->dev.prim, prim.data(), sizeof(double2) * prim.size());
+  put(b->d_aux_shell, b->aux.class_shell.data(), sizeof(int) * b->aux.class_shell.size());
+  put(b->d_aux_off, b->aux.class_off.data(), sizeof(int) * b->aux.class_off.size());
+  const cudaError_t e = cnt.used ? cudaMemcpy(b->dmem, stage.data(), cnt.used, cudaMemcpyHostToDevice) : cudaSuccess;
   if (e != cudaSuccess) {
     cudaFree(b->dmem);
     delete b;
@@ -778,6 +862,7 @@ int pa_basis_create(int nshells, int ndata, const int* bas_centers, const int* b
 int pa_basis_destroy(pa_basis basis) {
   if (!basis) return PA_OK;
   if (basis->dmem) cudaFree(basis->dmem);
+  if (basis->dpair) cudaFree(basis->dpair);
   delete basis;
   return PA_OK;
 }
@@ -809,7 +894,7 @@ int pa_df_4d(pa_basis orbital, pa_basis aux, int ndens, int nbf, const double* d
   if (st != PA_OK) return st;
   double* d_df = nullptr;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  PA_CUDA(cudaMallocAsync(&d_df, sizeof(double) * std::max<size_t>(1, static_cast<size_t>(aux ? aux->host.nsph : 0) * ndens), s));
+  PA_CUDA(cudaMallocFromPoolAsync(&d_df, sizeof(double) * std::max<size_t>(1, static_cast<size_t>(aux ? aux->host.nsph : 0) * ndens), c->pool, s));
   st = df_device(orbital, aux, ndens, nbf, d_densities, layout, d_df, nstates, d_coulomb, s);
   cudaFreeAsync(d_df, s);
   return st;
@@ -874,6 +959,8 @@ static int schwarz_impl(pa_basis orb, pa_basis aux, double* q_bra, double* q_aux
   cudaStream_t s = c->stream;
   int launches = 0;
   if (orb) {
+    const int pst = ensure_pairs(orb);
+    if (pst != PA_OK) return pst;
     const PairLists& P = orb->pairs;
     Carver cnt;
     double* Qab = cnt.take<double>(P.npairs);
@@ -1001,10 +1088,17 @@ int pa_metric(pa_basis aux, double* metric) {
   const size_t n = aux->host.nsph;
   PA_CUDA(c->arena.reserve(sizeof(double) * n * n + 256));
   double* M = reinterpret_cast<double*>(c->arena.base);
-  launch_metric(aux->dev, dt, options().boys_mode, M, c->stream);
+  PA_CUDA(cudaEventRecord(c->ev0, c->stream));
+  const int launches = launch_metric(aux->dev, dt, options().boys_mode, M, c->stream);
   PA_CUDA(cudaGetLastError());
+  PA_CUDA(cudaEventRecord(c->ev1, c->stream));
   PA_CUDA(cudaMemcpyAsync(metric, M, sizeof(double) * n * n, cudaMemcpyDeviceToHost, c->stream));
   PA_CUDA(cudaStreamSynchronize(c->stream));
+  float ms = 0.f;
+  PA_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  g_stats = pa_stats{};
+  g_stats.ms_metric = g_stats.ms_total = ms;
+  g_stats.kernel_launches = launches;
   return PA_OK;
 }
 
@@ -1017,7 +1111,7 @@ int pa_cholesky_solve(int n, double* A, int nrhs, double* B) {
   if (st != PA_OK) return st;
   std::lock_guard<std::mutex> lk(c->mu);
   const size_t nn = static_cast<size_t>(n) * n, nb = static_cast<size_t>(n) * nrhs;
-  PA_CUDA(c->arena.reserve(sizeof(double) * (nn + nb) + 1024));
+  PA_CUDA(c->arena.reserve(sizeof(double) * (nn + 2 * nb + linalg_workspace_doubles(n)) + 4096));
   Carver cv;
   cv.base = c->arena.base;
   double* dA = cv.take<double>(nn);
@@ -1026,13 +1120,22 @@ int pa_cholesky_solve(int n, double* A, int nrhs, double* B) {
   if (n == 0) return PA_OK;
   PA_CUDA(cudaMemcpyAsync(dA, A, sizeof(double) * nn, cudaMemcpyHostToDevice, c->stream));
   if (nb) PA_CUDA(cudaMemcpyAsync(dB, B, sizeof(double) * nb, cudaMemcpyHostToDevice, c->stream));
-  cholesky_lower(dA, n, info, c->stream);
-  if (nb) trsm_lower_left(dA, n, dB, n, nrhs, c->stream);
+  double* work = cv.take<double>(linalg_workspace_doubles(n));
+  double* dC = cv.take<double>(nb);
+  PA_CUDA(cudaEventRecord(c->ev0, c->stream));
+  int launches = cholesky_lower(dA, n, info, work, c->stream);
+  if (nb) launches += trsm_lower_left(dA, n, work, dB, n, nrhs, dC, n, c->stream);
   PA_CUDA(cudaGetLastError());
+  PA_CUDA(cudaEventRecord(c->ev1, c->stream));
   PA_CUDA(cudaMemcpyAsync(A, dA, sizeof(double) * nn, cudaMemcpyDeviceToHost, c->stream));
-  if (nb) PA_CUDA(cudaMemcpyAsync(B, dB, sizeof(double) * nb, cudaMemcpyDeviceToHost, c->stream));
+  if (nb) PA_CUDA(cudaMemcpyAsync(B, dC, sizeof(double) * nb, cudaMemcpyDeviceToHost, c->stream));
   PA_CUDA(cudaMemcpyAsync(c->h_info, info, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   PA_CUDA(cudaStreamSynchronize(c->stream));
+  float ms = 0.f;
+  PA_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  g_stats = pa_stats{};
+  g_stats.ms_solve = g_stats.ms_total = ms;
+  g_stats.kernel_launches = launches;
   if (*c->h_info != 0)
     return fail(PA_ERR_NOT_SPD, "matrix is not positive definite (Cholesky pivot " +
                                     std::to_string(*c->h_info) + ")");

@@ -16,6 +16,7 @@
 #include "boys.cuh"
 #include "k_df3c.cuh"
 #include "pa_internal.h"
+#include "sph_raw.cuh"
 
 namespace pa {
 
@@ -146,12 +147,20 @@ int build_tables(TablesOnDevice* out, std::string* err) {
   std::vector<int16_t> col;
   std::vector<double> val, dense;
   std::vector<int> dense_off;
+  std::vector<double> rownorm((PA_LAUXMAX + 1) * (PA_LAUXMAX + 1), 0.0);
   const int lsph = std::max(PA_LMAX, PA_LAUXMAX);
   for (int l = 0; l <= lsph; ++l) {
     const std::vector<double> T = solid_harmonics(l);
     const int nc = ncart(l);
     dense_off.push_back(static_cast<int>(dense.size()));
     dense.insert(dense.end(), T.begin(), T.end());
+    if (l <= PA_LAUXMAX)
+      for (int m = 0; m < 2 * l + 1; ++m)
+        for (int i = l, c = 0; i >= 0; --i)
+          for (int j = l - i; j >= 0; --j, ++c) {
+            const double r = sph_raw(l, m - l, i, j, l - i - j);
+            if (r != 0.0 && rownorm[l * l + m] == 0.0) rownorm[l * l + m] = T[m * nc + c] / r;
+          }
     for (int m = 0; m < 2 * l + 1; ++m) {
       for (int c = 0; c < nc; ++c) {
         const double v = T[m * nc + c];
@@ -191,7 +200,7 @@ int build_tables(TablesOnDevice* out, std::string* err) {
   dt.sph_start = reinterpret_cast<const int*>(put(start.data(), sizeof(int) * start.size()));
   dt.sph_col = reinterpret_cast<const int16_t*>(put(col.data(), sizeof(int16_t) * col.size()));
   dt.sph_val = reinterpret_cast<const double*>(put(val.data(), sizeof(double) * val.size()));
-  e = upload_sph_dense(dense.data(), static_cast<int>(dense.size()), dense_off.data(), 0);
+  e = upload_sph_dense(dense.data(), static_cast<int>(dense.size()), dense_off.data(), rownorm.data(), 0);
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
     *err = std::string("table upload: ") + cudaGetErrorString(e);

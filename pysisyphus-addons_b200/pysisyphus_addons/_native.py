@@ -221,7 +221,8 @@ def metric(aux):
 
 
 def cholesky_solve(A, B):
-    """(L, L^-1 B) computed on the device (lower Cholesky factor of A)."""
+    """(L, L^-1 B) computed on the device, A = L L^T (L in the lower triangle
+    of the first result; the linear algebra of the reference's inv_chol + dtrmm)."""
     A = np.array(A, dtype=np.float64, order="F", copy=True)
     B = np.array(B, dtype=np.float64, order="F", copy=True)
     n = A.shape[0]

@@ -213,15 +213,19 @@ def test_error_nan_coordinates():
 
 
 def test_cholesky_solve_vs_numpy():
+    """Blocked Cholesky (64-wide blocks, ragged last block) and the blocked
+    forward substitution on one and several 64-column tiles of B."""
     rng = np.random.default_rng(7)
-    for n in (1, 63, 64, 65, 200):
+    for n, nrhs in ((1, 5), (63, 5), (64, 5), (65, 100), (200, 36), (300, 5), (700, 130)):
         X = rng.normal(size=(n, n))
         A = X @ X.T + n * np.eye(n)
-        B = rng.normal(size=(n, 5))
+        B = rng.normal(size=(n, nrhs))
         L, Y = nat.cholesky_solve(A, B)
         Lref = np.linalg.cholesky(A)
         np.testing.assert_allclose(np.tril(L), Lref, atol=1e-12 * np.abs(Lref).max())
-        np.testing.assert_allclose(Y, np.linalg.solve(Lref, B), atol=1e-11)
+        np.testing.assert_allclose(np.triu(L, 1), np.triu(A, 1))
+        Yref = np.linalg.solve(Lref, B)
+        np.testing.assert_allclose(Y, Yref, atol=1e-12 * np.abs(Yref).max())
 
 
 def test_error_non_spd_metric():
