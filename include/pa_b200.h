@@ -182,6 +182,36 @@ int pa_metric(pa_basis aux, double* metric);
  * (n x nrhs) by L^-1 B. PA_ERR_NOT_SPD when A is not positive definite. */
 int pa_cholesky_solve(int n, double* A, int nrhs, double* B);
 
+/* Allocation-free variant of pa_cholesky_solve on device buffers. This entry
+ * point has no counterpart in the reference.
+ *
+ * Who it is for: callers that cannot allocate device memory at call time --
+ * applications whose GPU memory is handed out entirely by another allocator
+ * (e.g. a framework's caching allocator that reserved the device up front),
+ * and code that must not call cudaMalloc / cudaFree because those calls can
+ * synchronize the whole device and stall unrelated work. It calls no
+ * cudaMalloc, cudaFree, memory pool or allocating library routine; its
+ * scratch memory is one fixed array of PA_NOALLOC_SCRATCH_DOUBLES doubles
+ * (8 MiB) in the library's device image, which every GPU that loads the
+ * library holds until the process exits.
+ *
+ * d_A (n x n, column-major, device): its lower triangle is replaced by L with
+ * A = L L^T (entries above the diagonal are left as they were). d_B (n x nrhs,
+ * device) is read only; d_X (n x nrhs, device) receives L^-1 B. stream is a
+ * cudaStream_t (0 = default stream); the call returns after the work on it has
+ * finished. Limit: 4096 * ceil(n / 64) + n * nrhs + 32 <= PA_NOALLOC_SCRATCH_DOUBLES
+ * (e.g. n = 2240 with nrhs up to 404), else PA_ERR_SCRATCH before any device
+ * work. PA_ERR_NOT_SPD as for pa_cholesky_solve.
+ *
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture. All calls in the process share the one array per
+ * device: calls that overlap on the GPU (concurrent streams or host threads)
+ * race on it and must be serialized by the caller. */
+#define PA_NOALLOC_SCRATCH_DOUBLES (1 << 20)
+int pa_cholesky_solve_noalloc(int n, double* d_A, int nrhs, const double* d_B, double* d_X,
+                              void* stream);
+
 #ifdef __cplusplus
 }
 #endif

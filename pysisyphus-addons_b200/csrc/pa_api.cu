@@ -54,6 +54,10 @@ Options options() {
 
 }  // namespace
 
+// Records the calling thread's error message for pa_last_error (used by the
+// C-ABI entry points in other translation units).
+int set_error(int code, const std::string& msg) { return fail(code, msg); }
+
 // ---------------------------------------------------------------------------
 // Basis unpacking: common/shells.f90:97-187 and common/normalization.f90:10-38.
 int unpack_basis(int nshells, int ndata, const int* bas_centers, const int* bas_spec,

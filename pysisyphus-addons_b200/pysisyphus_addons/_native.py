@@ -29,6 +29,7 @@ PA_LAYOUT_FORTRAN = 0
 PA_LAYOUT_C = 1
 PA_LMAX_ORBITAL = 4
 PA_LMAX_AUX = 5
+PA_NOALLOC_SCRATCH_DOUBLES = 1 << 20
 
 _ERRNAMES = {
     PA_ERR_ARG: "invalid argument",
@@ -98,6 +99,7 @@ SIGNATURES = {
     "pa_boys_eval": [_i, _i, _i, _pd, _pd],
     "pa_metric": [_vp, _pd],
     "pa_cholesky_solve": [_i, _pd, _i, _pd],
+    "pa_cholesky_solve_noalloc": [_i, _vp, _i, _vp, _vp, _vp],
 }
 
 _lib = None
