@@ -165,6 +165,17 @@ int pa_contract_coulomb_densities_4d(pa_basis orbital, pa_basis aux, int ndens, 
                                      const double* densities, int layout, int nstates,
                                      double* coulomb_tensor);
 
+/* Device-resident sTDDFT tensors (std/intor.f90); outputs column-major on the
+ * device, synchronous on `stream`:
+ *   pa_std_df1c:    d_out(nbf, naux)  = (mu mu|P) L^-T            (intor_df1c)
+ *   pa_std_eri2c:   d_out(nbf, nbf)   = df1c df1c^T                (intor_eri2c)
+ *   pa_std_df2c_mo: d_out(nmos(nmos+1)/2, naux) = packed (pq|P) L^-T for the MO
+ *                   coefficients d_mo(nbf, nmos)                   (intor_df2c_mo) */
+int pa_std_df1c(pa_basis orbital, pa_basis aux, double* d_out, void* stream);
+int pa_std_eri2c(pa_basis orbital, pa_basis aux, double* d_out, void* stream);
+int pa_std_df2c_mo(pa_basis orbital, pa_basis aux, int nmos, const double* d_mo, double* d_out,
+                   void* stream);
+
 /* Screening statistics for a basis pair: number of shell triplets that pass
  * the Schwarz test and their spherical integral count (runs the Schwarz
  * kernels; host-side counting). */

@@ -833,7 +833,7 @@ void df1c(const OBasis& B, const OBasis& X, double* T) {
       }
     }
   }
-  trmm_right_lower_trans(metric, naux, T, nbf);
+  if (!g_skip_metric) trmm_right_lower_trans(metric, naux, T, nbf);
 }
 
 // intor_df2c_mo (std/intor.f90:141-292).
@@ -897,7 +897,7 @@ void df2c_mo(const OBasis& B, const OBasis& X, int nmos, const double* C, double
       }
     }
   }
-  trmm_right_lower_trans(metric, naux, out, npack);
+  if (!g_skip_metric) trmm_right_lower_trans(metric, naux, out, npack);
 }
 
 // erfinv: rational approximations of Blair, Edwards and Johnson (1976),

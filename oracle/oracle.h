@@ -28,7 +28,7 @@ extern "C" {
 void oracle_set_boys_mode(int mode);
 int oracle_get_boys_mode(void);
 void oracle_set_threads(int nthreads);
-/* 1: skip the metric (inv_chol + dtrmm) in the 2d/4d drivers (raw contraction). */
+/* 1: skip the metric (inv_chol + dtrmm) in the 2d/4d and std drivers (raw tensors). */
 void oracle_set_skip_metric(int skip);
 int oracle_get_threads(void);
 /* Optional BLAS/LAPACK (Fortran calling convention) used by inv_chol / dtrmm /

@@ -22,6 +22,7 @@
 #include "k_df3c.cuh"
 #include "k_integrals.cuh"
 #include "k_linalg.cuh"
+#include "k_std.cuh"
 #include "pa_b200.h"
 #include "pa_internal.h"
 
@@ -737,6 +738,197 @@ int df_host(pa_basis orb, pa_basis aux, int ndens, int nbf, const double* dens, 
   return PA_OK;
 }
 
+// ---------------------------------------------------------------------------
+// sTDDFT tensors (std/intor.f90). kind: 0 = df1c (nbf x naux), 1 = eri2c
+// (nbf x nbf), 2 = df2c_mo (nmos(nmos+1)/2 x naux); all column-major.
+enum StdKind { kStdDf1c = 0, kStdEri2c = 1, kStdDf2cMo = 2 };
+
+// Doubles of W per batch of the df2c_mo half transformation (1 GiB).
+constexpr size_t kStdWBudget = size_t(1) << 27;
+
+int std_device(pa_basis orb, pa_basis aux, int kind, int nmos, const double* d_mo, double* d_out,
+               cudaStream_t s) {
+  int st = check_pair(orb, aux);
+  if (st != PA_OK) return st;
+  if (kind == kStdDf2cMo && (nmos < 0 || (nmos > 0 && !d_mo))) return fail(PA_ERR_ARG, "invalid MO tensor");
+  if (!d_out) return fail(PA_ERR_ARG, "null output pointer");
+  if (orb->host.shells.size() > 65535) return fail(PA_ERR_ARG, "more than 65535 orbital shells");
+  Ctx* c = nullptr;
+  DeviceTables dt;
+  st = current_ctx(&c, &dt);
+  if (st != PA_OK) return st;
+  std::lock_guard<std::mutex> lk(c->mu);
+  const Options o = options();
+  const PairLists& P = orb->pairs;
+  const int nbf = orb->host.nsph, naux = aux->host.nsph;
+  const int nx = static_cast<int>(aux->host.shells.size());
+  const long long npack = static_cast<long long>(nmos) * (nmos + 1) / 2;
+  const long long ncols = kind == kStdDf2cMo ? npack : nbf;
+  // auxiliary shell batches of the df2c_mo half transformation
+  std::vector<int> batch{0};
+  size_t wmax = 0, resmax = 0;
+  if (kind == kStdDf2cMo && nmos > 0) {
+    const size_t per_fn = static_cast<size_t>(nmos) * nbf;
+    size_t fns = 0;
+    for (int i = 0; i < nx; ++i) {
+      const size_t f = 2 * aux->host.shells[i].L + 1;
+      if (fns > 0 && (fns + f) * per_fn > kStdWBudget) {
+        batch.push_back(i);
+        fns = 0;
+      }
+      fns += f;
+      wmax = std::max(wmax, fns * per_fn);
+      resmax = std::max(resmax, fns * static_cast<size_t>(nmos) * nmos);
+    }
+  }
+  batch.push_back(nx);
+  Carver cnt;
+  // one layout, carved twice (count, then real)
+  struct Bufs {
+    double *Qab, *Qc, *esph, *M, *lawork, *raw, *y, *W, *res;
+    double4* pP;
+    int* info;
+  } b{};
+  for (int pass = 0; pass < 2; ++pass) {
+    Carver cv;
+    if (pass == 1) {
+      PA_CUDA(c->arena.reserve(cnt.used));
+      cv.base = c->arena.base;
+    }
+    b.Qab = cv.take<double>(P.npairs);
+    b.Qc = cv.take<double>(nx);
+    b.pP = cv.take<double4>(P.nunits);
+    b.esph = cv.take<double>(P.esph_total);
+    b.M = cv.take<double>(static_cast<size_t>(naux) * naux);
+    b.lawork = cv.take<double>(linalg_workspace_doubles(naux));
+    b.info = cv.take<int>(4);
+    b.raw = cv.take<double>(static_cast<size_t>(naux) * ncols);
+    b.y = cv.take<double>(static_cast<size_t>(naux) * ncols);
+    b.W = cv.take<double>(wmax);
+    b.res = cv.take<double>(resmax);
+    if (pass == 0) cnt = cv;
+  }
+  PA_CUDA(cudaEventRecord(c->ev0, s));
+  int launches = 0;
+  // metric + Cholesky on the second stream
+  cudaStream_t s2 = c->stream2;
+  PA_CUDA(cudaEventRecord(c->fork, s));
+  PA_CUDA(cudaStreamWaitEvent(s2, c->fork, 0));
+  PA_CUDA(cudaEventRecord(c->m0, s2));
+  launches += launch_metric(aux->dev, dt, o.boys_mode, b.M, s2);
+  launches += cholesky_lower(b.M, naux, b.info, b.lawork, s2);
+  PA_CUDA(cudaEventRecord(c->m1, s2));
+  // Schwarz vectors (screener%init, common/screening.f90:101-163)
+  UnitArrays U;
+  U.unit_pair = orb->d_unit_pair;
+  U.unit_prims = orb->d_unit_prims;
+  U.unit_esph = orb->d_unit_esph;
+  U.unit_pP = b.pP;
+  U.esph = b.esph;
+  launches += launch_unit_setup(orb->dev, orb->d_pair_ab, U, P.nunits, dt, s);
+  launches += launch_schwarz_bra(orb->dev, orb->d_pair_ab, orb->d_pair_unit0, U, P.npairs, P.lab_max, dt,
+                                 o.boys_mode, b.Qab, s);
+  launches += launch_schwarz_aux(aux->dev, dt, o.boys_mode, b.Qc, s);
+  PA_CUDA(cudaEventRecord(c->ph[0], s));
+  StdArgs a;
+  a.B = orb->dev;
+  a.X = aux->dev;
+  a.dt = dt;
+  a.boys_mode = o.boys_mode;
+  a.thresh = o.screen_thresh;
+  a.pair_ab = orb->d_pair_ab;
+  a.pair_unit0 = orb->d_pair_unit0;
+  a.unit_pP = b.pP;
+  a.esph = b.esph;
+  a.unit_esph = orb->d_unit_esph;
+  a.Qab = b.Qab;
+  a.Qc = b.Qc;
+  const size_t raw_bytes = sizeof(double) * static_cast<size_t>(naux) * ncols;
+  if (kind != kStdDf2cMo) {
+    // screened (a, a, c) entries stay zero (the reference's output starts zeroed)
+    if (raw_bytes) PA_CUDA(cudaMemsetAsync(b.raw, 0, raw_bytes, s));
+    launches += launch_std_df1c(a, b.raw, s);
+  } else if (nmos > 0) {
+    for (size_t bi = 0; bi + 1 < batch.size(); ++bi) {
+      const int c0 = batch[bi], c1 = batch[bi + 1];
+      if (c1 <= c0) continue;
+      const int k0 = aux->host.shells[c0].sph_off;
+      const int k1 = c1 < nx ? aux->host.shells[c1].sph_off : naux;
+      const int nk = k1 - k0;
+      launches += launch_std_df2c_half(a, c0, c1, k0, nmos, d_mo, b.W, s);
+      // Res[(kk, p), q] = sum_nu W[(kk, p)][nu] C[nu, q] (std/intor.f90:263-279)
+      launches += gemm(true, false, nk * nmos, nmos, nbf, 1.0, b.W, nbf, d_mo, nbf, 0.0, b.res,
+                       static_cast<long long>(nk) * nmos, false, s);
+      launches += launch_std_pack(b.res, nk, nmos, k0, naux, b.raw, s);
+    }
+  }
+  PA_CUDA(cudaEventRecord(c->ph[1], s));
+  PA_CUDA(cudaStreamWaitEvent(s, c->m1, 0));
+  const double* y = b.raw;
+  if (!o.skip_metric && ncols > 0 && naux > 0) {
+    // T L^-T = (L^-1 T^T)^T (std/intor.f90:116,290: dtrmm("R","L","T","N"))
+    launches += trsm_lower_left(b.M, naux, b.lawork, b.raw, naux, static_cast<int>(ncols), b.y, naux, s);
+    y = b.y;
+  }
+  if (kind == kStdEri2c) {
+    // (mu mu|nu nu) = T T^T (std/intor.f90:137)
+    launches += gemm(true, false, nbf, nbf, naux, 1.0, y, naux, y, naux, 0.0, d_out, nbf, false, s);
+    if (naux == 0 && nbf > 0)
+      PA_CUDA(cudaMemsetAsync(d_out, 0, sizeof(double) * static_cast<size_t>(nbf) * nbf, s));
+  } else {
+    launches += launch_transpose(y, static_cast<int>(ncols), naux, d_out, s);
+  }
+  PA_CUDA(cudaGetLastError());
+  PA_CUDA(cudaEventRecord(c->ev1, s));
+  PA_CUDA(cudaMemcpyAsync(c->h_info, b.info, sizeof(int), cudaMemcpyDeviceToHost, s));
+  PA_CUDA(cudaStreamSynchronize(s));
+  float t[4] = {0, 0, 0, 0};
+  PA_CUDA(cudaEventElapsedTime(&t[0], c->ev0, c->ev1));
+  PA_CUDA(cudaEventElapsedTime(&t[1], c->ev0, c->ph[0]));
+  PA_CUDA(cudaEventElapsedTime(&t[2], c->ph[0], c->ph[1]));
+  PA_CUDA(cudaEventElapsedTime(&t[3], c->m0, c->m1));
+  g_stats = pa_stats{};
+  g_stats.ms_total = t[0];
+  g_stats.ms_screen = t[1];
+  g_stats.ms_3c = t[2];
+  g_stats.ms_metric = t[3];
+  g_stats.ms_solve = t[0] - t[1] - t[2];
+  g_stats.kernel_launches = launches;
+  g_stats.launches_3c = 0;
+  g_stats.ntriplets = -1;
+  g_stats.nskipped = -1;
+  g_stats.nints = -1;
+  if (*c->h_info != 0)
+    return fail(PA_ERR_NOT_SPD, "metric (P|Q) is not positive definite (Cholesky pivot " +
+                                    std::to_string(*c->h_info) + ")");
+  return PA_OK;
+}
+
+// Host-buffer std call: uploads the MO tensor, runs, downloads.
+int std_host(pa_basis orb, pa_basis aux, int kind, int nmos, const double* mo, double* out,
+             size_t out_count) {
+  int st = check_pair(orb, aux);
+  if (st != PA_OK) return st;
+  Ctx* c = nullptr;
+  DeviceTables dt;
+  st = current_ctx(&c, &dt);
+  if (st != PA_OK) return st;
+  const size_t mo_bytes = sizeof(double) * static_cast<size_t>(orb->host.nsph) * std::max(nmos, 0);
+  double *d_mo = nullptr, *d_out = nullptr;
+  PA_CUDA(cudaMallocFromPoolAsync(&d_mo, std::max<size_t>(mo_bytes, 8), c->pool, c->stream));
+  PA_CUDA(cudaMallocFromPoolAsync(&d_out, sizeof(double) * std::max<size_t>(out_count, 1), c->pool, c->stream));
+  if (mo_bytes) PA_CUDA(cudaMemcpyAsync(d_mo, mo, mo_bytes, cudaMemcpyHostToDevice, c->stream));
+  st = std_device(orb, aux, kind, nmos, d_mo, d_out, c->stream);
+  if (st == PA_OK && out_count)
+    cudaMemcpyAsync(out, d_out, sizeof(double) * out_count, cudaMemcpyDeviceToHost, c->stream);
+  cudaFreeAsync(d_mo, c->stream);
+  cudaFreeAsync(d_out, c->stream);
+  const cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (st != PA_OK) return st;
+  if (e != cudaSuccess) return fail(PA_ERR_CUDA, std::string("download: ") + cudaGetErrorString(e));
+  return PA_OK;
+}
+
 struct BasisGuard {
   pa_basis b = nullptr;
   ~BasisGuard() {
@@ -1146,17 +1338,74 @@ int pa_cholesky_solve(int n, double* A, int nrhs, double* B) {
   return PA_OK;
 }
 
-int f_intor_eri2c(int, int, const int*, const int*, const double*, int, int, const int*, const int*,
-                  const double*, int, double*) {
-  return fail(PA_ERR_ARG, "f_intor_eri2c: not available in this build");
+}  // extern "C"
+
+extern "C" {
+
+int pa_std_df1c(pa_basis orbital, pa_basis aux, double* d_out, void* stream) {
+  return std_device(orbital, aux, kStdDf1c, 0, nullptr, d_out, static_cast<cudaStream_t>(stream));
 }
-int f_intor_df1c(int, int, const int*, const int*, const double*, int, int, const int*, const int*,
-                 const double*, int, int, double*) {
-  return fail(PA_ERR_ARG, "f_intor_df1c: not available in this build");
+
+int pa_std_eri2c(pa_basis orbital, pa_basis aux, double* d_out, void* stream) {
+  return std_device(orbital, aux, kStdEri2c, 0, nullptr, d_out, static_cast<cudaStream_t>(stream));
 }
-int f_intor_df2c_mo(int, int, const int*, const int*, const double*, int, int, const int*,
-                    const int*, const double*, int, int, const double*, int, double*) {
-  return fail(PA_ERR_ARG, "f_intor_df2c_mo: not available in this build");
+
+int pa_std_df2c_mo(pa_basis orbital, pa_basis aux, int nmos, const double* d_mo, double* d_out,
+                   void* stream) {
+  return std_device(orbital, aux, kStdDf2cMo, nmos, d_mo, d_out, static_cast<cudaStream_t>(stream));
+}
+
+int f_intor_eri2c(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
+                  const double* bas_data, int nshells_aux, int ndata_aux,
+                  const int* bas_centers_aux, const int* bas_spec_aux,
+                  const double* bas_data_aux, int nbfs, double* eri2c_tensor) {
+  BasisGuard orb, aux;
+  int st = pa_basis_create(nshells, ndata, bas_centers, bas_spec, bas_data, PA_LMAX, &orb.b);
+  if (st != PA_OK) return st;
+  st = pa_basis_create(nshells_aux, ndata_aux, bas_centers_aux, bas_spec_aux, bas_data_aux,
+                       PA_LAUXMAX, &aux.b);
+  if (st != PA_OK) return st;
+  if (nbfs != orb.b->host.nsph)
+    return fail(PA_ERR_ARG, "nbfs does not match the orbital basis");
+  if (nbfs > 0 && !eri2c_tensor) return fail(PA_ERR_ARG, "null output pointer");
+  return std_host(orb.b, aux.b, kStdEri2c, 0, nullptr, eri2c_tensor,
+                  static_cast<size_t>(nbfs) * nbfs);
+}
+
+int f_intor_df1c(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
+                 const double* bas_data, int nshells_aux, int ndata_aux,
+                 const int* bas_centers_aux, const int* bas_spec_aux, const double* bas_data_aux,
+                 int nbfs, int nbfs_aux, double* df1c_tensor) {
+  BasisGuard orb, aux;
+  int st = pa_basis_create(nshells, ndata, bas_centers, bas_spec, bas_data, PA_LMAX, &orb.b);
+  if (st != PA_OK) return st;
+  st = pa_basis_create(nshells_aux, ndata_aux, bas_centers_aux, bas_spec_aux, bas_data_aux,
+                       PA_LAUXMAX, &aux.b);
+  if (st != PA_OK) return st;
+  if (nbfs != orb.b->host.nsph || nbfs_aux != aux.b->host.nsph)
+    return fail(PA_ERR_ARG, "nbfs / nbfs_aux do not match the bases");
+  if (static_cast<long long>(nbfs) * nbfs_aux > 0 && !df1c_tensor) return fail(PA_ERR_ARG, "null output pointer");
+  return std_host(orb.b, aux.b, kStdDf1c, 0, nullptr, df1c_tensor,
+                  static_cast<size_t>(nbfs) * nbfs_aux);
+}
+
+int f_intor_df2c_mo(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
+                    const double* bas_data, int nshells_aux, int ndata_aux,
+                    const int* bas_centers_aux, const int* bas_spec_aux,
+                    const double* bas_data_aux, int nbfs, int nmos, const double* mo_tensor,
+                    int nbfs_aux, double* df2c_mo_tensor) {
+  BasisGuard orb, aux;
+  int st = pa_basis_create(nshells, ndata, bas_centers, bas_spec, bas_data, PA_LMAX, &orb.b);
+  if (st != PA_OK) return st;
+  st = pa_basis_create(nshells_aux, ndata_aux, bas_centers_aux, bas_spec_aux, bas_data_aux,
+                       PA_LAUXMAX, &aux.b);
+  if (st != PA_OK) return st;
+  if (nbfs != orb.b->host.nsph || nbfs_aux != aux.b->host.nsph)
+    return fail(PA_ERR_ARG, "nbfs / nbfs_aux do not match the bases");
+  if (nmos < 0 || (nmos > 0 && (!mo_tensor || !df2c_mo_tensor)))
+    return fail(PA_ERR_ARG, "invalid MO tensor or output");
+  const size_t npack = static_cast<size_t>(nmos) * (nmos + 1) / 2;
+  return std_host(orb.b, aux.b, kStdDf2cMo, nmos, mo_tensor, df2c_mo_tensor, npack * nbfs_aux);
 }
 
 }  // extern "C"

@@ -99,6 +99,9 @@ SIGNATURES = {
     "pa_boys_eval": [_i, _i, _i, _pd, _pd],
     "pa_metric": [_vp, _pd],
     "pa_cholesky_solve": [_i, _pd, _i, _pd],
+    "pa_std_df1c": [_vp, _vp, _vp, _vp],
+    "pa_std_eri2c": [_vp, _vp, _vp, _vp],
+    "pa_std_df2c_mo": [_vp, _vp, _i, _vp, _vp, _vp],
     "pa_cholesky_solve_noalloc": [_i, _vp, _i, _vp, _vp, _vp],
 }
 

@@ -1,0 +1,116 @@
+"""sTDDFT tensors (pysisyphus_addons.std.intor) on the GPU against the oracle.
+
+The raw tensors (before the metric factor L^-T) are compared at 1e-13 of their
+largest element. The full tensors include L^-T: the reference forms L^-1
+explicitly (dtrtri) and multiplies (dtrmm), the GPU path solves with L, and
+the two differ by the metric's conditioning times the rounding of either
+(common/linalg.f90:60-82), so they are compared at 1e-11 of their largest
+element at the 8-atom size (metric condition number ~1e8 there).
+
+intor_df2c_mo drops integrals |(ab|c)| <= 1e-10 and half-transformed values
+<= 1e-10 (std/intor.f90:247,269); the GPU kernel reproduces both skips, which
+move the result by ~4e-9 at this size, so agreement at 1e-13 shows they are
+applied triple by triple as in the reference.
+"""
+
+import numpy as np
+import pytest
+
+import oracle
+from pysisyphus_addons import _native as nat
+from pysisyphus_addons.common.shells import Shell, Shells
+from pysisyphus_addons.common.synthetic import config_workload
+from pysisyphus_addons.std import intor as std
+
+pytestmark = pytest.mark.gpu
+
+
+def close(x, ref, rel_of_max, atol=1e-14):
+    tol = atol + rel_of_max * np.abs(ref).max()
+    err = np.abs(x - ref).max()
+    assert err <= tol, f"max abs err {err:.3e} > {tol:.3e}"
+
+
+@pytest.fixture(params=["reference", "exact"])
+def mode(request):
+    nat.set_boys_mode(request.param)
+    oracle.set_boys_mode(request.param)
+    yield request.param
+    nat.set_boys_mode("reference")
+    oracle.set_boys_mode("reference")
+
+
+@pytest.fixture
+def raw():
+    nat.set_skip_metric(1)
+    oracle.set_skip_metric(1)
+    yield
+    nat.set_skip_metric(0)
+    oracle.set_skip_metric(0)
+
+
+@pytest.fixture(scope="module")
+def w1():
+    return config_workload("cfg1")
+
+
+def test_df1c_raw(w1, mode, raw):
+    T = std.int_df1c(w1.shells, w1.shells_aux)
+    To = oracle.int_df1c(w1.shells, w1.shells_aux)
+    assert T.shape == (w1.shells.sph_size, w1.shells_aux.sph_size) and T.flags.f_contiguous
+    close(T, To, 1e-13)
+
+
+def test_df1c_and_eri2c(w1, mode):
+    T = std.int_df1c(w1.shells, w1.shells_aux)
+    close(T, oracle.int_df1c(w1.shells, w1.shells_aux), 1e-11)
+    E = std.int_eri2c(w1.shells, w1.shells_aux)
+    Eo = oracle.int_eri2c(w1.shells, w1.shells_aux)
+    assert E.shape == (w1.shells.sph_size,) * 2
+    close(E, Eo, 1e-11)
+    np.testing.assert_allclose(E, E.T, atol=1e-12 * np.abs(E).max())
+
+
+def test_eri2c_raw(w1, raw):
+    close(std.int_eri2c(w1.shells, w1.shells_aux), oracle.int_eri2c(w1.shells, w1.shells_aux), 1e-13)
+
+
+@pytest.mark.parametrize("nocc,nvirt", [(6, 6), (1, 0), (20, 45)])
+def test_df2c_mo_raw(w1, mode, raw, nocc, nvirt):
+    """nmos 12, 1 and 65 (two MO chunks of the half-transformation kernel)."""
+    C = w1.mo_coeffs[:, : nocc + nvirt]
+    X = std.int_df2c_mo(w1.shells, w1.shells_aux, C)
+    Xo = oracle.int_df2c_mo(w1.shells, w1.shells_aux, C)
+    n = C.shape[1]
+    assert X.shape == (n * (n + 1) // 2, w1.shells_aux.sph_size) and X.flags.f_contiguous
+    close(X, Xo, 1e-13)
+
+
+def test_df2c_mo_full(w1):
+    C = w1.mo_coeffs[:, :12]
+    close(std.int_df2c_mo(w1.shells, w1.shells_aux, C), oracle.int_df2c_mo(w1.shells, w1.shells_aux, C), 1e-11)
+
+
+def test_df2c_mo_reconstructs_df1c_pairs(w1, raw):
+    """With C = identity columns the packed rows (mu mu) equal (mu mu|P) of df1c
+    away from the value skips (a consistency check between the two kernels)."""
+    nbf = w1.shells.sph_size
+    sel = [0, 3, 17, 40]
+    C = np.eye(nbf)[:, sel]
+    X = std.int_df2c_mo(w1.shells, w1.shells_aux, C)
+    T = std.int_df1c(w1.shells, w1.shells_aux)
+    for k, mu in enumerate(sel):
+        row = X[k * (k + 1) // 2 + k]
+        big = np.abs(T[mu]) > 1e-8
+        np.testing.assert_allclose(row[big], T[mu][big], rtol=1e-12)
+
+
+def test_std_errors():
+    sh = Shells([Shell(5, [0, 0, 0], [1.0], [1.0])])
+    aux = Shells([Shell(0, [0, 0, 0], [1.0], [1.0])])
+    with pytest.raises(nat.PaError) as e:
+        std.int_df1c(sh, aux)
+    assert e.value.code == nat.PA_ERR_LMAX
+    w = config_workload("cfg1")
+    with pytest.raises(ValueError):
+        std.int_df2c_mo(w.shells, w.shells_aux, np.zeros(5))
