@@ -124,6 +124,12 @@ int pa_set_screen_threshold(double thresh);
 /* 1: return the raw contraction sum_(a>=b) (ab|P) Dsym without the metric
  * solve L^-1 (the first half of the density fit); 0 (default): full path. */
 int pa_set_skip_metric(int skip);
+/* Adds shift * I to (P|Q) before its Cholesky factorization in every
+ * density-fitting entry point (default 0: the reference's behaviour). An
+ * option for auxiliary bases that are linearly dependent to machine precision
+ * (dpotrf fails; the reference then continues with a broken factor, its info
+ * being ignored, common/linalg.f90:78). */
+int pa_set_metric_shift(double shift);
 
 /* Statistics of the last density-fitting call on this process. */
 typedef struct {

@@ -31,6 +31,8 @@ const double DF2C_SKIP2 = 1e-10;
 
 int g_boys_mode = 0;
 int g_skip_metric = 0;
+// Optional diagonal shift of (P|Q) before the factorization (0 = the reference).
+double g_metric_shift = 0.0;
 OracleStats g_stats{};
 
 // ---------------------------------------------------------------------------
@@ -622,6 +624,8 @@ std::vector<double> metric_2c2e(const OBasis& B) {
 // lower triangle then holds L^-1. LAPACK's info is ignored, as in the
 // reference.
 void inv_chol(std::vector<double>& A, int n) {
+  if (g_metric_shift != 0.0)
+    for (int j = 0; j < n; ++j) A[j + static_cast<size_t>(j) * n] += g_metric_shift;
   if (p_dpotrf && p_dtrtri) {
     int info = 0;
     const char lo = 'L', nu = 'N';
@@ -949,6 +953,7 @@ extern "C" {
 void oracle_set_boys_mode(int mode) { g_boys_mode = mode; }
 int oracle_get_boys_mode(void) { return g_boys_mode; }
 void oracle_set_skip_metric(int skip) { g_skip_metric = skip ? 1 : 0; }
+void oracle_set_metric_shift(double shift) { g_metric_shift = shift; }
 void oracle_set_threads(int nthreads) {
   if (nthreads > 0) omp_set_num_threads(nthreads);
 }

@@ -30,6 +30,10 @@ int oracle_get_boys_mode(void);
 void oracle_set_threads(int nthreads);
 /* 1: skip the metric (inv_chol + dtrmm) in the 2d/4d and std drivers (raw tensors). */
 void oracle_set_skip_metric(int skip);
+/* Adds shift * I to (P|Q) before its Cholesky factorization (default 0: the
+ * reference's behaviour). For auxiliary bases that are linearly dependent to
+ * machine precision, where dpotrf fails. */
+void oracle_set_metric_shift(double shift);
 int oracle_get_threads(void);
 /* Optional BLAS/LAPACK (Fortran calling convention) used by inv_chol / dtrmm /
  * dgemm, exactly as the reference calls them; naive loops when unset. */

@@ -84,6 +84,7 @@ def lib():
     L.oracle_get_boys_mode.restype = _i
     L.oracle_set_threads.argtypes = [_i]
     L.oracle_set_skip_metric.argtypes = [_i]
+    L.oracle_set_metric_shift.argtypes = [_d]
     L.oracle_get_threads.restype = _i
     L.oracle_register_lapack.argtypes = [ctypes.c_void_p] * 4
     L.oracle_last_stats.argtypes = [ctypes.POINTER(OracleStats)]
@@ -127,6 +128,10 @@ def get_boys_mode():
 
 def set_skip_metric(skip):
     lib().oracle_set_skip_metric(int(bool(skip)))
+
+
+def set_metric_shift(shift):
+    lib().oracle_set_metric_shift(float(shift))
 
 
 def set_threads(n):

@@ -318,6 +318,11 @@ __global__ void k_coulomb4d(const double* __restrict__ gram, int ndens, int ns, 
   }
 }
 
+__global__ void k_add_diagonal(double* A, int n, double shift) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) A[i + static_cast<long long>(n) * i] += shift;
+}
+
 constexpr size_t kTileSmem = sizeof(double) * NB * (NB + 1);
 
 int gemm_impl(bool ta, bool tb, int m, int n, int k, double alpha, const double* A, long long lda,
@@ -382,6 +387,12 @@ int trsm_lower_left(const double* L, int n, const double* dinv, double* B, long 
     k_trsm_step<<<dim3(nblk - k, ct), 256, 0, s>>>(L, n, n, k, dinv + static_cast<size_t>(k) * NB * NB, B,
                                                    ldb, nrhs, C, ldc);
   return nblk;
+}
+
+int add_diagonal(double* A, int n, double shift, cudaStream_t s) {
+  if (shift == 0.0 || n <= 0) return 0;
+  k_add_diagonal<<<(n + 255) / 256, 256, 0, s>>>(A, n, shift);
+  return 1;
 }
 
 int coulomb_4d(const double* df, int naux, int ndens, int nstates, double* gram_scratch,

@@ -22,6 +22,8 @@ int cholesky_lower(double* A, int n, int* d_info, double* work, cudaStream_t s);
 // overwritten (used as scratch).
 int trsm_lower_left(const double* L, int n, const double* dinv, double* B, long long ldb, int nrhs,
                     double* C, long long ldc, cudaStream_t s);
+// A[i + n i] += shift for i < n (no launch when shift == 0).
+int add_diagonal(double* A, int n, double shift, cudaStream_t s);
 // Coulomb tensor R[ns,ns,ns,ns] (column-major) from df[naux, ndens].
 int coulomb_4d(const double* df, int naux, int ndens, int nstates, double* gram_scratch,
                double* R, cudaStream_t s);

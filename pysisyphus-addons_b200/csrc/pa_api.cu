@@ -486,6 +486,7 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
   cudaStreamWaitEvent(s2, ctx->fork, 0);
   cudaEventRecord(ctx->m0, s2);
   *launches += launch_metric(aux->dev, dt, o.boys_mode, b.M, s2);
+  *launches += add_diagonal(b.M, naux, o.metric_shift, s2);
   *launches += cholesky_lower(b.M, naux, b.info, b.lawork, s2);
   cudaEventRecord(ctx->m1, s2);
   int st = run_screening(orb, aux, dt, o, b, s, launches);
@@ -816,6 +817,7 @@ int std_device(pa_basis orb, pa_basis aux, int kind, int nmos, const double* d_m
   PA_CUDA(cudaStreamWaitEvent(s2, c->fork, 0));
   PA_CUDA(cudaEventRecord(c->m0, s2));
   launches += launch_metric(aux->dev, dt, o.boys_mode, b.M, s2);
+  launches += add_diagonal(b.M, naux, o.metric_shift, s2);
   launches += cholesky_lower(b.M, naux, b.info, b.lawork, s2);
   PA_CUDA(cudaEventRecord(c->m1, s2));
   // Schwarz vectors (screener%init, common/screening.f90:101-163)
@@ -963,6 +965,13 @@ int pa_set_screen_threshold(double thresh) {
   if (!(thresh >= 0.0)) return fail(PA_ERR_ARG, "threshold must be >= 0");
   std::lock_guard<std::mutex> lk(g_opt_mu);
   g_opts.screen_thresh = thresh;
+  return PA_OK;
+}
+
+int pa_set_metric_shift(double shift) {
+  if (!(shift >= 0.0) || !std::isfinite(shift)) return fail(PA_ERR_ARG, "metric shift must be finite and >= 0");
+  std::lock_guard<std::mutex> lk(g_opt_mu);
+  g_opts.metric_shift = shift;
   return PA_OK;
 }
 

@@ -72,6 +72,7 @@ struct Options {
   double screen_thresh = static_cast<double>(1e-10f);
   int verbose = 0;
   int skip_metric = 0;
+  double metric_shift = 0.0;  // added to the diagonal of (P|Q) before the Cholesky
 };
 
 struct Stats {

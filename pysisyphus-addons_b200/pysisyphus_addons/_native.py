@@ -86,6 +86,7 @@ SIGNATURES = {
     "pa_get_boys_mode": [],
     "pa_set_screen_threshold": [_d],
     "pa_set_skip_metric": [_i],
+    "pa_set_metric_shift": [_d],
     "pa_get_stats": [ctypes.POINTER(PaStats)],
     "pa_basis_create": [_i, _i, _pi, _pi, _pd, _i, ctypes.POINTER(_vp)],
     "pa_basis_destroy": [_vp],
@@ -163,6 +164,11 @@ def get_boys_mode():
 
 def set_screen_threshold(thresh):
     check(load().pa_set_screen_threshold(float(thresh)))
+
+
+def set_metric_shift(shift):
+    """Diagonal shift added to (P|Q) before the Cholesky factorization (0 = reference)."""
+    check(load().pa_set_metric_shift(float(shift)))
 
 
 def set_skip_metric(skip):

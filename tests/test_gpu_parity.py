@@ -236,3 +236,24 @@ def test_error_non_spd_metric():
         nat.cholesky_solve(A, np.ones((4, 1)))
     assert e.value.code == nat.PA_ERR_NOT_SPD
     assert "3" in str(e.value)
+
+
+def test_metric_shift_matches_oracle():
+    """The opt-in diagonal shift of (P|Q) (for auxiliary bases that are
+    numerically linearly dependent, where the Cholesky fails) is applied the
+    same way by the GPU path and the oracle; 0 restores the reference."""
+    w = config_workload("cfg1")
+    nat.set_metric_shift(1e-6)
+    oracle.set_metric_shift(1e-6)
+    oracle.set_boys_mode("reference")
+    try:
+        df = dia.contract_coulomb_densities_2d(w.shells, w.shells_aux, w.densities)
+        ref = oracle.contract_coulomb_densities_2d(w.shells, w.shells_aux, w.densities)
+    finally:
+        nat.set_metric_shift(0.0)
+        oracle.set_metric_shift(0.0)
+    assert_tensor_close(df, ref, atol=1e-11)
+    plain = dia.contract_coulomb_densities_2d(w.shells, w.shells_aux, w.densities)
+    assert np.abs(plain - df).max() > 1e-9  # the shift is actually applied
+    with pytest.raises(nat.PaError):
+        nat.set_metric_shift(-1.0)
