@@ -46,6 +46,10 @@ extern "C" {
 #define PA_BOYS_EXACT 0     /* ~1e-16 relative                                    */
 #define PA_BOYS_REFERENCE 1 /* behaviour of common/integrals/boys.f90 (default)    */
 
+/* Precision forms of the three-center contraction. */
+#define PA_PRECISION_FP64 0  /* FP64 throughout (default)                          */
+#define PA_PRECISION_MIXED 1 /* FP32 recurrences for triplets below a Schwarz bound */
+
 /* Density layouts for the pa_* entry points. */
 #define PA_LAYOUT_FORTRAN 0 /* (ndens, nbf, nbf) column-major: d fastest          */
 #define PA_LAYOUT_C 1       /* (ndens, nbf, nbf) row-major: last index fastest    */
@@ -130,6 +134,13 @@ int pa_set_skip_metric(int skip);
  * (dpotrf fails; the reference then continues with a broken factor, its info
  * being ignored, common/linalg.f90:78). */
 int pa_set_metric_shift(double shift);
+/* Precision form of the density-fitting contraction (process-wide):
+ * PA_PRECISION_FP64 (default) or PA_PRECISION_MIXED, in which shell triplets
+ * with Schwarz bound Q_ab * Q_c < fp32_thresh (e.g. 1e-6) evaluate the Boys
+ * function (below T = 27 / 30), the Hermite recurrence and the solid-harmonic
+ * contraction in FP32; their contributions are accumulated in FP64. */
+int pa_set_precision(int mode, double fp32_thresh);
+int pa_get_precision(void);
 
 /* Statistics of the last density-fitting call on this process. */
 typedef struct {

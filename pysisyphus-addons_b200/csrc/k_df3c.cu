@@ -34,6 +34,7 @@
 #include "md.cuh"
 #include "sph_raw.cuh"
 
+#include <algorithm>
 #include <utility>
 
 namespace pa {
@@ -133,9 +134,8 @@ __device__ __forceinline__ void cp_async_commit_wait_all() {
 }
 
 // Per-thread Hermite R (small L): in-place level recursion in registers.
-template <int L>
-__device__ __forceinline__ void hermite_R_thread(const double* Rn, double X, double Y, double Z,
-                                                 double* R) {
+template <int L, class Real>
+__device__ __forceinline__ void hermite_R_thread(const Real* Rn, Real X, Real Y, Real Z, Real* R) {
   R[0] = Rn[L];
 #pragma unroll
   for (int n = L - 1; n >= 0; --n) {
@@ -146,16 +146,16 @@ __device__ __forceinline__ void hermite_R_thread(const double* Rn, double X, dou
 #pragma unroll
         for (int u = deg - t; u >= 0; --u) {
           const int v = deg - t - u;
-          double val;
+          Real val;
           if (t > 0) {
             val = X * R[cidx(t - 1, u, v)];
-            if (t > 1) val = fma(static_cast<double>(t - 1), R[cidx(t - 2, u, v)], val);
+            if (t > 1) val = fma(static_cast<Real>(t - 1), R[cidx(t - 2, u, v)], val);
           } else if (u > 0) {
             val = Y * R[cidx(0, u - 1, v)];
-            if (u > 1) val = fma(static_cast<double>(u - 1), R[cidx(0, u - 2, v)], val);
+            if (u > 1) val = fma(static_cast<Real>(u - 1), R[cidx(0, u - 2, v)], val);
           } else {
             val = Z * R[cidx(0, 0, v - 1)];
-            if (v > 1) val = fma(static_cast<double>(v - 1), R[cidx(0, 0, v - 2)], val);
+            if (v > 1) val = fma(static_cast<Real>(v - 1), R[cidx(0, 0, v - 2)], val);
           }
           R[cidx(t, u, v)] = val;
         }
@@ -184,35 +184,38 @@ __host__ __device__ constexpr int cart_y(int l, int c) {
 }
 
 // One solid-harmonic term w * R[t + tau] with w a compile-time constant (the
-// term vanishes at compile time when w == 0).
-template <int LC, int M, int C>
-__device__ __forceinline__ double sph_term(const double* R, int tx, int ty, int tz) {
+// term vanishes at compile time when w == 0). Real is double, or float for the
+// FP32 recurrences of weak triplets.
+template <int LC, int M, int C, class Real>
+__device__ __forceinline__ Real sph_term(const Real* R, int tx, int ty, int tz) {
   constexpr int ax = cart_x(LC, C), ay = cart_y(LC, C), az = LC - ax - ay;
   constexpr double w = sph_raw(LC, M - LC, ax, ay, az);
   if constexpr (w != 0.0)
-    return w * R[cidx(tx + ax, ty + ay, tz + az)];
+    return static_cast<Real>(w) * R[cidx(tx + ax, ty + ay, tz + az)];
   else
-    return -0.0;  // x + (-0.0) == x exactly, so the compiler drops the term
+    return static_cast<Real>(-0.0);  // x + (-0.0) == x exactly, so the compiler drops the term
 }
 
-template <int LC, int M, int... Cs>
-__device__ __forceinline__ double sph_row(const double* R, int tx, int ty, int tz,
-                                          std::integer_sequence<int, Cs...>) {
-  return (-0.0 + ... + sph_term<LC, M, Cs>(R, tx, ty, tz));
+template <int LC, int M, class Real, int... Cs>
+__device__ __forceinline__ Real sph_row(const Real* R, int tx, int ty, int tz,
+                                        std::integer_sequence<int, Cs...>) {
+  return (static_cast<Real>(-0.0) + ... + sph_term<LC, M, Cs, Real>(R, tx, ty, tz));
 }
 
-template <int LC, int... Ms>
-__device__ __forceinline__ void sph_rows(const double* R, int tx, int ty, int tz, double* xr,
+// xr[m] += N_lc,m * sum_tau S_lc,m[tau] R[t + tau] (accumulated in FP64)
+template <int LC, class Real, int... Ms>
+__device__ __forceinline__ void sph_rows(const Real* R, int tx, int ty, int tz, double* xr,
                                          std::integer_sequence<int, Ms...>) {
   ((xr[Ms] = fma(c_sph_rownorm[LC * LC + Ms],
-                 sph_row<LC, Ms>(R, tx, ty, tz, std::make_integer_sequence<int, ncart(LC)>{}),
+                 static_cast<double>(sph_row<LC, Ms, Real>(R, tx, ty, tz,
+                                                           std::make_integer_sequence<int, ncart(LC)>{})),
                  xr[Ms])),
    ...);
 }
 
 // X rows of one triplet, per thread: rows t with t % TPT == part.
-template <int LAB, int LC, int TPT>
-__device__ __forceinline__ void x_rows_thread(const double* R, double* xrow0, int mpad, int part) {
+template <int LAB, int LC, int TPT, class Real>
+__device__ __forceinline__ void x_rows_thread(const Real* R, double* xrow0, int mpad, int part) {
 #pragma unroll
   for (int tl = 0; tl <= LAB; ++tl)
 #pragma unroll
@@ -222,14 +225,118 @@ __device__ __forceinline__ void x_rows_thread(const double* R, double* xrow0, in
         const int tz = tl - tx - ty;
         const int th = cidx(tx, ty, tz);
         if (th % TPT != part) continue;
-        sph_rows<LC>(R, tx, ty, tz, xrow0 + th * mpad, std::make_integer_sequence<int, 2 * LC + 1>{});
+        sph_rows<LC, Real>(R, tx, ty, tz, xrow0 + th * mpad, std::make_integer_sequence<int, 2 * LC + 1>{});
       }
 }
 
+// X of one triplet by one thread (L <= 5): Boys, R in registers, solid harmonics.
+template <int LAB, int LC, int NR, int MPAD, int TPT, class Real>
+__device__ __forceinline__ void x_triplet_thread(const Df3cArgs& a, double p, double X, double Y,
+                                                 double Z, int np, int po, double* xrow0, int part) {
+  constexpr int L = LAB + LC;
+  const double RPC2 = X * X + Y * Y + Z * Z;
+  for (int kp = 0; kp < np; ++kp) {
+    const double2 gp = a.X.prim[po + kp];
+    const double gam = gp.x, pg = p + gam, alpha = p * gam / pg;
+    double pref = kTwoPi52 / (p * gam * sqrt(pg)) * gp.y;
+#pragma unroll
+    for (int l = 0; l < LC; ++l) pref *= -0.5 / gam;  // (-1)^LC (2 gam)^-LC
+    Real F[L + 1];
+    boys_all(a.dt, a.boys_mode, L, alpha * RPC2, F);
+    Real Rn[L + 1];
+    double f = pref;
+#pragma unroll
+    for (int n = 0; n <= L; ++n) {
+      Rn[n] = static_cast<Real>(f) * F[n];
+      f *= -2.0 * alpha;
+    }
+    Real R[NR];
+    hermite_R_thread<L, Real>(Rn, static_cast<Real>(X), static_cast<Real>(Y), static_cast<Real>(Z), R);
+    x_rows_thread<LAB, LC, TPT, Real>(R, xrow0, MPAD, part);
+  }
+}
+
+// X of one triplet by a team of TS lanes of one warp (L > 5): orders of the
+// Boys function across lanes, R level by level in shared memory, X rows across
+// the lanes. Every lane of the warp calls this with the same Real (the caller
+// makes the precision choice warp-uniform), so the warp barriers pair up.
+template <int LAB, int LC, int TS, class Real>
+__device__ __forceinline__ void x_triplet_team(const Df3cArgs& a, const uchar4* txyz, const short4* tminus,
+                                               double* rbuf, int tl, bool active, int np, int po,
+                                               int maxprim, double p, double X, double Y, double Z,
+                                               double* xrow, int mpad) {
+  constexpr int L = LAB + LC;
+  constexpr int NR = ncum(L);
+  constexpr int NH = ncum(LAB);
+  Real* Rn = reinterpret_cast<Real*>(rbuf);
+  Real* b0 = Rn + 16;
+  Real* b1 = b0 + NR;
+  const double RPC2 = X * X + Y * Y + Z * Z;
+  const Real Xr = static_cast<Real>(X), Yr = static_cast<Real>(Y), Zr = static_cast<Real>(Z);
+  for (int kp = 0; kp < maxprim; ++kp) {
+    const bool has = active && kp < np;
+    if (has) {
+      const double2 gp = a.X.prim[po + kp];
+      const double gam = gp.x, pg = p + gam, alpha = p * gam / pg;
+      double pref = kTwoPi52 / (p * gam * sqrt(pg)) * gp.y;
+      for (int l = 0; l < LC; ++l) pref *= -0.5 / gam;
+      // orders n = tl, tl + TS, ...: a team may have fewer lanes than L + 1
+      const typename BoysAtT<Real>::type F(a.boys_mode, alpha * RPC2);
+      for (int n = tl; n <= L; n += TS) {
+        double f = pref;
+        for (int k = 0; k < n; ++k) f *= -2.0 * alpha;
+        Rn[n] = static_cast<Real>(f) * F(a.dt, n);
+      }
+    }
+    __syncwarp();
+    // Hermite R, level by level
+    {
+      Real* top = (L & 1) ? b1 : b0;
+      if (has && tl == 0) top[0] = Rn[L];
+      __syncwarp();
+      for (int n = L - 1; n >= 0; --n) {
+        Real* dst = (n & 1) ? b1 : b0;
+        const Real* src = (n & 1) ? b0 : b1;
+        const int cnt = has ? ncum(L - n) : 0;
+        for (int idx = tl; idx < cnt; idx += TS) {
+          Real v;
+          if (idx == 0) {
+            v = Rn[n];
+          } else {
+            const uchar4 e = txyz[idx];
+            const short4 mi = tminus[idx];
+            if (e.x) {
+              v = Xr * src[mi.x];
+              if (e.x > 1) v = fma(static_cast<Real>(e.x - 1), src[tminus[mi.x].x], v);
+            } else if (e.y) {
+              v = Yr * src[mi.y];
+              if (e.y > 1) v = fma(static_cast<Real>(e.y - 1), src[tminus[mi.y].y], v);
+            } else {
+              v = Zr * src[mi.z];
+              if (e.z > 1) v = fma(static_cast<Real>(e.z - 1), src[tminus[mi.z].z], v);
+            }
+          }
+          dst[idx] = v;
+        }
+        __syncwarp();
+      }
+    }
+    // X rows: lanes over the Hermite components t of the bra, compile-time
+    // solid-harmonic terms of the auxiliary shell
+    if (has) {
+      for (int t = tl; t < NH; t += TS) {
+        const uchar4 e = txyz[t];
+        sph_rows<LC, Real>(b0, e.x, e.y, e.z, xrow + t * mpad, std::make_integer_sequence<int, 2 * LC + 1>{});
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// One work item: aux tile bx (TC shells), bra-unit chunk by, density chunk bz.
 template <int LAB, int LC>
-__global__ void __launch_bounds__(kThreads, 1) k_df3c(Df3cArgs a) {
+__device__ __forceinline__ void df3c_item(const Df3cArgs& a, int bx, int by, int bz, double* smem) {
   using C = Cfg<LAB, LC>;
-  extern __shared__ __align__(16) double smem[];
   double* Xs = smem;                               // [KP][MPAD]
   double* Gs = Xs + C::KP * C::MPAD;               // [KP][kGStride]
   double* misc = Gs + C::KP * kGStride;            // unit / aux parameters
@@ -240,13 +347,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_df3c(Df3cArgs a) {
   int* c_info = reinterpret_cast<int*>(misc + 320 + 512);             // [TC] (nprim, prim_off)
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int c0 = blockIdx.x * C::TC;
+  const int c0 = bx * C::TC;
   const int tile_n = min(C::TC, a.n_aux - c0);
-  const int z = blockIdx.z;
+  const int z = bz;
   const int d0 = z * a.dw;
   const int ndc = min(a.dw, a.nd - d0);
   const int nt_rt = a.dw / 8;  // n-tiles of this launch (dw multiple of 8, <= 40)
-  const int ub = blockIdx.y * a.units_per_chunk;
+  const int ub = by * a.units_per_chunk;
   const int ue = min(a.n_units, ub + a.units_per_chunk);
 
   if (tid < C::TC) {
@@ -329,28 +436,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_df3c(Df3cArgs a) {
         const double4 up = u_pP[ui];
         const double p = up.x;
         const double X = up.y - cc.x, Y = up.z - cc.y, Z = up.w - cc.z;
-        const double RPC2 = X * X + Y * Y + Z * Z;
         const int np = c_info[2 * ci], po = c_info[2 * ci + 1];
         double* xrow0 = Xs + (ui * C::NH) * C::MPAD + ci * C::NC;
-        for (int kp = 0; kp < np; ++kp) {
-          const double2 gp = a.X.prim[po + kp];
-          const double gam = gp.x, pg = p + gam, alpha = p * gam / pg;
-          double pref = kTwoPi52 / (p * gam * sqrt(pg)) * gp.y;
-#pragma unroll
-          for (int l = 0; l < LC; ++l) pref *= -0.5 / gam;  // (-1)^LC (2 gam)^-LC
-          double F[C::L + 1];
-          boys_all(a.dt, a.boys_mode, C::L, alpha * RPC2, F);
-          double Rn[C::L + 1];
-          double f = pref;
-#pragma unroll
-          for (int n = 0; n <= C::L; ++n) {
-            Rn[n] = f * F[n];
-            f *= -2.0 * alpha;
-          }
-          double R[C::NR];
-          hermite_R_thread<C::L>(Rn, X, Y, Z, R);
-          x_rows_thread<LAB, LC, C::TPT>(R, xrow0, C::MPAD, part);
-        }
+        if (u_Q[ui] * cc.w < a.thr32)
+          x_triplet_thread<LAB, LC, C::NR, C::MPAD, C::TPT, float>(a, p, X, Y, Z, np, po, xrow0, part);
+        else
+          x_triplet_thread<LAB, LC, C::NR, C::MPAD, C::TPT, double>(a, p, X, Y, Z, np, po, xrow0, part);
       }
     } else {
       // team index tables (shared memory copies of the decoded multi-indices)
@@ -367,75 +458,22 @@ __global__ void __launch_bounds__(kThreads, 1) k_df3c(Df3cArgs a) {
       const int team = tid / C::TS, tl = tid - team * C::TS;
       const bool in_team = team < C::NTRIP;
       const int ui = in_team ? team / C::TC : 0, ci = in_team ? team - ui * C::TC : 0;
-      double* Rn = Rteam + (in_team ? team : 0) * (2 * C::NR + 16);
-      double* b0 = Rn + 16;
-      double* b1 = b0 + C::NR;
+      double* rbuf = Rteam + (in_team ? team : 0) * (2 * C::NR + 16);
       const double4 cc = c_C[ci];
       const bool active = in_team && ci < tile_n && ui < nvalid && (u_Q[ui] * cc.w >= thr);
       const double4 up = u_pP[ui];
-      const double p = up.x;
       const double X = up.y - cc.x, Y = up.z - cc.y, Z = up.w - cc.z;
-      const double RPC2 = X * X + Y * Y + Z * Z;
       const int np = active ? c_info[2 * ci] : 0, po = c_info[2 * ci + 1];
-      // Teams are warp-aligned (TS | 32): every barrier below is a warp barrier.
-      for (int kp = 0; kp < maxprim; ++kp) {
-        const bool has = active && kp < np;
-        if (has) {
-          const double2 gp = a.X.prim[po + kp];
-          const double gam = gp.x, pg = p + gam, alpha = p * gam / pg;
-          double pref = kTwoPi52 / (p * gam * sqrt(pg)) * gp.y;
-          for (int l = 0; l < LC; ++l) pref *= -0.5 / gam;
-          // orders n = tl, tl + TS, ...: a team may have fewer lanes than L + 1
-          for (int n = tl; n <= C::L; n += C::TS) {
-            double f = pref;
-            for (int k = 0; k < n; ++k) f *= -2.0 * alpha;
-            Rn[n] = f * boys_n(a.dt, a.boys_mode, n, alpha * RPC2);
-          }
-        }
-        __syncwarp();
-        // Hermite R, level by level
-        {
-          double* top = (C::L & 1) ? b1 : b0;
-          if (has && tl == 0) top[0] = Rn[C::L];
-          __syncwarp();
-          for (int n = C::L - 1; n >= 0; --n) {
-            double* dst = (n & 1) ? b1 : b0;
-            const double* src = (n & 1) ? b0 : b1;
-            const int cnt = has ? ncum(C::L - n) : 0;
-            for (int idx = tl; idx < cnt; idx += C::TS) {
-              double v;
-              if (idx == 0) {
-                v = Rn[n];
-              } else {
-                const uchar4 e = txyz[idx];
-                const short4 mi = tminus[idx];
-                if (e.x) {
-                  v = X * src[mi.x];
-                  if (e.x > 1) v = fma(static_cast<double>(e.x - 1), src[tminus[mi.x].x], v);
-                } else if (e.y) {
-                  v = Y * src[mi.y];
-                  if (e.y > 1) v = fma(static_cast<double>(e.y - 1), src[tminus[mi.y].y], v);
-                } else {
-                  v = Z * src[mi.z];
-                  if (e.z > 1) v = fma(static_cast<double>(e.z - 1), src[tminus[mi.z].z], v);
-                }
-              }
-              dst[idx] = v;
-            }
-            __syncwarp();
-          }
-        }
-        // X rows: lanes over the Hermite components t of the bra, compile-time
-        // solid-harmonic terms of the auxiliary shell
-        if (has) {
-          for (int t = tl; t < C::NH; t += C::TS) {
-            const uchar4 e = txyz[t];
-            sph_rows<LC>(b0, e.x, e.y, e.z, Xs + (ui * C::NH + t) * C::MPAD + ci * C::NC,
-                         std::make_integer_sequence<int, C::NC>{});
-          }
-        }
-        __syncwarp();
-      }
+      double* xrow = Xs + (ui * C::NH) * C::MPAD + ci * C::NC;
+      // FP32 recurrences only when every active team of the warp has a weak triplet
+      const bool weak = !active || u_Q[ui] * cc.w < a.thr32;
+      const bool f32 = __all_sync(0xffffffffu, weak) && __any_sync(0xffffffffu, active);
+      if (f32)
+        x_triplet_team<LAB, LC, C::TS, float>(a, txyz, tminus, rbuf, tl, active, np, po, maxprim, up.x, X, Y, Z,
+                                              xrow, C::MPAD);
+      else
+        x_triplet_team<LAB, LC, C::TS, double>(a, txyz, tminus, rbuf, tl, active, np, po, maxprim, up.x, X, Y,
+                                               Z, xrow, C::MPAD);
     }
     cp_async_commit_wait_all();
     __syncthreads();
@@ -461,7 +499,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_df3c(Df3cArgs a) {
   }
 
   // partial[y][fn][d]
-  double* out = a.partial + static_cast<long long>(blockIdx.y) * a.n_aux * C::NC * a.nd;
+  double* out = a.partial + static_cast<long long>(by) * a.n_aux * C::NC * a.nd;
 #pragma unroll
   for (int j = 0; j < C::MTW; ++j) {
     const int mt = warp + kWarps * j;
@@ -475,6 +513,26 @@ __global__ void __launch_bounds__(kThreads, 1) k_df3c(Df3cArgs a) {
         const int col = 8 * n + 2 * t4 + i;
         if (n < nt_rt && col < ndc) out[fn * a.nd + d0 + col] = acc[j][n][i];
       }
+  }
+}
+
+// Persistent blocks: each pulls work items from the class's counter, heaviest
+// first (items are numbered with the bra-unit chunk slowest; units and aux
+// shells are sorted by Schwarz value, so early chunks and tiles carry the most
+// surviving triplets).
+template <int LAB, int LC>
+__global__ void __launch_bounds__(kThreads, 1) k_df3c(Df3cArgs a) {
+  extern __shared__ __align__(16) double smem[];
+  __shared__ int s_item;
+  for (;;) {
+    __syncthreads();  // the previous item is done with shared memory and s_item
+    if (threadIdx.x == 0) s_item = atomicAdd(a.counter, 1);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= a.n_items) return;
+    const int bz = item % a.nbz;
+    const int r = item / a.nbz;
+    df3c_item<LAB, LC>(a, r % a.nbx, r / a.nbx, bz, smem);
   }
 }
 
@@ -504,10 +562,28 @@ template <int LAB, int LC>
 int launch_class(const Df3cArgs& a, int ny, cudaStream_t s) {
   using C = Cfg<LAB, LC>;
   const size_t smem = sizeof(double) * C::SMEM;
-  cudaFuncSetAttribute(k_df3c<LAB, LC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       static_cast<int>(smem));
-  dim3 grid((a.n_aux + C::TC - 1) / C::TC, ny, (a.nd + a.dw - 1) / a.dw);
-  k_df3c<LAB, LC><<<grid, kThreads, smem, s>>>(a);
+  // per-device cache of the occupancy (resident blocks per SM)
+  static int occ[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  if (occ[dev] == 0) {
+    cudaFuncSetAttribute(k_df3c<LAB, LC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(smem));
+    int o = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_df3c<LAB, LC>, kThreads, smem);
+    occ[dev] = o > 0 ? o : 1;
+  }
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  Df3cArgs b = a;
+  b.nbx = (a.n_aux + C::TC - 1) / C::TC;
+  b.nby = ny;
+  b.nbz = (a.nd + a.dw - 1) / a.dw;
+  b.n_items = b.nbx * b.nby * b.nbz;
+  if (b.n_items == 0) return 0;
+  const int blocks = std::min(b.n_items, sms * occ[dev]);
+  k_df3c<LAB, LC><<<blocks, kThreads, smem, s>>>(b);
   return 1;
 }
 

@@ -12,6 +12,9 @@ struct Df3cArgs {
   DeviceTables dt;
   int boys_mode = 1;
   double thresh = 0.0;
+  // triplets with Q_ab * Q_c below thr32 build X with FP32 recurrences
+  // (precision form); 0 keeps every triplet in FP64
+  double thr32 = 0.0;
   // bra units of class LAB, sorted by Schwarz value (descending)
   int unit_slot0 = 0, n_units = 0;   // global slot offset, count
   const double* unit_Q = nullptr;    // [slot]
@@ -25,6 +28,11 @@ struct Df3cArgs {
   const double* aux_Q = nullptr;     // [slot]
   int nd = 0;
   double* partial = nullptr;         // [chunk][n_aux * NC][nd]
+  // persistent scheduling (filled in by launch_df3c_class): work items are
+  // (aux tile, bra chunk, density chunk), pulled from *counter (zeroed before
+  // the launch)
+  int* counter = nullptr;
+  int n_items = 0, nbx = 0, nby = 0, nbz = 0;
 };
 
 struct Df3cReduceArgs {

@@ -235,6 +235,11 @@ struct Ctx {
   cudaEvent_t ph[5] = {};  // phase boundaries on the main stream: screen | bra | 3c | solve
   cudaStream_t stream2 = nullptr;     // metric + Cholesky + inverse, overlapped with the 3c work
   cudaEvent_t fork = nullptr, m0 = nullptr, m1 = nullptr;
+  // streams of the three-center class launches: the tail of one class overlaps
+  // the start of the next
+  static constexpr int kNs3c = 4;
+  cudaStream_t s3c[kNs3c] = {};
+  cudaEvent_t j3c[kNs3c] = {};
   int* h_info = nullptr;  // pinned
   // Stream-ordered pool of the host-buffer entry points (densities, df, R).
   // Freed blocks stay mapped in this private pool, so repeated calls of the
@@ -268,6 +273,10 @@ int current_ctx(Ctx** out, DeviceTables* dt) {
     PA_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
     PA_CUDA(cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, prio_hi));
     PA_CUDA(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
+    for (int i = 0; i < Ctx::kNs3c; ++i) {
+      PA_CUDA(cudaStreamCreateWithFlags(&c->s3c[i], cudaStreamNonBlocking));
+      PA_CUDA(cudaEventCreateWithFlags(&c->j3c[i], cudaEventDisableTiming));
+    }
     PA_CUDA(cudaEventCreate(&c->m0));
     PA_CUDA(cudaEventCreate(&c->m1));
     PA_CUDA(cudaMallocHost(&c->h_info, sizeof(int) * 4));
@@ -329,6 +338,7 @@ struct DfBuffers {
       *df_raw;
   double4 *unit_pP, *slot_pP;
   int *uvals, *sorted_unit, *avals, *sorted_aux, *info;
+  int* counters = nullptr;  // one work counter per class run
   void* cub_tmp;
   size_t cub_bytes;
   std::vector<long long> g_off;      // per Lab class
@@ -402,7 +412,7 @@ void layout_df(Carver& c, const pa_basis_s* orb, const pa_basis_s* aux, int nd, 
       df3c_class_info(lab, lc, &ci);
       const int bx = (nxc + ci.tc - 1) / ci.tc;
       const int bz = nz;
-      const int target = 2 * 148;
+      const int target = 4 * 148;  // work items per class (persistent blocks pull them)
       int ny = std::max(1, (target + bx * bz - 1) / (bx * bz));
       const int max_ny = (nu + ci.ub - 1) / ci.ub;
       ny = std::min(ny, max_ny);
@@ -415,6 +425,7 @@ void layout_df(Carver& c, const pa_basis_s* orb, const pa_basis_s* aux, int nd, 
     }
   }
   double* part = c.take<double>(part_total);
+  b->counters = c.take<int>(std::max<size_t>(b->runs.size(), 1));
   size_t off = 0;
   for (auto& r : b->runs) {
     const int nxc = X.class_off[r.lc + 1] - X.class_off[r.lc];
@@ -518,13 +529,19 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
   cudaEventRecord(ph[1], s);
   // three-center contraction
   const int before3c = *launches;
-  if (nd > 0) {
+  if (nd > 0 && !b.runs.empty()) {
+    PA_CUDA(cudaMemsetAsync(b.counters, 0, sizeof(int) * b.runs.size(), s));
+    PA_CUDA(cudaEventRecord(ctx->fork, s));
+    for (int i = 0; i < Ctx::kNs3c; ++i) PA_CUDA(cudaStreamWaitEvent(ctx->s3c[i], ctx->fork, 0));
+    int ri = 0;
     for (const auto& r : b.runs) {
+      const int run_index = ri++;
       Df3cArgs a;
       a.X = aux->dev;
       a.dt = dt;
       a.boys_mode = o.boys_mode;
       a.thresh = o.screen_thresh;
+      a.thr32 = o.precision == PA_PRECISION_MIXED ? o.fp32_thresh : 0.0;
       a.unit_slot0 = P.class_off[r.lab];
       a.n_units = P.class_off[r.lab + 1] - P.class_off[r.lab];
       a.unit_Q = b.slot_Q;
@@ -538,7 +555,12 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
       a.aux_Q = b.aux_Q;
       a.nd = nd;
       a.partial = r.partial;
-      *launches += launch_df3c_class(r.lab, r.lc, a, r.ny, s);
+      a.counter = b.counters + run_index;
+      *launches += launch_df3c_class(r.lab, r.lc, a, r.ny, ctx->s3c[run_index % Ctx::kNs3c]);
+    }
+    for (int i = 0; i < Ctx::kNs3c; ++i) {
+      PA_CUDA(cudaEventRecord(ctx->j3c[i], ctx->s3c[i]));
+      PA_CUDA(cudaStreamWaitEvent(s, ctx->j3c[i], 0));
     }
     for (int lc = 0; lc <= X.lc_max; ++lc) {
       Df3cReduceArgs ra;
@@ -966,6 +988,20 @@ int pa_set_screen_threshold(double thresh) {
   std::lock_guard<std::mutex> lk(g_opt_mu);
   g_opts.screen_thresh = thresh;
   return PA_OK;
+}
+
+int pa_set_precision(int mode, double fp32_thresh) {
+  if (mode != PA_PRECISION_FP64 && mode != PA_PRECISION_MIXED) return fail(PA_ERR_ARG, "unknown precision mode");
+  if (!(fp32_thresh >= 0.0) || !std::isfinite(fp32_thresh)) return fail(PA_ERR_ARG, "FP32 threshold must be finite and >= 0");
+  std::lock_guard<std::mutex> lk(g_opt_mu);
+  g_opts.precision = mode;
+  g_opts.fp32_thresh = fp32_thresh;
+  return PA_OK;
+}
+
+int pa_get_precision(void) {
+  std::lock_guard<std::mutex> lk(g_opt_mu);
+  return g_opts.precision;
 }
 
 int pa_set_metric_shift(double shift) {

@@ -73,6 +73,8 @@ struct Options {
   int verbose = 0;
   int skip_metric = 0;
   double metric_shift = 0.0;  // added to the diagonal of (P|Q) before the Cholesky
+  int precision = 0;          // 0 = FP64 throughout, 1 = mixed (FP32 recurrences for weak triplets)
+  double fp32_thresh = 1e-6;  // Schwarz bound below which the mixed form uses FP32
 };
 
 struct Stats {

@@ -25,6 +25,8 @@ PA_ERR_SCRATCH = 7
 
 PA_BOYS_EXACT = 0
 PA_BOYS_REFERENCE = 1
+PA_PRECISION_FP64 = 0
+PA_PRECISION_MIXED = 1
 PA_LAYOUT_FORTRAN = 0
 PA_LAYOUT_C = 1
 PA_LMAX_ORBITAL = 4
@@ -87,6 +89,8 @@ SIGNATURES = {
     "pa_set_screen_threshold": [_d],
     "pa_set_skip_metric": [_i],
     "pa_set_metric_shift": [_d],
+    "pa_set_precision": [_i, _d],
+    "pa_get_precision": [],
     "pa_get_stats": [ctypes.POINTER(PaStats)],
     "pa_basis_create": [_i, _i, _pi, _pi, _pd, _i, ctypes.POINTER(_vp)],
     "pa_basis_destroy": [_vp],
@@ -164,6 +168,17 @@ def get_boys_mode():
 
 def set_screen_threshold(thresh):
     check(load().pa_set_screen_threshold(float(thresh)))
+
+
+def set_precision(mode="fp64", fp32_thresh=1e-6):
+    """'fp64' (default) or 'mixed': FP32 recurrences for shell triplets whose
+    Schwarz bound is below fp32_thresh."""
+    code = {"fp64": PA_PRECISION_FP64, "mixed": PA_PRECISION_MIXED}.get(mode, mode)
+    check(load().pa_set_precision(int(code), float(fp32_thresh)))
+
+
+def get_precision():
+    return {PA_PRECISION_FP64: "fp64", PA_PRECISION_MIXED: "mixed"}[load().pa_get_precision()]
 
 
 def set_metric_shift(shift):
