@@ -17,7 +17,7 @@
 // tile, and individual triplets below the threshold contribute exactly zero, as
 // the reference skips them (schwarz_estimate < 1e-10 -> cycle).
 //
-// A block (8 warps) owns a tile of TC auxiliary shells and a density chunk of
+// A block (8 warps; two blocks per SM) owns a tile of TC auxiliary shells and a density chunk of
 // up to 40 columns, and walks a range of bra units, UB units per step:
 //   1. cp.async stages G of the UB units (one contiguous range) into shared
 //      memory while
@@ -47,7 +47,7 @@ struct BlockSync {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kSmemBudget = 200 * 1024 / 8;  // doubles
+constexpr int kSmemBudget = 110 * 1024 / 8;  // doubles (two blocks per SM)
 constexpr int kGStride = 44;                 // shared-memory row stride of G (>= 40, = 4 mod 16)
 
 __constant__ double c_sph_dense[1024];  // solid harmonics, row (l, m) at c_sph_off[l] + m * ncart(l)
@@ -521,7 +521,7 @@ __device__ __forceinline__ void df3c_item(const Df3cArgs& a, int bx, int by, int
 // shells are sorted by Schwarz value, so early chunks and tiles carry the most
 // surviving triplets).
 template <int LAB, int LC>
-__global__ void __launch_bounds__(kThreads, 1) k_df3c(Df3cArgs a) {
+__global__ void __launch_bounds__(kThreads, 2) k_df3c(Df3cArgs a) {
   extern __shared__ __align__(16) double smem[];
   __shared__ int s_item;
   for (;;) {
