@@ -174,6 +174,21 @@ int pa_df_2d(pa_basis orbital, pa_basis aux, int ndens, int nbf, const double* d
 /* Coulomb tensor (nstates^4, column-major) from device densities. */
 int pa_df_4d(pa_basis orbital, pa_basis aux, int ndens, int nbf, const double* d_densities,
              int layout, int nstates, double* d_coulomb, void* stream);
+/* Batched form: the Coulomb tensors of nmol molecules in one call. Molecule m
+ * has the bases orbital[m] / aux[m], ndens[m] = nstates[m] (nstates[m] + 1) / 2
+ * device densities d_densities[m] (in `layout`) and the device output
+ * d_coulomb[m] (nstates[m]^4, column-major). Every molecule's screening,
+ * density folding and metric chain run concurrently; the three-center work of
+ * all molecules runs as one persistent launch per shell-triplet class, fed by
+ * the class's queue of work items (molecules by decreasing work, each heavy
+ * first). With use_graph = 1 the whole sequence is recorded once as a CUDA
+ * graph and replayed by later calls with the same handles, sizes, pointers and
+ * options (the last batch is kept per device). Synchronous: returns after the
+ * tensors are complete; work already queued on `stream` is waited for first. */
+int pa_df_4d_batch(int nmol, const pa_basis* orbital, const pa_basis* aux, const int* ndens,
+                   const double* const* d_densities, int layout, const int* nstates,
+                   double* const* d_coulomb, int use_graph, void* stream);
+
 /* Host-buffer variants of f_contract_coulomb_densities_{2d,4d} with an explicit
  * density layout (PA_LAYOUT_C avoids a transposed host copy). */
 int pa_contract_coulomb_densities_2d(pa_basis orbital, pa_basis aux, int ndens, int nbf,

@@ -536,6 +536,54 @@ __global__ void __launch_bounds__(kThreads, 2) k_df3c(Df3cArgs a) {
   }
 }
 
+// Batched form: the work items of one class for many molecules in one
+// persistent launch. Molecule m owns items [item_off[m], item_off[m + 1]) and
+// its own descriptor args[m]; molecules are ordered by decreasing work, and a
+// molecule's items heavy-first, so the queue drains with light items last.
+template <int LAB, int LC>
+__global__ void __launch_bounds__(kThreads, 2) k_df3c_batch(const Df3cArgs* __restrict__ args,
+                                                            const int* __restrict__ item_off, int nm,
+                                                            int* counter) {
+  extern __shared__ __align__(16) double smem[];
+  __shared__ int s_item, s_m;
+  __shared__ __align__(16) unsigned char s_raw[sizeof(Df3cArgs)];
+  const Df3cArgs& sa = *reinterpret_cast<const Df3cArgs*>(s_raw);
+  const int total = item_off[nm];
+  for (;;) {
+    __syncthreads();  // the previous item is done with shared memory and the descriptor
+    if (threadIdx.x == 0) {
+      const int item = atomicAdd(counter, 1);
+      int m = 0;
+      if (item < total) {
+        int lo = 0, hi = nm - 1;  // last m with item_off[m] <= item
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) / 2;
+          if (item_off[mid] <= item)
+            lo = mid;
+          else
+            hi = mid - 1;
+        }
+        m = lo;
+      }
+      s_item = item;
+      s_m = m;
+    }
+    __syncthreads();
+    const int item = s_item;
+    if (item >= total) return;
+    const int m = s_m;
+    static_assert(sizeof(Df3cArgs) % 4 == 0, "descriptor copied in 32-bit words");
+    const unsigned* src = reinterpret_cast<const unsigned*>(args + m);
+    unsigned* dst = reinterpret_cast<unsigned*>(s_raw);
+    for (int i = threadIdx.x; i < static_cast<int>(sizeof(Df3cArgs) / 4); i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+    const int local = item - item_off[m];
+    const int bz = local % sa.nbz;
+    const int r = local / sa.nbz;
+    df3c_item<LAB, LC>(sa, r % sa.nbx, r / sa.nbx, bz, smem);
+  }
+}
+
 // df_raw[sph_off(P) + m][d] (column-major, naux rows) = sum over LAB classes and
 // bra chunks of the partial slabs of class LC.
 __global__ void k_df3c_reduce(Df3cReduceArgs r) {
@@ -558,32 +606,56 @@ __global__ void k_df3c_reduce(Df3cReduceArgs r) {
   }
 }
 
+// Resident blocks of a kernel on the current device (cached per device and
+// kernel), after raising its dynamic shared-memory limit to smem.
+template <class K>
+int resident_blocks(K kernel, size_t smem, int* occ_cache) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) dev = 0;
+  if (occ_cache[dev] == 0) {
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    int o = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kernel, kThreads, smem);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    occ_cache[dev] = (o > 0 ? o : 1) * sms;
+  }
+  return occ_cache[dev];
+}
+
+template <int LAB, int LC>
+void fill_items(Df3cArgs* a, int ny) {
+  using C = Cfg<LAB, LC>;
+  a->nbx = (a->n_aux + C::TC - 1) / C::TC;
+  a->nby = ny;
+  a->nbz = (a->nd + a->dw - 1) / a->dw;
+  a->n_items = a->nbx * a->nby * a->nbz;
+}
+
 template <int LAB, int LC>
 int launch_class(const Df3cArgs& a, int ny, cudaStream_t s) {
   using C = Cfg<LAB, LC>;
   const size_t smem = sizeof(double) * C::SMEM;
-  // per-device cache of the occupancy (resident blocks per SM)
   static int occ[64] = {};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 0 || dev >= 64) dev = 0;
-  if (occ[dev] == 0) {
-    cudaFuncSetAttribute(k_df3c<LAB, LC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         static_cast<int>(smem));
-    int o = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_df3c<LAB, LC>, kThreads, smem);
-    occ[dev] = o > 0 ? o : 1;
-  }
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int resident = resident_blocks(k_df3c<LAB, LC>, smem, occ);
   Df3cArgs b = a;
-  b.nbx = (a.n_aux + C::TC - 1) / C::TC;
-  b.nby = ny;
-  b.nbz = (a.nd + a.dw - 1) / a.dw;
-  b.n_items = b.nbx * b.nby * b.nbz;
+  fill_items<LAB, LC>(&b, ny);
   if (b.n_items == 0) return 0;
-  const int blocks = std::min(b.n_items, sms * occ[dev]);
-  k_df3c<LAB, LC><<<blocks, kThreads, smem, s>>>(b);
+  k_df3c<LAB, LC><<<std::min(b.n_items, resident), kThreads, smem, s>>>(b);
+  return 1;
+}
+
+template <int LAB, int LC>
+int launch_class_batch(const Df3cArgs* d_args, const int* d_item_off, int nm, int total_items,
+                       int* counter, cudaStream_t s) {
+  using C = Cfg<LAB, LC>;
+  const size_t smem = sizeof(double) * C::SMEM;
+  static int occ[64] = {};
+  const int resident = resident_blocks(k_df3c_batch<LAB, LC>, smem, occ);
+  if (total_items <= 0 || nm <= 0) return 0;
+  k_df3c_batch<LAB, LC><<<std::min(total_items, resident), kThreads, smem, s>>>(d_args, d_item_off, nm,
+                                                                                 counter);
   return 1;
 }
 
@@ -598,6 +670,8 @@ void class_info(Df3cClassInfo* ci) {
 
 using LaunchFn = int (*)(const Df3cArgs&, int, cudaStream_t);
 using InfoFn = void (*)(Df3cClassInfo*);
+using FillFn = void (*)(Df3cArgs*, int);
+using BatchFn = int (*)(const Df3cArgs*, const int*, int, int, int*, cudaStream_t);
 
 #define PA_ROW(LAB)                                                                    \
   {&launch_class<LAB, 0>, &launch_class<LAB, 1>, &launch_class<LAB, 2>, &launch_class<LAB, 3>, \
@@ -611,6 +685,18 @@ const LaunchFn kLaunch[2 * PA_LMAX + 1][PA_LAUXMAX + 1] = {
 const InfoFn kInfo[2 * PA_LMAX + 1][PA_LAUXMAX + 1] = {
     PA_IROW(0), PA_IROW(1), PA_IROW(2), PA_IROW(3), PA_IROW(4),
     PA_IROW(5), PA_IROW(6), PA_IROW(7), PA_IROW(8)};
+#define PA_FROW(LAB)                                                                            \
+  {&fill_items<LAB, 0>, &fill_items<LAB, 1>, &fill_items<LAB, 2>, &fill_items<LAB, 3>,             \
+   &fill_items<LAB, 4>, &fill_items<LAB, 5>}
+const FillFn kFill[2 * PA_LMAX + 1][PA_LAUXMAX + 1] = {
+    PA_FROW(0), PA_FROW(1), PA_FROW(2), PA_FROW(3), PA_FROW(4),
+    PA_FROW(5), PA_FROW(6), PA_FROW(7), PA_FROW(8)};
+#define PA_BROW(LAB)                                                                            \
+  {&launch_class_batch<LAB, 0>, &launch_class_batch<LAB, 1>, &launch_class_batch<LAB, 2>,          \
+   &launch_class_batch<LAB, 3>, &launch_class_batch<LAB, 4>, &launch_class_batch<LAB, 5>}
+const BatchFn kBatch[2 * PA_LMAX + 1][PA_LAUXMAX + 1] = {
+    PA_BROW(0), PA_BROW(1), PA_BROW(2), PA_BROW(3), PA_BROW(4),
+    PA_BROW(5), PA_BROW(6), PA_BROW(7), PA_BROW(8)};
 
 }  // namespace
 
@@ -618,6 +704,13 @@ void df3c_class_info(int lab, int lc, Df3cClassInfo* ci) { kInfo[lab][lc](ci); }
 
 int launch_df3c_class(int lab, int lc, const Df3cArgs& a, int ny, cudaStream_t s) {
   return kLaunch[lab][lc](a, ny, s);
+}
+
+void df3c_fill_items(int lab, int lc, Df3cArgs* a, int ny) { kFill[lab][lc](a, ny); }
+
+int launch_df3c_class_batch(int lab, int lc, const Df3cArgs* d_args, const int* d_item_off, int nm,
+                            int total_items, int* counter, cudaStream_t s) {
+  return kBatch[lab][lc](d_args, d_item_off, nm, total_items, counter, s);
 }
 
 int launch_df3c_reduce(const Df3cReduceArgs& r, cudaStream_t s) {

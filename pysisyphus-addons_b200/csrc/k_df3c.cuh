@@ -52,6 +52,12 @@ struct Df3cClassInfo {
 
 void df3c_class_info(int lab, int lc, Df3cClassInfo* ci);
 int launch_df3c_class(int lab, int lc, const Df3cArgs& a, int ny, cudaStream_t s);
+// Fills a->nbx, nby, nbz and n_items of one class run (host side).
+void df3c_fill_items(int lab, int lc, Df3cArgs* a, int ny);
+// One persistent launch of class (lab, lc) over the runs of nm molecules:
+// d_args[m] (device) with items [d_item_off[m], d_item_off[m + 1]).
+int launch_df3c_class_batch(int lab, int lc, const Df3cArgs* d_args, const int* d_item_off, int nm,
+                            int total_items, int* counter, cudaStream_t s);
 int launch_df3c_reduce(const Df3cReduceArgs& r, cudaStream_t s);
 cudaError_t upload_sph_dense(const double* vals, int n, const int* offs, const double* rownorm,
                              cudaStream_t s);

@@ -1,8 +1,9 @@
 // Dense FP64 linear algebra of the density-fitting path (column-major):
 //  * blocked right-looking Cholesky of the metric, lower triangle
 //    (replaces dpotrf("L"), common/linalg.f90:78); each 64 x 64 diagonal block is
-//    factorized and inverted by one thread block, the panel below it is
-//    scaled in place and the trailing matrix updated by a lower GEMM;
+//    factorized (and inverted, for the later solves) by one thread block, the
+//    panel below it solved against it in place and the trailing matrix updated
+//    by a lower GEMM;
 //  * L^-1 df as a blocked forward substitution on the density columns, using
 //    the inverted diagonal blocks (replaces dtrtri("L","N"), common/linalg.f90:81,
 //    followed by dtrmm("L","L","N","N"), diabatization/intor.f90:198: the
@@ -118,44 +119,36 @@ __global__ void __launch_bounds__(256) k_potrf_diag_inv(double* A, long long lda
 }
 
 // Panel below the diagonal block (rows j0 + NB.., columns j0..j0 + nb):
-// P := P Dinv^T in place. One block per 64 rows; the whole row slice is read
-// into shared memory before it is overwritten.
-__global__ void __launch_bounds__(256) k_panel_inplace(double* A, long long lda, int j0, int nb,
-                                                       int rows, const double* __restrict__ dinv) {
+// P := P L11^-T in place, by forward substitution against the factored
+// diagonal block L11 (what dtrsm does inside dpotrf). Multiplying by the
+// explicit inverse of L11 instead loses accuracy on the ill-conditioned
+// blocks of a nearly singular metric. One block of 64 threads per 64 rows;
+// thread r solves row r: x_j = (p_j - sum_(k<j) L_jk x_k) / L_jj.
+__global__ void __launch_bounds__(NB) k_panel_inplace(double* A, long long lda, int j0, int nb,
+                                                      int rows) {
   extern __shared__ double psm[];
-  double(*P)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(psm);           // [row][p]
-  double(*D)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(psm + NB * (NB + 1));  // [j][p]
+  double(*P)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(psm);                   // [row][p]
+  double(*Ls)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(psm + NB * (NB + 1));  // [j][k]
   const int tid = threadIdx.x;
   const int i0 = blockIdx.x * NB;
   double* base = A + (j0 + nb) + lda * j0;
-#pragma unroll
-  for (int idx = tid; idx < NB * NB; idx += 256) {
-    const int i = idx & (NB - 1), p = idx >> 6;
-    P[i][p] = (i0 + i < rows && p < nb) ? base[(i0 + i) + lda * p] : 0.0;
-    D[i][p] = dinv[i + NB * p];
+  for (int idx = tid; idx < NB * NB; idx += NB) {
+    const int i = idx & (NB - 1), c = idx >> 6;
+    P[i][c] = (i0 + i < rows && c < nb) ? base[(i0 + i) + lda * c] : 0.0;
+    Ls[i][c] = (i < nb && c <= i) ? A[(j0 + i) + lda * (j0 + c)] : 0.0;
   }
   __syncthreads();
-  const int tx = tid & 15, ty = tid >> 4;
-  double acc[4][4] = {};
-  for (int p = 0; p < NB; ++p) {
-    double x[4], y[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      x[u] = P[tx + 16 * u][p];
-      y[u] = D[ty + 16 * u][p];
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-#pragma unroll
-      for (int v = 0; v < 4; ++v) acc[u][v] = fma(x[u], y[v], acc[u][v]);
+  const int r = tid;
+  for (int j = 0; j < nb; ++j) {
+    double v = P[r][j];
+    for (int k = 0; k < j; ++k) v = fma(-Ls[j][k], P[r][k], v);
+    P[r][j] = v / Ls[j][j];
   }
-#pragma unroll
-  for (int u = 0; u < 4; ++u)
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-      const int i = i0 + tx + 16 * u, j = ty + 16 * v;
-      if (i < rows && j < nb) base[i + lda * j] = acc[u][v];
-    }
+  __syncthreads();
+  for (int idx = tid; idx < NB * NB; idx += NB) {
+    const int i = idx & (NB - 1), c = idx >> 6;
+    if (i0 + i < rows && c < nb) base[(i0 + i) + lda * c] = P[i][c];
+  }
 }
 
 // One step k of the blocked forward substitution B := L^-1 B (right-looking).
@@ -369,7 +362,7 @@ int cholesky_lower(double* A, int n, int* d_info, double* work, cudaStream_t s) 
     ++launches;
     const int rest = n - j0 - nb;
     if (rest > 0) {
-      k_panel_inplace<<<(rest + NB - 1) / NB, 256, 2 * kTileSmem, s>>>(A, n, j0, nb, rest, Db);
+      k_panel_inplace<<<(rest + NB - 1) / NB, NB, 2 * kTileSmem, s>>>(A, n, j0, nb, rest);
       double* P = A + (j0 + nb) + static_cast<long long>(n) * j0;
       double* A22 = A + (j0 + nb) + static_cast<long long>(n) * (j0 + nb);
       launches += 1 + gemm_impl(false, true, rest, rest, nb, -1.0, P, n, P, n, 1.0, A22, n, true,

@@ -12,6 +12,7 @@
 #include <cub/device/device_segmented_radix_sort.cuh>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -203,6 +204,7 @@ cudaError_t Arena::reserve(size_t bytes) {
 // Opaque basis handle.
 struct pa_basis_s {
   int device = 0;
+  long long serial = 0;  // unique per handle in the process
   pa::HostBasis host;
   pa::PairLists pairs;
   pa::AuxLists aux;
@@ -246,6 +248,10 @@ struct Ctx {
   // same size do not map device memory again; the device's default pool and
   // other allocators in the process are untouched.
   cudaMemPool_t pool = nullptr;
+  // batched form: metric chains of different molecules on their own streams
+  cudaStream_t smet[kNs3c] = {};
+  cudaEvent_t jmet[kNs3c] = {};
+  struct BatchPlan* plan = nullptr;  // the last batch, kept for replay
 };
 
 std::mutex g_ctx_mu;
@@ -276,6 +282,8 @@ int current_ctx(Ctx** out, DeviceTables* dt) {
     for (int i = 0; i < Ctx::kNs3c; ++i) {
       PA_CUDA(cudaStreamCreateWithFlags(&c->s3c[i], cudaStreamNonBlocking));
       PA_CUDA(cudaEventCreateWithFlags(&c->j3c[i], cudaEventDisableTiming));
+      PA_CUDA(cudaStreamCreateWithPriority(&c->smet[i], cudaStreamNonBlocking, prio_hi));
+      PA_CUDA(cudaEventCreateWithFlags(&c->jmet[i], cudaEventDisableTiming));
     }
     PA_CUDA(cudaEventCreate(&c->m0));
     PA_CUDA(cudaEventCreate(&c->m1));
@@ -481,30 +489,25 @@ int run_screening(const pa_basis_s* orb, const pa_basis_s* aux, const DeviceTabl
   return PA_OK;
 }
 
-// df[naux, nd] (column-major) = L^-1 sum (ab|P) Dsym, into d_df.
-int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d_dens,
-           long long sd, long long si, long long sj, double* d_df, DfBuffers& b,
-           const DeviceTables& dt, const Options& o, cudaStream_t s, int* launches,
-           Ctx* ctx, int* launches_3c) {
-  const PairLists& P = orb->pairs;
-  const AuxLists& X = aux->aux;
+// ---------------------------------------------------------------------------
+// Stages of one density-fitting run, shared by the single-molecule path
+// (run_df) and the batched path (pa_df_4d_batch).
+
+// (P|Q) [+ shift], its Cholesky factor and the inverted diagonal blocks.
+void stage_metric(const pa_basis_s* aux, DfBuffers& b, const DeviceTables& dt, const Options& o,
+                  cudaStream_t s2, int* launches) {
   const int naux = aux->host.nsph;
-  cudaEvent_t* ph = ctx->ph;
-  // metric (P|Q), its Cholesky factor and L^-1 on the second stream: independent
-  // of everything until the final L^-1 df
-  cudaStream_t s2 = ctx->stream2;
-  cudaEventRecord(ctx->fork, s);
-  cudaStreamWaitEvent(s2, ctx->fork, 0);
-  cudaEventRecord(ctx->m0, s2);
   *launches += launch_metric(aux->dev, dt, o.boys_mode, b.M, s2);
   *launches += add_diagonal(b.M, naux, o.metric_shift, s2);
   *launches += cholesky_lower(b.M, naux, b.info, b.lawork, s2);
-  cudaEventRecord(ctx->m1, s2);
-  int st = run_screening(orb, aux, dt, o, b, s, launches);
-  if (st != PA_OK) return st;
-  cudaEventRecord(ph[0], s);
+}
+
+// Density folding of the sorted bra units, per L_ab class.
+void stage_bra_prep(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d_dens,
+                    long long sd, long long si, long long sj, DfBuffers& b, const Options& o,
+                    cudaStream_t s, int* launches) {
+  const PairLists& P = orb->pairs;
   UnitArrays U = unit_arrays(orb, b);
-  // density folding per bra class
   for (int lab = 0; lab <= P.lab_max; ++lab) {
     BraPrepArgs a;
     a.slot0 = P.class_off[lab];
@@ -526,8 +529,92 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
     a.n_class = a.slot_end - a.slot0;
     *launches += launch_bra_prep(orb->dev, orb->d_pair_ab, U, a, lab, s);
   }
-  cudaEventRecord(ph[1], s);
-  // three-center contraction
+}
+
+// Kernel arguments of one (L_ab, L_c) class run.
+Df3cArgs class_args(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const DfBuffers& b,
+                    const DeviceTables& dt, const Options& o, const DfBuffers::ClassRun& r) {
+  const PairLists& P = orb->pairs;
+  const AuxLists& X = aux->aux;
+  Df3cArgs a;
+  a.X = aux->dev;
+  a.dt = dt;
+  a.boys_mode = o.boys_mode;
+  a.thresh = o.screen_thresh;
+  a.thr32 = o.precision == PA_PRECISION_MIXED ? o.fp32_thresh : 0.0;
+  a.unit_slot0 = P.class_off[r.lab];
+  a.n_units = P.class_off[r.lab + 1] - P.class_off[r.lab];
+  a.unit_Q = b.slot_Q;
+  a.slot_pP = b.slot_pP;
+  a.G = b.G + b.g_off[r.lab];
+  a.dw = b.dw;
+  a.units_per_chunk = r.upc;
+  a.aux_slot0 = X.class_off[r.lc];
+  a.n_aux = X.class_off[r.lc + 1] - X.class_off[r.lc];
+  a.sorted_aux = b.sorted_aux;
+  a.aux_Q = b.aux_Q;
+  a.nd = nd;
+  a.partial = r.partial;
+  return a;
+}
+
+// Ordered sum of the partial slabs into df_raw.
+void stage_reduce(const pa_basis_s* aux, int nd, DfBuffers& b, cudaStream_t s, int* launches) {
+  const AuxLists& X = aux->aux;
+  for (int lc = 0; lc <= X.lc_max && nd > 0; ++lc) {
+    Df3cReduceArgs ra;
+    ra.X = aux->dev;
+    ra.aux_slot0 = X.class_off[lc];
+    ra.n_aux = X.class_off[lc + 1] - X.class_off[lc];
+    if (ra.n_aux == 0) continue;
+    ra.nc = 2 * lc + 1;
+    ra.nd = nd;
+    ra.naux = aux->host.nsph;
+    ra.sorted_aux = b.sorted_aux;
+    ra.nclasses = 0;
+    for (const auto& r : b.runs)
+      if (r.lc == lc) {
+        ra.part[ra.nclasses] = r.partial;
+        ra.ny[ra.nclasses] = r.ny;
+        ++ra.nclasses;
+      }
+    ra.df = b.df_raw;
+    *launches += launch_df3c_reduce(ra, s);
+  }
+}
+
+// d_df = L^-1 df_raw (or df_raw itself when the metric is skipped).
+int stage_solve(const pa_basis_s* aux, int nd, DfBuffers& b, const Options& o, double* d_df,
+                cudaStream_t s, int* launches) {
+  const int naux = aux->host.nsph;
+  if (nd <= 0) return PA_OK;
+  if (o.skip_metric)
+    PA_CUDA(cudaMemcpyAsync(d_df, b.df_raw, sizeof(double) * naux * nd, cudaMemcpyDeviceToDevice, s));
+  else
+    *launches += trsm_lower_left(b.M, naux, b.lawork, b.df_raw, naux, nd, d_df, naux, s);
+  return PA_OK;
+}
+
+// df[naux, nd] (column-major) = L^-1 sum (ab|P) Dsym, into d_df.
+int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d_dens,
+           long long sd, long long si, long long sj, double* d_df, DfBuffers& b,
+           const DeviceTables& dt, const Options& o, cudaStream_t s, int* launches,
+           Ctx* ctx, int* launches_3c) {
+  cudaEvent_t* ph = ctx->ph;
+  // metric (P|Q), its Cholesky factor and L^-1 on the second stream: independent
+  // of everything until the final L^-1 df
+  cudaStream_t s2 = ctx->stream2;
+  PA_CUDA(cudaEventRecord(ctx->fork, s));
+  PA_CUDA(cudaStreamWaitEvent(s2, ctx->fork, 0));
+  PA_CUDA(cudaEventRecord(ctx->m0, s2));
+  stage_metric(aux, b, dt, o, s2, launches);
+  PA_CUDA(cudaEventRecord(ctx->m1, s2));
+  int st = run_screening(orb, aux, dt, o, b, s, launches);
+  if (st != PA_OK) return st;
+  PA_CUDA(cudaEventRecord(ph[0], s));
+  stage_bra_prep(orb, aux, nd, d_dens, sd, si, sj, b, o, s, launches);
+  PA_CUDA(cudaEventRecord(ph[1], s));
+  // three-center contraction: one persistent launch per class, on four streams
   const int before3c = *launches;
   if (nd > 0 && !b.runs.empty()) {
     PA_CUDA(cudaMemsetAsync(b.counters, 0, sizeof(int) * b.runs.size(), s));
@@ -536,25 +623,7 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
     int ri = 0;
     for (const auto& r : b.runs) {
       const int run_index = ri++;
-      Df3cArgs a;
-      a.X = aux->dev;
-      a.dt = dt;
-      a.boys_mode = o.boys_mode;
-      a.thresh = o.screen_thresh;
-      a.thr32 = o.precision == PA_PRECISION_MIXED ? o.fp32_thresh : 0.0;
-      a.unit_slot0 = P.class_off[r.lab];
-      a.n_units = P.class_off[r.lab + 1] - P.class_off[r.lab];
-      a.unit_Q = b.slot_Q;
-      a.slot_pP = b.slot_pP;
-      a.G = b.G + b.g_off[r.lab];
-      a.dw = b.dw;
-      a.units_per_chunk = r.upc;
-      a.aux_slot0 = X.class_off[r.lc];
-      a.n_aux = X.class_off[r.lc + 1] - X.class_off[r.lc];
-      a.sorted_aux = b.sorted_aux;
-      a.aux_Q = b.aux_Q;
-      a.nd = nd;
-      a.partial = r.partial;
+      Df3cArgs a = class_args(orb, aux, nd, b, dt, o, r);
       a.counter = b.counters + run_index;
       *launches += launch_df3c_class(r.lab, r.lc, a, r.ny, ctx->s3c[run_index % Ctx::kNs3c]);
     }
@@ -562,37 +631,12 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
       PA_CUDA(cudaEventRecord(ctx->j3c[i], ctx->s3c[i]));
       PA_CUDA(cudaStreamWaitEvent(s, ctx->j3c[i], 0));
     }
-    for (int lc = 0; lc <= X.lc_max; ++lc) {
-      Df3cReduceArgs ra;
-      ra.X = aux->dev;
-      ra.aux_slot0 = X.class_off[lc];
-      ra.n_aux = X.class_off[lc + 1] - X.class_off[lc];
-      if (ra.n_aux == 0) continue;
-      ra.nc = 2 * lc + 1;
-      ra.nd = nd;
-      ra.naux = naux;
-      ra.sorted_aux = b.sorted_aux;
-      ra.nclasses = 0;
-      for (const auto& r : b.runs)
-        if (r.lc == lc) {
-          ra.part[ra.nclasses] = r.partial;
-          ra.ny[ra.nclasses] = r.ny;
-          ++ra.nclasses;
-        }
-      ra.df = b.df_raw;
-      *launches += launch_df3c_reduce(ra, s);
-    }
+    stage_reduce(aux, nd, b, s, launches);
   }
   *launches_3c = *launches - before3c;
-  cudaEventRecord(ph[2], s);
-  cudaStreamWaitEvent(s, ctx->m1, 0);  // join the metric stream
-  if (nd > 0) {
-    if (o.skip_metric)
-      cudaMemcpyAsync(d_df, b.df_raw, sizeof(double) * naux * nd, cudaMemcpyDeviceToDevice, s);
-    else
-      *launches += trsm_lower_left(b.M, naux, b.lawork, b.df_raw, naux, nd, d_df, naux, s);
-  }
-  return PA_OK;
+  PA_CUDA(cudaEventRecord(ph[2], s));
+  PA_CUDA(cudaStreamWaitEvent(s, ctx->m1, 0));  // join the metric stream
+  return stage_solve(aux, nd, b, o, d_df, s, launches);
 }
 
 int finish(Ctx* c, const DfBuffers& b, cudaStream_t s, int launches, float* ms) {
@@ -723,6 +767,309 @@ int df_device(pa_basis orb, pa_basis aux, int ndens, int nbf, const double* d_de
   g_stats.nskipped = -1;
   g_stats.nints = -1;
   return finish(c, b, s, launches, &ms);
+}
+
+// ---------------------------------------------------------------------------
+// Batched form: the Coulomb tensors of many molecules in one sequence --
+// every molecule's screening, density folding and metric chain, then one
+// persistent launch per shell-triplet class over the work items of all
+// molecules, then the reductions, solves and tensors -- recorded once as a
+// CUDA graph and replayed while the batch (handles, sizes, pointers and
+// options) stays the same.
+struct BatchPlan {
+  std::vector<long long> sig;
+  char* dmem = nullptr;
+  std::vector<DfBuffers> bufs;
+  std::vector<double*> df, gram;
+  int* infos = nullptr;      // device: 4 ints per molecule
+  int* h_infos = nullptr;    // pinned copy
+  int* counters = nullptr;   // one per class launch
+  cudaGraphExec_t exec = nullptr;
+  int launches = 0;
+  ~BatchPlan() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (dmem) cudaFree(dmem);
+    if (h_infos) cudaFreeHost(h_infos);
+  }
+};
+
+struct BatchMol {
+  pa_basis orb, aux;
+  int nd, ns;
+  const double* dens;
+  double* R;
+  long long sd, si, sj;
+};
+
+// Records the whole batch on c->stream (the origin of a capture when graphed).
+int record_batch(Ctx* c, BatchPlan& plan, const std::vector<BatchMol>& mols, const DeviceTables& dt,
+                 const Options& o, const std::vector<int>& class_lab, const std::vector<int>& class_lc,
+                 const std::vector<const Df3cArgs*>& class_args_d, const std::vector<const int*>& class_off_d,
+                 const std::vector<int>& class_nm, const std::vector<int>& class_items, int* launches) {
+  cudaStream_t s = c->stream;
+  const int nmol = static_cast<int>(mols.size());
+  constexpr int W = Ctx::kNs3c;
+  PA_CUDA(cudaEventRecord(c->fork, s));
+  for (int i = 0; i < W; ++i) {
+    PA_CUDA(cudaStreamWaitEvent(c->s3c[i], c->fork, 0));
+    PA_CUDA(cudaStreamWaitEvent(c->smet[i], c->fork, 0));
+  }
+  // per molecule: metric chain on a metric stream, screening + folding on a worker
+  for (int m = 0; m < nmol; ++m) {
+    const BatchMol& M = mols[m];
+    DfBuffers& b = plan.bufs[m];
+    stage_metric(M.aux, b, dt, o, c->smet[m % W], launches);
+    const int st = run_screening(M.orb, M.aux, dt, o, b, c->s3c[m % W], launches);
+    if (st != PA_OK) return st;
+    stage_bra_prep(M.orb, M.aux, M.nd, M.dens, M.sd, M.si, M.sj, b, o, c->s3c[m % W], launches);
+  }
+  for (int i = 0; i < W; ++i) {
+    PA_CUDA(cudaEventRecord(c->j3c[i], c->s3c[i]));
+    PA_CUDA(cudaStreamWaitEvent(s, c->j3c[i], 0));
+  }
+  // one persistent launch per class over all molecules
+  const int ncls = static_cast<int>(class_lab.size());
+  if (ncls > 0) PA_CUDA(cudaMemsetAsync(plan.counters, 0, sizeof(int) * ncls, s));
+  PA_CUDA(cudaEventRecord(c->fork, s));
+  for (int i = 0; i < W; ++i) PA_CUDA(cudaStreamWaitEvent(c->s3c[i], c->fork, 0));
+  for (int k = 0; k < ncls; ++k)
+    *launches += launch_df3c_class_batch(class_lab[k], class_lc[k], class_args_d[k], class_off_d[k], class_nm[k],
+                                         class_items[k], plan.counters + k, c->s3c[k % W]);
+  for (int i = 0; i < W; ++i) {
+    PA_CUDA(cudaEventRecord(c->j3c[i], c->s3c[i]));
+    PA_CUDA(cudaStreamWaitEvent(s, c->j3c[i], 0));
+  }
+  // per molecule: reduction, then (after its metric chain) solve and tensor
+  PA_CUDA(cudaEventRecord(c->fork, s));
+  for (int i = 0; i < W; ++i) {
+    PA_CUDA(cudaStreamWaitEvent(c->s3c[i], c->fork, 0));
+    PA_CUDA(cudaEventRecord(c->jmet[i], c->smet[i]));
+    PA_CUDA(cudaStreamWaitEvent(c->s3c[i], c->jmet[i], 0));
+  }
+  for (int m = 0; m < nmol; ++m) {
+    const BatchMol& M = mols[m];
+    DfBuffers& b = plan.bufs[m];
+    cudaStream_t w = c->s3c[m % W];
+    stage_reduce(M.aux, M.nd, b, w, launches);
+    const int st = stage_solve(M.aux, M.nd, b, o, plan.df[m], w, launches);
+    if (st != PA_OK) return st;
+    *launches += coulomb_4d(plan.df[m], M.aux->host.nsph, M.nd, M.ns, plan.gram[m], M.R, w);
+  }
+  for (int i = 0; i < W; ++i) {
+    PA_CUDA(cudaEventRecord(c->j3c[i], c->s3c[i]));
+    PA_CUDA(cudaStreamWaitEvent(s, c->j3c[i], 0));
+  }
+  return PA_OK;
+}
+
+int batch_4d(int nmol, const pa_basis* orbs, const pa_basis* auxs, const int* ndens,
+             const double* const* d_dens, int layout, const int* nstates, double* const* d_R,
+             int use_graph, cudaStream_t user_stream) {
+  if (nmol < 0 || (nmol > 0 && (!orbs || !auxs || !ndens || !d_dens || !nstates || !d_R)))
+    return fail(PA_ERR_ARG, "invalid batch arguments");
+  if (layout != PA_LAYOUT_FORTRAN && layout != PA_LAYOUT_C) return fail(PA_ERR_ARG, "unknown layout");
+  std::vector<BatchMol> mols(nmol);
+  for (int m = 0; m < nmol; ++m) {
+    int st = check_pair(orbs[m], auxs[m]);
+    if (st != PA_OK) return st;
+    const int nd = ndens[m], ns = nstates[m];
+    if (ns <= 0 || ns * (ns + 1) / 2 != nd) return fail(PA_ERR_ARG, "molecule " + std::to_string(m) + ": ndens must equal nstates (nstates + 1) / 2");
+    if (!d_dens[m] || !d_R[m]) return fail(PA_ERR_ARG, "molecule " + std::to_string(m) + ": null pointer");
+    const long long n = orbs[m]->host.nsph;
+    BatchMol& M = mols[m];
+    M.orb = orbs[m];
+    M.aux = auxs[m];
+    M.nd = nd;
+    M.ns = ns;
+    M.dens = d_dens[m];
+    M.R = d_R[m];
+    if (layout == PA_LAYOUT_FORTRAN) {
+      M.sd = 1;
+      M.si = nd;
+      M.sj = static_cast<long long>(nd) * n;
+    } else {
+      M.sd = n * n;
+      M.si = n;
+      M.sj = 1;
+    }
+  }
+  Ctx* c = nullptr;
+  DeviceTables dt;
+  int st = current_ctx(&c, &dt);
+  if (st != PA_OK) return st;
+  std::lock_guard<std::mutex> lk(c->mu);
+  const Options o = options();
+  // signature of the batch: options, then per molecule handles, sizes, pointers
+  std::vector<long long> sig{nmol, layout, use_graph ? 1 : 0, o.boys_mode, o.skip_metric, o.precision};
+  for (double v : {o.screen_thresh, o.fp32_thresh, o.metric_shift}) {
+    long long bits;
+    std::memcpy(&bits, &v, sizeof bits);
+    sig.push_back(bits);
+  }
+  for (const BatchMol& M : mols) {
+    sig.push_back(M.orb->serial);
+    sig.push_back(M.aux->serial);
+    sig.push_back(M.nd);
+    sig.push_back(reinterpret_cast<long long>(M.dens));
+    sig.push_back(reinterpret_cast<long long>(M.R));
+  }
+  // the user's stream is ordered before the batch, the batch before the return
+  PA_CUDA(cudaStreamSynchronize(user_stream));
+  BatchPlan* plan = c->plan;
+  const bool reuse = use_graph && plan && plan->sig == sig && plan->exec;
+  int launches = 0;
+  if (!reuse) {
+    if (plan) {
+      PA_CUDA(cudaStreamSynchronize(c->stream));
+      delete plan;
+      c->plan = nullptr;
+    }
+    plan = new BatchPlan();
+    plan->sig = sig;
+    plan->bufs.resize(nmol);
+    plan->df.resize(nmol);
+    plan->gram.resize(nmol);
+    // classes present in the batch, and for each the molecules' runs
+    std::vector<int> class_lab, class_lc, class_nm, class_items;
+    std::vector<std::vector<std::pair<int, int>>> class_runs;  // (molecule, run index)
+    for (int lab = 0; lab <= 2 * PA_LMAX; ++lab)
+      for (int lc = 0; lc <= PA_LAUXMAX; ++lc) {
+        class_lab.push_back(lab);
+        class_lc.push_back(lc);
+        class_runs.emplace_back();
+      }
+    // count, allocate, carve
+    std::vector<size_t> off(nmol + 1, 0);
+    for (int pass = 0; pass < 2; ++pass) {
+      Carver cv;
+      if (pass == 1) cv.base = plan->dmem;
+      for (int m = 0; m < nmol; ++m) {
+        const BatchMol& M = mols[m];
+        layout_df(cv, M.orb, M.aux, M.nd, &plan->bufs[m]);
+        plan->df[m] = cv.take<double>(static_cast<size_t>(M.aux->host.nsph) * M.nd);
+        plan->gram[m] = cv.take<double>(static_cast<size_t>(M.nd) * M.nd);
+      }
+      plan->infos = cv.take<int>(4 * std::max(nmol, 1));
+      plan->counters = cv.take<int>(class_lab.size());
+      if (pass == 0) {
+        off[0] = cv.used;
+        // room for the class descriptors: at most one per (class, molecule)
+        cv.take<Df3cArgs>(class_lab.size() * std::max(nmol, 1));
+        cv.take<int>(class_lab.size() * (std::max(nmol, 1) + 1));
+        if (cudaMalloc(&plan->dmem, std::max<size_t>(cv.used, 256)) != cudaSuccess) {
+          delete plan;
+          return fail(PA_ERR_CUDA, "cudaMalloc(batch plan) failed");
+        }
+      }
+    }
+    for (int m = 0; m < nmol; ++m) plan->bufs[m].info = plan->infos + 4 * m;
+    Df3cArgs* d_args = reinterpret_cast<Df3cArgs*>(plan->dmem + off[0]);
+    int* d_off = reinterpret_cast<int*>(d_args + class_lab.size() * std::max(nmol, 1));
+    // class descriptors (host), molecules by decreasing work within a class
+    std::vector<Df3cArgs> h_args(class_lab.size() * std::max(nmol, 1));
+    std::vector<int> h_off(class_lab.size() * (std::max(nmol, 1) + 1), 0);
+    std::vector<const Df3cArgs*> args_d;
+    std::vector<const int*> off_d;
+    std::vector<int> keep_lab, keep_lc;
+    for (size_t k = 0; k < class_lab.size(); ++k) {
+      std::vector<std::pair<long long, Df3cArgs>> items;
+      for (int m = 0; m < nmol; ++m) {
+        const BatchMol& M = mols[m];
+        const DfBuffers& b = plan->bufs[m];
+        for (const auto& r : b.runs) {
+          if (r.lab != class_lab[k] || r.lc != class_lc[k]) continue;
+          Df3cArgs a = class_args(M.orb, M.aux, M.nd, b, dt, o, r);
+          df3c_fill_items(r.lab, r.lc, &a, r.ny);
+          const long long work = static_cast<long long>(a.n_units) * a.n_aux * a.nd;
+          if (a.n_items > 0) items.push_back({work, a});
+        }
+      }
+      if (items.empty()) continue;
+      std::stable_sort(items.begin(), items.end(),
+                       [](const auto& x, const auto& y) { return x.first > y.first; });
+      const size_t slot = keep_lab.size();
+      Df3cArgs* ha = h_args.data() + slot * std::max(nmol, 1);
+      int* ho = h_off.data() + slot * (std::max(nmol, 1) + 1);
+      ho[0] = 0;
+      for (size_t i = 0; i < items.size(); ++i) {
+        ha[i] = items[i].second;
+        ho[i + 1] = ho[i] + items[i].second.n_items;
+      }
+      keep_lab.push_back(class_lab[k]);
+      keep_lc.push_back(class_lc[k]);
+      class_nm.push_back(static_cast<int>(items.size()));
+      class_items.push_back(ho[items.size()]);
+      args_d.push_back(d_args + slot * std::max(nmol, 1));
+      off_d.push_back(d_off + slot * (std::max(nmol, 1) + 1));
+    }
+    PA_CUDA(cudaMemcpy(d_args, h_args.data(), sizeof(Df3cArgs) * h_args.size(), cudaMemcpyHostToDevice));
+    PA_CUDA(cudaMemcpy(d_off, h_off.data(), sizeof(int) * h_off.size(), cudaMemcpyHostToDevice));
+    PA_CUDA(cudaMallocHost(&plan->h_infos, sizeof(int) * 4 * std::max(nmol, 1)));
+    c->plan = plan;
+    if (use_graph) {
+      cudaGraph_t graph = nullptr;
+      PA_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+      st = record_batch(c, *plan, mols, dt, o, keep_lab, keep_lc, args_d, off_d, class_nm, class_items, &launches);
+      const cudaError_t ec = cudaStreamEndCapture(c->stream, &graph);
+      if (st != PA_OK || ec != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        c->plan = nullptr;
+        delete plan;
+        if (st != PA_OK) return st;
+        return fail(PA_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
+      }
+      const cudaError_t ei = cudaGraphInstantiate(&plan->exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ei != cudaSuccess) {
+        c->plan = nullptr;
+        delete plan;
+        return fail(PA_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+      }
+      plan->launches = launches;
+    } else {
+      PA_CUDA(cudaEventRecord(c->ev0, c->stream));
+      st = record_batch(c, *plan, mols, dt, o, keep_lab, keep_lc, args_d, off_d, class_nm, class_items, &launches);
+      plan->launches = launches;
+      if (st != PA_OK) {
+        cudaStreamSynchronize(c->stream);
+        c->plan = nullptr;
+        delete plan;
+        return st;
+      }
+    }
+  }
+  if (use_graph) {
+    PA_CUDA(cudaEventRecord(c->ev0, c->stream));
+    PA_CUDA(cudaGraphLaunch(plan->exec, c->stream));
+  }
+  PA_CUDA(cudaGetLastError());
+  PA_CUDA(cudaEventRecord(c->ev1, c->stream));
+  PA_CUDA(cudaMemcpyAsync(plan->h_infos, plan->infos, sizeof(int) * 4 * std::max(nmol, 1),
+                          cudaMemcpyDeviceToHost, c->stream));
+  PA_CUDA(cudaStreamSynchronize(c->stream));
+  float ms = 0.f;
+  PA_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  g_stats = pa_stats{};
+  g_stats.ms_total = ms;
+  g_stats.kernel_launches = plan->launches;
+  g_stats.ntriplets = g_stats.nskipped = g_stats.nints = -1;
+  if (!use_graph) {
+    // an ungraphed plan is not kept for replay
+    c->plan = nullptr;
+    const int nm = nmol;
+    std::vector<int> infos(plan->h_infos, plan->h_infos + 4 * std::max(nm, 1));
+    delete plan;
+    for (int m = 0; m < nm; ++m)
+      if (infos[4 * m] != 0)
+        return fail(PA_ERR_NOT_SPD, "molecule " + std::to_string(m) + ": metric (P|Q) is not positive definite (Cholesky pivot " +
+                                        std::to_string(infos[4 * m]) + ")");
+    return PA_OK;
+  }
+  for (int m = 0; m < nmol; ++m)
+    if (plan->h_infos[4 * m] != 0)
+      return fail(PA_ERR_NOT_SPD, "molecule " + std::to_string(m) + ": metric (P|Q) is not positive definite (Cholesky pivot " +
+                                      std::to_string(plan->h_infos[4 * m]) + ")");
+  return PA_OK;
 }
 
 int nstates_of(int ndens) {
@@ -1040,6 +1387,10 @@ int pa_basis_create(int nshells, int ndata, const int* bas_centers, const int* b
   int st = current_ctx(&c, &dt);
   if (st != PA_OK) return st;
   pa_basis b = new pa_basis_s();
+  {
+    static std::atomic<long long> next_serial{1};
+    b->serial = next_serial++;
+  }
   cudaGetDevice(&b->device);
   std::string err;
   st = unpack_basis(nshells, ndata, bas_centers, bas_spec, bas_data, lmax_allowed, &b->host, &err);
@@ -1454,3 +1805,11 @@ int f_intor_df2c_mo(int nshells, int ndata, const int* bas_centers, const int* b
 }
 
 }  // extern "C"
+
+extern "C" int pa_df_4d_batch(int nmol, const pa_basis* orbital, const pa_basis* aux, const int* ndens,
+                              const double* const* d_densities, int layout, const int* nstates,
+                              double* const* d_coulomb, int use_graph, void* stream) {
+  return pa::batch_4d(nmol, orbital, aux, ndens, d_densities, layout, nstates, d_coulomb, use_graph,
+                      static_cast<cudaStream_t>(stream));
+}
+

@@ -97,6 +97,8 @@ SIGNATURES = {
     "pa_basis_info": [_vp, _pi, _pi, _pi],
     "pa_df_2d": [_vp, _vp, _i, _i, _vp, _i, _vp, _vp],
     "pa_df_4d": [_vp, _vp, _i, _i, _vp, _i, _i, _vp, _vp],
+    "pa_df_4d_batch": [_i, ctypes.POINTER(_vp), ctypes.POINTER(_vp), _pi, ctypes.POINTER(_vp), _i, _pi,
+                       ctypes.POINTER(_vp), _i, _vp],
     "pa_contract_coulomb_densities_2d": [_vp, _vp, _i, _i, _pd, _i, _pd],
     "pa_contract_coulomb_densities_4d": [_vp, _vp, _i, _i, _pd, _i, _i, _pd],
     "pa_count_triplets": [_vp, _vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
@@ -254,3 +256,21 @@ def cholesky_solve(A, B):
     n = A.shape[0]
     check(load().pa_cholesky_solve(n, ptr(A), B.shape[1] if B.ndim == 2 else 1, ptr(B)))
     return A, B
+
+
+def df_4d_batch(orbitals, auxes, densities, nstates, outputs, layout=PA_LAYOUT_C, use_graph=True, stream=None):
+    """Coulomb tensors of many molecules in one call (pa_df_4d_batch).
+
+    orbitals, auxes: Basis objects; densities: device tensors (ndens, nbf, nbf);
+    outputs: device tensors with nstates**4 elements each (column-major)."""
+    n = len(orbitals)
+    V = _vp * max(n, 1)
+    I = ctypes.c_int * max(n, 1)
+    orb = V(*[b.handle for b in orbitals])
+    aux = V(*[b.handle for b in auxes])
+    nd = I(*[int(d.shape[0]) for d in densities])
+    dp = V(*[d.data_ptr() for d in densities])
+    ns = I(*[int(x) for x in nstates])
+    op = V(*[o.data_ptr() for o in outputs])
+    check(load().pa_df_4d_batch(n, orb, aux, nd, dp, int(layout), ns, op, int(bool(use_graph)), stream))
+

@@ -155,3 +155,15 @@ CONFIGS = {
 
 def config_workload(key, seed=0):
     return make_workload(seed=seed, **CONFIGS[key])
+
+
+def batch_workloads(nmol=64, lmax=3, lauxmax=4, atoms=(5, 60), states=(4, 16), seed=4321):
+    """The batched workload: nmol molecules with seeds 0..nmol-1, atom counts
+    uniform in [atoms[0], atoms[1]] and state counts uniform in
+    [states[0], states[1]] (drawn from one generator seeded with `seed`)."""
+    rng = np.random.default_rng(seed)
+    natoms = rng.integers(atoms[0], atoms[1] + 1, size=nmol)
+    nstates = rng.integers(states[0], states[1] + 1, size=nmol)
+    return [make_workload(int(n), lmax, lauxmax, int(k), seed=i,
+                          name=f"batch{i}_{int(n)}atoms_{int(k)}states")
+            for i, (n, k) in enumerate(zip(natoms, nstates))]
