@@ -137,7 +137,9 @@ __global__ void __launch_bounds__(256) k_schwarz_bra(DevBasis B, const int2* __r
       __syncthreads();  // previous users of Rn / R buffers / Y are done
       if (threadIdx.x <= L4) {
         const int n = threadIdx.x;
-        Rn[n] = pref * pow(-2.0 * alpha, n) * boys_n(dt, boys_mode, n, T);
+        double f = pref;
+        for (int k = 0; k < n; ++k) f *= -2.0 * alpha;
+        Rn[n] = f * boys_n(dt, boys_mode, n, T);
       }
       __syncthreads();
       hermite_R(it, L4, Rn, X, Yd, Z, R0, R1, threadIdx.x, blockDim.x, BlockSync());
@@ -149,7 +151,8 @@ __global__ void __launch_bounds__(256) k_schwarz_bra(DevBasis B, const int2* __r
           const int rr = idx / NH, tp = idx - rr * NH;
           const double* e = Ei + (r0 + rr) * NH;
           double y = 0.0;
-          for (int t = 0; t < NH; ++t) y = fma(e[t], R0[cidx_sum(it, t, tp)], y);
+          const int16_t* sidx = dt.sum_idx + tp;  // column tp of the sum table (symmetric)
+          for (int t = 0; t < NH; ++t) y = fma(e[t], R0[__ldg(sidx + t * kNSum)], y);
           const int deg = it->xyz[tp][3];
           Y[rr * NH + tp] = (deg & 1) ? -y : y;
         }
@@ -209,7 +212,11 @@ __device__ void twoc_block_warp(const DevBasis& X, int P, int Q, const DeviceTab
       if (lQ & 1) pref = -pref;
       const double T = alpha * RPQ2;
       __syncwarp();
-      if (lane <= L) s.Rn[lane] = pref * pow(-2.0 * alpha, lane) * boys_n(dt, boys_mode, lane, T);
+      if (lane <= L) {
+        double f = pref;
+        for (int k = 0; k < lane; ++k) f *= -2.0 * alpha;
+        s.Rn[lane] = f * boys_n(dt, boys_mode, lane, T);
+      }
       __syncwarp();
       hermite_R(it, L, s.Rn, Xd, Yd, Zd, s.R0, s.R1, lane, 32, WarpSync());
       for (int idx = lane; idx < nsP * ncQ; idx += 32) {

@@ -52,7 +52,12 @@ struct DeviceTables {
   const int* sph_start;       // [(PA_LAUXMAX+1)^2 + 1] row starts into sph_col/sph_val
   const int16_t* sph_col;     // local Cartesian index within degree l
   const double* sph_val;
+  // sum_idx[i * kNSum + j] = index of the multi-index sum (i) + (j) for
+  // components i, j of degree <= 2 * PA_LMAX
+  const int16_t* sum_idx;
 };
+
+constexpr int kNSum = ncum(2 * PA_LMAX);  // 165
 
 enum : int {
   PA_OK = 0,

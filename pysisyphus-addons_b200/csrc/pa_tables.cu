@@ -173,13 +173,20 @@ int build_tables(TablesOnDevice* out, std::string* err) {
     }
   }
   dense_off.push_back(static_cast<int>(dense.size()));
+  // multi-index sums of two bra Hermite components
+  std::vector<int16_t> sum_idx(static_cast<size_t>(kNSum) * kNSum);
+  for (int i = 0; i < kNSum; ++i)
+    for (int j = 0; j < kNSum; ++j)
+      sum_idx[static_cast<size_t>(i) * kNSum + j] = static_cast<int16_t>(
+          cidx(h_idx.xyz[i][0] + h_idx.xyz[j][0], h_idx.xyz[i][1] + h_idx.xyz[j][1], h_idx.xyz[i][2] + h_idx.xyz[j][2]));
   if (dense.size() > 1024) {
     *err = "solid-harmonic table exceeds its constant-memory slot";
     return PA_ERR_ARG;
   }
   // upload
   const size_t bytes = sizeof(IndexTables) + sizeof(double) * (taylor.size() + ref.size() + val.size()) +
-                       sizeof(int) * start.size() + sizeof(int16_t) * col.size() + 6 * 256;
+                       sizeof(int) * start.size() + sizeof(int16_t) * col.size() +
+                       sizeof(int16_t) * sum_idx.size() + 7 * 256;
   char* base = nullptr;
   cudaError_t e = cudaMalloc(&base, bytes);
   if (e != cudaSuccess) {
@@ -200,6 +207,7 @@ int build_tables(TablesOnDevice* out, std::string* err) {
   dt.sph_start = reinterpret_cast<const int*>(put(start.data(), sizeof(int) * start.size()));
   dt.sph_col = reinterpret_cast<const int16_t*>(put(col.data(), sizeof(int16_t) * col.size()));
   dt.sph_val = reinterpret_cast<const double*>(put(val.data(), sizeof(double) * val.size()));
+  dt.sum_idx = reinterpret_cast<const int16_t*>(put(sum_idx.data(), sizeof(int16_t) * sum_idx.size()));
   e = upload_sph_dense(dense.data(), static_cast<int>(dense.size()), dense_off.data(), rownorm.data(), 0);
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
