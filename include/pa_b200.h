@@ -140,6 +140,10 @@ int pa_set_metric_shift(double shift);
  * function (below T = 27 / 30), the Hermite recurrence and the solid-harmonic
  * contraction in FP32; their contributions are accumulated in FP64. */
 int pa_set_precision(int mode, double fp32_thresh);
+/* Granularity of the three-center work queue: work items per SM and shell
+ * class (default 4). Finer items shorten the tail of each class launch and
+ * cost more partial sums; the best value depends on the system size. */
+int pa_set_items_per_sm(int items);
 int pa_get_precision(void);
 
 /* Statistics of the last density-fitting call on this process. */

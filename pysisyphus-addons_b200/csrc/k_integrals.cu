@@ -8,6 +8,8 @@
 //  * k_metric       the symmetric (P|Q) matrix (intor.f90:40-95);
 //  * k_bra_prep     density folding G_d[tuv] = sum_(ma,mb) Dsym_d[ma,mb] E_sph[(ma,mb)][tuv]
 //                   with Dsym = D + (a != b) D^T as in diabatization/intor.f90:155-177.
+#include <algorithm>
+
 #include "boys.cuh"
 #include "k_integrals.cuh"
 #include "md.cuh"
@@ -105,11 +107,12 @@ constexpr int kSchwarzRowChunk = 8;
 
 __global__ void __launch_bounds__(256) k_schwarz_bra(DevBasis B, const int2* __restrict__ pair_ab,
                                                      const int* __restrict__ pair_unit0,
-                                                     UnitArrays U, int npairs, DeviceTables dt,
-                                                     int boys_mode, double* __restrict__ Qab) {
+                                                     const int* __restrict__ pair_list, UnitArrays U,
+                                                     int npairs, DeviceTables dt, int boys_mode,
+                                                     double* __restrict__ Qab) {
   extern __shared__ double smem[];
-  const int pair = blockIdx.x;
-  if (pair >= npairs) return;
+  if (static_cast<int>(blockIdx.x) >= npairs) return;
+  const int pair = pair_list[blockIdx.x];
   const int2 ab = pair_ab[pair];
   const int4 sa = B.shell[ab.x], sb = B.shell[ab.y];
   const int la = sa.x, lb = sb.x;
@@ -178,6 +181,83 @@ __global__ void __launch_bounds__(256) k_schwarz_bra(DevBasis B, const int2* __r
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
     Qab[pair] = sqrt(sqrt(tot));
   }
+}
+
+// Schwarz values of low-L pairs (Lab <= kSwLab), one warp per pair: the same
+// arithmetic as k_schwarz_bra with warp barriers instead of block barriers
+// (most pairs of a basis are low-L, and for them the block version mostly
+// waits at its barriers).
+constexpr int kSwLab = 4;
+constexpr int kSwNR = ncum(2 * kSwLab);
+constexpr int kSwNH = ncum(kSwLab);
+constexpr int kSwNab = 25;  // largest (2la+1)(2lb+1) with la + lb <= 4, la, lb <= PA_LMAX
+constexpr int kSwScratch = 32 + 2 * kSwNR + kSwNab * kSwNH + kSwNab * kSwNab;
+constexpr int kSwWarps = 4;
+
+__global__ void __launch_bounds__(32 * kSwWarps) k_schwarz_bra_warp(
+    DevBasis B, const int2* __restrict__ pair_ab, const int* __restrict__ pair_unit0,
+    const int* __restrict__ pair_list, UnitArrays U, int npairs, DeviceTables dt, int boys_mode,
+    double* __restrict__ Qab) {
+  extern __shared__ double sw_smem[];  // [kSwWarps][kSwScratch]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = blockIdx.x * kSwWarps + warp;
+  if (i >= npairs) return;  // warp-uniform
+  const int pair = pair_list[i];
+  const int2 ab = pair_ab[pair];
+  const int4 sa = B.shell[ab.x], sb = B.shell[ab.y];
+  const int la = sa.x, lb = sb.x;
+  const int nab = (2 * la + 1) * (2 * lb + 1);
+  const int NH = ncum(la + lb);
+  const int L4 = 2 * (la + lb);
+  double* Rn = sw_smem + warp * kSwScratch;
+  double* R0 = Rn + 32;
+  double* R1 = R0 + kSwNR;
+  double* Y = R1 + kSwNR;          // [nab][NH]
+  double* out = Y + kSwNab * kSwNH;  // [nab][nab]
+  const IndexTables* it = dt.idx;
+  for (int k = lane; k < nab * nab; k += 32) out[k] = 0.0;
+  const int u0 = pair_unit0[pair];
+  const int nu = sa.y * sb.y;
+  for (int iu = 0; iu < nu; ++iu)
+    for (int ku = 0; ku < nu; ++ku) {
+      const double4 P = U.unit_pP[u0 + iu], Q = U.unit_pP[u0 + ku];
+      const double p = P.x, q = Q.x, pq = p + q, alpha = p * q / pq;
+      const double X = P.y - Q.y, Yd = P.z - Q.z, Z = P.w - Q.w;
+      const double T = alpha * (X * X + Yd * Yd + Z * Z);
+      const double pref = kTwoPi52 / (p * q * sqrt(pq));
+      __syncwarp();  // previous users of Rn / R / Y are done
+      if (lane <= L4) {
+        double f = pref;
+        for (int k = 0; k < lane; ++k) f *= -2.0 * alpha;
+        Rn[lane] = f * boys_n(dt, boys_mode, lane, T);
+      }
+      __syncwarp();
+      hermite_R(it, L4, Rn, X, Yd, Z, R0, R1, lane, 32, WarpSync());
+      const double* Ei = U.esph + U.unit_esph[u0 + iu];
+      const double* Ek = U.esph + U.unit_esph[u0 + ku];
+      for (int idx = lane; idx < nab * NH; idx += 32) {
+        const int rr = idx / NH, tp = idx - rr * NH;
+        const double* e = Ei + rr * NH;
+        const int16_t* sidx = dt.sum_idx + tp;
+        double y = 0.0;
+        for (int t = 0; t < NH; ++t) y = fma(e[t], R0[__ldg(sidx + t * kNSum)], y);
+        Y[idx] = (it->xyz[tp][3] & 1) ? -y : y;
+      }
+      __syncwarp();
+      for (int idx = lane; idx < nab * nab; idx += 32) {
+        const int rr = idx / nab, sc = idx - rr * nab;
+        const double* e = Ek + sc * NH;
+        const double* yr = Y + rr * NH;
+        double v = 0.0;
+        for (int tp = 0; tp < NH; ++tp) v = fma(yr[tp], e[tp], v);
+        out[idx] += v;
+      }
+    }
+  __syncwarp();
+  double s2 = 0.0;
+  for (int k = lane; k < nab * nab; k += 32) s2 += out[k] * out[k];
+  for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+  if (lane == 0) Qab[pair] = sqrt(sqrt(s2));
 }
 
 // ---------------------------------------------------------------------------
@@ -373,14 +453,29 @@ size_t schwarz_bra_smem(int lab_max) {
 }
 
 int launch_schwarz_bra(const DevBasis& B, const int2* pair_ab, const int* pair_unit0,
-                       UnitArrays U, int npairs, int lab_max, const DeviceTables& dt,
+                       const int* class_pair, const PairLists& P, UnitArrays U, const DeviceTables& dt,
                        int boys_mode, double* Qab, cudaStream_t s) {
-  if (npairs == 0) return 0;
-  const size_t smem = schwarz_bra_smem(lab_max);
-  cudaFuncSetAttribute(k_schwarz_bra, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       static_cast<int>(smem));
-  k_schwarz_bra<<<npairs, 256, smem, s>>>(B, pair_ab, pair_unit0, U, npairs, dt, boys_mode, Qab);
-  return 1;
+  if (P.npairs == 0) return 0;
+  int launches = 0;
+  const int split = std::min(kSwLab, P.lab_max) + 1;  // classes [0, split) by warps
+  const int nlow = P.pair_class_off[split];
+  if (nlow > 0) {
+    const size_t wsm = sizeof(double) * kSwWarps * kSwScratch;
+    cudaFuncSetAttribute(k_schwarz_bra_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(wsm));
+    k_schwarz_bra_warp<<<(nlow + kSwWarps - 1) / kSwWarps, 32 * kSwWarps, wsm, s>>>(
+        B, pair_ab, pair_unit0, class_pair, U, nlow, dt, boys_mode, Qab);
+    ++launches;
+  }
+  const int nhigh = P.npairs - nlow;
+  if (nhigh > 0) {
+    const size_t smem = schwarz_bra_smem(P.lab_max);
+    cudaFuncSetAttribute(k_schwarz_bra, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(smem));
+    k_schwarz_bra<<<nhigh, 256, smem, s>>>(B, pair_ab, pair_unit0, class_pair + nlow, U, nhigh, dt,
+                                           boys_mode, Qab);
+    ++launches;
+  }
+  return launches;
 }
 
 int launch_schwarz_aux(const DevBasis& X, const DeviceTables& dt, int boys_mode, double* Qc,

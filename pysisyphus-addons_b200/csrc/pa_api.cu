@@ -163,6 +163,18 @@ void build_pair_lists(const HostBasis& b, PairLists* out) {
   p.class_unit.assign(p.nunits, 0);
   std::vector<int> fill(p.class_off.begin(), p.class_off.end() - 1);
   for (int u = 0; u < p.nunits; ++u) p.class_unit[fill[lab[u]]++] = u;
+  p.pair_class_off.assign(p.lab_max + 2, 0);
+  for (int q = 0; q < p.npairs; ++q) {
+    const int2 ab = p.pair_ab[q];
+    p.pair_class_off[b.shells[ab.x].L + b.shells[ab.y].L + 1]++;
+  }
+  for (int c = 0; c <= p.lab_max; ++c) p.pair_class_off[c + 1] += p.pair_class_off[c];
+  p.class_pair.assign(p.npairs, 0);
+  std::vector<int> pfill(p.pair_class_off.begin(), p.pair_class_off.end() - 1);
+  for (int q = 0; q < p.npairs; ++q) {
+    const int2 ab = p.pair_ab[q];
+    p.class_pair[pfill[b.shells[ab.x].L + b.shells[ab.y].L]++] = q;
+  }
   *out = std::move(p);
 }
 
@@ -222,6 +234,7 @@ struct pa_basis_s {
   long long* d_unit_esph = nullptr;
   int* d_class_unit = nullptr;   // units grouped by Lab
   int* d_class_off = nullptr;    // [lab_max + 2]
+  int* d_class_pair = nullptr;   // pairs grouped by Lab
   int* d_aux_shell = nullptr;    // aux shells grouped by L
   int* d_aux_off = nullptr;      // [lc_max + 2]
 };
@@ -374,7 +387,8 @@ size_t cub_temp_bytes(const pa_basis_s* orb, const pa_basis_s* aux) {
 }
 
 // Lays out all buffers of a run (counting when c.base == nullptr).
-void layout_df(Carver& c, const pa_basis_s* orb, const pa_basis_s* aux, int nd, DfBuffers* b) {
+void layout_df(Carver& c, const pa_basis_s* orb, const pa_basis_s* aux, int nd, DfBuffers* b,
+               int items_per_sm) {
   const PairLists& P = orb->pairs;
   const int nx = static_cast<int>(aux->host.shells.size());
   const long long naux = aux->host.nsph;
@@ -420,7 +434,7 @@ void layout_df(Carver& c, const pa_basis_s* orb, const pa_basis_s* aux, int nd, 
       df3c_class_info(lab, lc, &ci);
       const int bx = (nxc + ci.tc - 1) / ci.tc;
       const int bz = nz;
-      const int target = 4 * 148;  // work items per class (persistent blocks pull them)
+      const int target = items_per_sm * 148;  // work items per class (persistent blocks pull them)
       int ny = std::max(1, (target + bx * bz - 1) / (bx * bz));
       const int max_ny = (nu + ci.ub - 1) / ci.ub;
       ny = std::min(ny, max_ny);
@@ -459,8 +473,8 @@ int run_screening(const pa_basis_s* orb, const pa_basis_s* aux, const DeviceTabl
   const int nx = static_cast<int>(aux->host.shells.size());
   UnitArrays U = unit_arrays(orb, b);
   *launches += launch_unit_setup(orb->dev, orb->d_pair_ab, U, P.nunits, dt, s);
-  *launches += launch_schwarz_bra(orb->dev, orb->d_pair_ab, orb->d_pair_unit0, U, P.npairs,
-                                  P.lab_max, dt, o.boys_mode, b.Qab, s);
+  *launches += launch_schwarz_bra(orb->dev, orb->d_pair_ab, orb->d_pair_unit0, orb->d_class_pair, P, U, dt,
+                                  o.boys_mode, b.Qab, s);
   *launches += launch_schwarz_aux(aux->dev, dt, o.boys_mode, b.Qc, s);
   if (nx > 0) {
     size_t bytes = b.cub_bytes;
@@ -688,6 +702,7 @@ int ensure_pairs(pa_basis b) {
     b->d_unit_esph = cnt.take<long long>(P.unit_esph.size());
     b->d_class_unit = cnt.take<int>(P.class_unit.size());
     b->d_class_off = cnt.take<int>(P.class_off.size());
+    b->d_class_pair = cnt.take<int>(P.class_pair.size());
   }
   std::vector<char> stage(cnt.used);
   auto put = [&](const void* dst, const void* src, size_t bytes) {
@@ -700,6 +715,7 @@ int ensure_pairs(pa_basis b) {
   put(b->d_unit_esph, P.unit_esph.data(), sizeof(long long) * P.unit_esph.size());
   put(b->d_class_unit, P.class_unit.data(), sizeof(int) * P.class_unit.size());
   put(b->d_class_off, P.class_off.data(), sizeof(int) * P.class_off.size());
+  put(b->d_class_pair, P.class_pair.data(), sizeof(int) * P.class_pair.size());
   const cudaError_t e = cudaMemcpy(dpair, stage.data(), cnt.used, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     cudaFree(dpair);
@@ -738,12 +754,12 @@ int df_device(pa_basis orb, pa_basis aux, int ndens, int nbf, const double* d_de
   cudaStream_t s = user_stream;
   DfBuffers b;
   Carver cnt;
-  layout_df(cnt, orb, aux, ndens, &b);
+  layout_df(cnt, orb, aux, ndens, &b, o.items_per_sm);
   if (d_R) cnt.take<double>(static_cast<size_t>(ndens) * ndens);
   PA_CUDA(c->arena.reserve(cnt.used));
   Carver real;
   real.base = c->arena.base;
-  layout_df(real, orb, aux, ndens, &b);
+  layout_df(real, orb, aux, ndens, &b, o.items_per_sm);
   double* gram = d_R ? real.take<double>(static_cast<size_t>(ndens) * ndens) : nullptr;
   const long long n = nbf;
   long long sd, si, sj;
@@ -900,7 +916,8 @@ int batch_4d(int nmol, const pa_basis* orbs, const pa_basis* auxs, const int* nd
   std::lock_guard<std::mutex> lk(c->mu);
   const Options o = options();
   // signature of the batch: options, then per molecule handles, sizes, pointers
-  std::vector<long long> sig{nmol, layout, use_graph ? 1 : 0, o.boys_mode, o.skip_metric, o.precision};
+  std::vector<long long> sig{nmol, layout, use_graph ? 1 : 0, o.boys_mode, o.skip_metric, o.precision,
+                             o.items_per_sm};
   for (double v : {o.screen_thresh, o.fp32_thresh, o.metric_shift}) {
     long long bits;
     std::memcpy(&bits, &v, sizeof bits);
@@ -945,7 +962,7 @@ int batch_4d(int nmol, const pa_basis* orbs, const pa_basis* auxs, const int* nd
       if (pass == 1) cv.base = plan->dmem;
       for (int m = 0; m < nmol; ++m) {
         const BatchMol& M = mols[m];
-        layout_df(cv, M.orb, M.aux, M.nd, &plan->bufs[m]);
+        layout_df(cv, M.orb, M.aux, M.nd, &plan->bufs[m], o.items_per_sm);
         plan->df[m] = cv.take<double>(static_cast<size_t>(M.aux->host.nsph) * M.nd);
         plan->gram[m] = cv.take<double>(static_cast<size_t>(M.nd) * M.nd);
       }
@@ -1197,7 +1214,7 @@ int std_device(pa_basis orb, pa_basis aux, int kind, int nmos, const double* d_m
   U.unit_pP = b.pP;
   U.esph = b.esph;
   launches += launch_unit_setup(orb->dev, orb->d_pair_ab, U, P.nunits, dt, s);
-  launches += launch_schwarz_bra(orb->dev, orb->d_pair_ab, orb->d_pair_unit0, U, P.npairs, P.lab_max, dt,
+  launches += launch_schwarz_bra(orb->dev, orb->d_pair_ab, orb->d_pair_unit0, orb->d_class_pair, P, U, dt,
                                  o.boys_mode, b.Qab, s);
   launches += launch_schwarz_aux(aux->dev, dt, o.boys_mode, b.Qc, s);
   PA_CUDA(cudaEventRecord(c->ph[0], s));
@@ -1349,6 +1366,13 @@ int pa_set_precision(int mode, double fp32_thresh) {
 int pa_get_precision(void) {
   std::lock_guard<std::mutex> lk(g_opt_mu);
   return g_opts.precision;
+}
+
+int pa_set_items_per_sm(int items) {
+  if (items < 1 || items > 1024) return fail(PA_ERR_ARG, "items per SM must be in [1, 1024]");
+  std::lock_guard<std::mutex> lk(g_opt_mu);
+  g_opts.items_per_sm = items;
+  return PA_OK;
 }
 
 int pa_set_metric_shift(double shift) {
@@ -1571,8 +1595,8 @@ static int schwarz_impl(pa_basis orb, pa_basis aux, double* q_bra, double* q_aux
     U.unit_pP = pP;
     U.esph = esph;
     launches += launch_unit_setup(orb->dev, orb->d_pair_ab, U, P.nunits, dt, s);
-    launches += launch_schwarz_bra(orb->dev, orb->d_pair_ab, orb->d_pair_unit0, U, P.npairs,
-                                   P.lab_max, dt, o.boys_mode, Qab, s);
+    launches += launch_schwarz_bra(orb->dev, orb->d_pair_ab, orb->d_pair_unit0, orb->d_class_pair, P, U, dt,
+                                   o.boys_mode, Qab, s);
     if (P.npairs) PA_CUDA(cudaMemcpyAsync(q_bra, Qab, sizeof(double) * P.npairs, cudaMemcpyDeviceToHost, s));
     PA_CUDA(cudaStreamSynchronize(s));
   }

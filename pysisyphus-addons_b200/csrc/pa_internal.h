@@ -54,6 +54,9 @@ struct PairLists {
   // units sorted by class: class_units[c] = list of units with Lab = c (host order)
   std::vector<int> class_off;         // [lab_max + 2] offsets into class_unit
   std::vector<int> class_unit;        // units grouped by class
+  // shell pairs grouped by class Lab (host order within a class)
+  std::vector<int> pair_class_off;    // [lab_max + 2] offsets into class_pair
+  std::vector<int> class_pair;
 };
 
 struct AuxLists {
@@ -75,6 +78,7 @@ struct Options {
   double metric_shift = 0.0;  // added to the diagonal of (P|Q) before the Cholesky
   int precision = 0;          // 0 = FP64 throughout, 1 = mixed (FP32 recurrences for weak triplets)
   double fp32_thresh = 1e-6;  // Schwarz bound below which the mixed form uses FP32
+  int items_per_sm = 4;       // work items per SM and class of the three-center kernel
 };
 
 struct Stats {
@@ -118,8 +122,10 @@ struct UnitArrays {
 
 int launch_unit_setup(const DevBasis& B, const int2* pair_ab, UnitArrays U, int nunits,
                       const DeviceTables& dt, cudaStream_t s);
+// Schwarz values of all pairs: pairs with Lab <= 4 one warp each, the others
+// one block each (class_pair: device copy of P.class_pair).
 int launch_schwarz_bra(const DevBasis& B, const int2* pair_ab, const int* pair_unit0,
-                       UnitArrays U, int npairs, int lab_max, const DeviceTables& dt,
+                       const int* class_pair, const PairLists& P, UnitArrays U, const DeviceTables& dt,
                        int boys_mode, double* Qab, cudaStream_t s);
 int launch_schwarz_aux(const DevBasis& X, const DeviceTables& dt, int boys_mode, double* Qc,
                        cudaStream_t s);

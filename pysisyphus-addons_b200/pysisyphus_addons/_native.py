@@ -90,6 +90,7 @@ SIGNATURES = {
     "pa_set_skip_metric": [_i],
     "pa_set_metric_shift": [_d],
     "pa_set_precision": [_i, _d],
+    "pa_set_items_per_sm": [_i],
     "pa_get_precision": [],
     "pa_get_stats": [ctypes.POINTER(PaStats)],
     "pa_basis_create": [_i, _i, _pi, _pi, _pd, _i, ctypes.POINTER(_vp)],
@@ -177,6 +178,11 @@ def set_precision(mode="fp64", fp32_thresh=1e-6):
     Schwarz bound is below fp32_thresh."""
     code = {"fp64": PA_PRECISION_FP64, "mixed": PA_PRECISION_MIXED}.get(mode, mode)
     check(load().pa_set_precision(int(code), float(fp32_thresh)))
+
+
+def set_items_per_sm(items):
+    """Work items per SM and shell class of the three-center queue (default 4)."""
+    check(load().pa_set_items_per_sm(int(items)))
 
 
 def get_precision():
