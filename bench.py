@@ -1,15 +1,25 @@
 """Benchmark of the density-fitting Coulomb-tensor path on B200.
 
-One step = one full Coulomb tensor of the 40-atom workload (lmax 3 / lauxmax 4,
-8 states, 36 densities) on the device: Schwarz screening, class sorting,
-density folding, metric + Cholesky, screened 3c2e contraction, L^-1 df and
-the tensor assembly. Inputs (basis handles, densities) are resident in HBM
-when the timed region starts; the densities (133 MB) exceed the 126 MB L2.
+Default (the headline line): one step = one full Coulomb tensor of the 40-atom
+workload (lmax 3 / lauxmax 4, 8 states, 36 densities) on the device: Schwarz
+screening, class sorting, density folding, metric + Cholesky, screened 3c2e
+contraction, L^-1 df and the tensor assembly. Inputs (basis handles, densities)
+are resident in HBM when the timed region starts; the densities (133 MB)
+exceed the 126 MB L2.
 
 metric: surviving spherical 3c2e integrals per second (the integrals the
 reference evaluates after Schwarz screening, diabatization/intor.f90:126-151).
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+                  [--config cfg1|cfg2|cfg5|cfg4] [--precision fp64|mixed]
+
+--config cfg5 is the 200-atom cluster (lmax 4 / lauxmax 5), cfg4 the batch of 64
+molecules (5-60 atoms, 4-16 states) run through pa_df_4d_batch (one CUDA graph
+per step). Both use the exact Boys function and a 1e-7 diagonal shift of the
+metric: with the reference's Boys interpolation their auxiliary metrics are
+indefinite and the Cholesky fails (the reference ignores that failure).
+--precision mixed runs the precision form (FP32 recurrences for triplets with
+Schwarz bound < 1e-6).
 
 --impl reference times the reference's CPU algorithm (the C++ OpenMP
 restatement under oracle/, as the Fortran reference cannot be built here) on
@@ -33,9 +43,16 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT / "pysisyphus-addons_b200"))
 sys.path.insert(0, str(ROOT / "oracle"))
 
-METRIC = "3c2e ints/s (Coulomb tensor, FP64 plain path)"
 UNIT = "ints/s"
 CONFIG_KEY = "cfg2"
+# workloads whose auxiliary metric needs the exact Boys function and a shift
+SHIFTED = {"cfg5": 1e-7, "cfg4": 1e-7}
+
+
+def metric_name(args):
+    form = "mixed precision" if args.precision == "mixed" else "FP64 plain"
+    path = "batched Coulomb tensors" if args.config == "cfg4" else "Coulomb tensor"
+    return f"3c2e ints/s ({path}, {form} path)"
 
 
 def parse():
@@ -44,33 +61,52 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default=CONFIG_KEY)
-    ap.add_argument("--boys", default="reference", choices=["reference", "exact"])
+    ap.add_argument("--config", default=CONFIG_KEY, choices=["cfg1", "cfg2", "cfg5", "cfg4"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--boys", default=None, choices=["reference", "exact"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="device steps only (for ncu): no e2e, CPU baseline, FP64 probe or clocks")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.boys is None:
+        a.boys = "exact" if a.config in SHIFTED else "reference"
+    return a
 
 
-def workload_config(key, w, nd):
+def workloads(args, rank=0):
+    from pysisyphus_addons.common.synthetic import batch_workloads, config_workload
+
+    if args.config == "cfg4":
+        return batch_workloads(nmol=64)
+    return [config_workload(args.config, seed=rank)]
+
+
+def workload_config(args, ws):
     from pysisyphus_addons.common.synthetic import CONFIGS
 
-    c = CONFIGS[key]
-    return {
-        "workload": f"df_coulomb_tensor_{c['natoms']}atoms_lmax{c['lmax']}_lauxmax{c['lauxmax']}_{c['nstates']}states",
-        "natoms": c["natoms"],
-        "lmax": c["lmax"],
-        "lauxmax": c["lauxmax"],
-        "nstates": c["nstates"],
-        "ndens": nd,
-        "nbf": w.shells.sph_size,
-        "naux": w.shells_aux.sph_size,
-        "nshells": len(w.shells),
-        "nshells_aux": len(w.shells_aux),
-        "screen_thresh": "float32(1e-10)",
-        "l2": "inputs larger than L2 (densities %.0f MB > 126 MB)" % (w.densities.nbytes / 1e6),
-    }
+    shift = SHIFTED.get(args.config, 0.0)
+    base = {"boys_mode": args.boys, "precision": args.precision, "screen_thresh": "float32(1e-10)",
+            "metric_shift": shift}
+    if shift:
+        base["metric_shift_reason"] = ("auxiliary metric numerically singular for this workload "
+                                       "(smallest eigenvalues ~ -1e-13 with exact Boys)")
+    dens_mb = sum(w.densities.nbytes for w in ws) / 1e6
+    base["l2"] = (f"inputs larger than L2 (densities {dens_mb:.0f} MB > 126 MB)" if dens_mb > 126 else
+                  f"inputs smaller than L2 (densities {dens_mb:.1f} MB): not flushed between steps")
+    if args.config == "cfg4":
+        return dict(base, workload="df_coulomb_tensor_batch_64molecules_5to60atoms_lmax3_lauxmax4_4to16states",
+                    nmol=len(ws), natoms_total=int(sum(len(w.mol.atomic_nums) for w in ws)),
+                    nbf_total=int(sum(w.shells.sph_size for w in ws)),
+                    naux_total=int(sum(w.shells_aux.sph_size for w in ws)),
+                    ndens_total=int(sum(len(w.densities) for w in ws)))
+    w = ws[0]
+    c = CONFIGS[args.config]
+    return dict(base,
+                workload=f"df_coulomb_tensor_{c['natoms']}atoms_lmax{c['lmax']}_lauxmax{c['lauxmax']}_{c['nstates']}states",
+                natoms=c["natoms"], lmax=c["lmax"], lauxmax=c["lauxmax"], nstates=c["nstates"],
+                ndens=len(w.densities), nbf=w.shells.sph_size, naux=w.shells_aux.sph_size,
+                nshells=len(w.shells), nshells_aux=len(w.shells_aux))
 
 
 class Clocks:
@@ -160,51 +196,69 @@ def fp64_peak_tflops(torch):
     return 2 * n**3 / best / 1e12
 
 
-def cpu_baseline(w, nints, steps=1):
+def oracle_sample(args, ws, budget_s=20.0):
+    """Time the oracle (C++ OpenMP restatement of the reference driver) on a
+    bounded sample of the workload: whole tensors while they fit the budget,
+    else the leading auxiliary shells of the molecule (every (ab|c) of those c,
+    their metric and solve). Returns (ints/s, cores, description)."""
     import oracle
 
-    oracle.set_boys_mode("reference")
+    from pysisyphus_addons.common.shells import Shells
+
+    oracle.set_boys_mode(args.boys)
+    oracle.set_metric_shift(SHIFTED.get(args.config, 0.0))
     threads = os.cpu_count() or 1
     oracle.set_threads(threads)
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        oracle.contract_coulomb_densities_4d(w.shells, w.shells_aux, w.densities)
-    dt = (time.perf_counter() - t0) / steps
-    return {"value": nints / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{steps} full Coulomb tensor(s) of the same workload, C++ OpenMP restatement of the "
-                      f"reference driver (oracle/), {dt:.2f} s each"}
+    if args.config in ("cfg1", "cfg2"):
+        t0 = time.perf_counter()
+        oracle.contract_coulomb_densities_4d(ws[0].shells, ws[0].shells_aux, ws[0].densities)
+        dt = time.perf_counter() - t0
+        n = oracle.last_stats()["nints"]
+        return n / dt, threads, f"one full Coulomb tensor of the workload ({dt:.2f} s)"
+    if args.config == "cfg4":
+        done, ints, t_tot = 0, 0, 0.0
+        for w in ws:
+            t0 = time.perf_counter()
+            oracle.contract_coulomb_densities_4d(w.shells, w.shells_aux, w.densities)
+            t_tot += time.perf_counter() - t0
+            ints += oracle.last_stats()["nints"]
+            done += 1
+            if t_tot > budget_s:
+                break
+        return ints / t_tot, threads, f"the first {done} molecules of the batch, whole tensors ({t_tot:.1f} s)"
+    w = ws[0]
+    k = 8
+    while True:
+        sub = Shells(w.shells_aux.shells[:k])
+        t0 = time.perf_counter()
+        oracle.contract_coulomb_densities_2d(w.shells, sub, w.densities)
+        dt = time.perf_counter() - t0
+        n = oracle.last_stats()["nints"]
+        if dt > budget_s / 4 or k >= len(w.shells_aux):
+            return n / dt, threads, (f"the first {k} of {len(w.shells_aux)} auxiliary shells of the workload: "
+                                     f"all their surviving (ab|c), metric and solve ({dt:.1f} s)")
+        k *= 2
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from pysisyphus_addons.common.synthetic import config_workload
-
-    import oracle
-
-    w = config_workload(args.config, seed=0)
-    nd = len(w.densities)
-    oracle.set_boys_mode("reference")
-    threads = os.cpu_count() or 1
-    oracle.set_threads(threads)
-    for _ in range(args.warmup):
-        oracle.contract_coulomb_densities_4d(w.shells, w.shells_aux, w.densities)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        oracle.contract_coulomb_densities_4d(w.shells, w.shells_aux, w.densities)
-    dt = (time.perf_counter() - t0) / max(1, args.steps)
-    nints = oracle.last_stats()["nints"]
-    value = nints / dt
+    ws = workloads(args)
+    steps = []
+    for i in range(args.warmup + args.steps):
+        v, threads, sample = oracle_sample(args, ws, budget_s=20.0 if args.config in SHIFTED else 1e9)
+        if i >= args.warmup:
+            steps.append(v)
+    value = statistics.mean(steps) if steps else v
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+        "metric": metric_name(args), "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-        "config": workload_config(args.config, w, nd), "impl": "reference",
+        "config": workload_config(args, ws), "impl": "reference",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": "every step one full Coulomb tensor of the workload; C++ OpenMP restatement of "
-                                   "the reference driver (the Fortran reference and its generated integral "
-                                   "kernels cannot be built here)"},
+                         "sample": "every step: " + sample + "; C++ OpenMP restatement of the reference driver "
+                                   "(the Fortran reference and its generated integral kernels cannot be built here)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -220,7 +274,6 @@ def main():
 
     from pysisyphus_addons import _native as nat
     from pysisyphus_addons import flops as fl
-    from pysisyphus_addons.common.synthetic import config_workload
     from pysisyphus_addons.diabatization import intor as dia
     from pysisyphus_addons.intor import intor as sch
 
@@ -238,26 +291,38 @@ def main():
             dist.barrier()
 
     nat.set_boys_mode(args.boys)
-    w = config_workload(args.config, seed=rank)
-    nd = len(w.densities)
-    ns = w.nstates
-    nbf = w.shells.sph_size
-    orb = nat.Basis(w.shells, "orbital")
-    aux = nat.Basis(w.shells_aux, "aux")
-    ntrip_all, ntrip, nints = nat.count_triplets(orb, aux)
-    qb = sch.int_schwarz_bra(w.shells)
-    qa = sch.int_schwarz_aux(w.shells_aux)
-    flops_3c, ntrip_model, nints_model = fl.model(w.shells, w.shells_aux, qb, qa, nd)
-    assert ntrip_model == ntrip and nints_model == nints, (ntrip_model, ntrip, nints_model, nints)
+    nat.set_metric_shift(SHIFTED.get(args.config, 0.0))
+    nat.set_precision(args.precision, 1e-6)
+    ws = workloads(args, rank)
+    orbs = [nat.Basis(w.shells, "orbital") for w in ws]
+    auxs = [nat.Basis(w.shells_aux, "aux") for w in ws]
+    nints, ntrip_all, ntrip, flops_3c = 0, 0, 0, 0.0
+    for w, o, a in zip(ws, orbs, auxs):
+        t_all, t_c, n_i = nat.count_triplets(o, a)
+        nints += n_i
+        ntrip_all += t_all
+        ntrip += t_c
+        if len(ws) == 1:
+            qb = sch.int_schwarz_bra(w.shells)
+            qa = sch.int_schwarz_aux(w.shells_aux)
+            f, tm, im = fl.model(w.shells, w.shells_aux, qb, qa, len(w.densities))
+            assert tm == t_c and im == n_i, (tm, t_c, im, n_i)
+            flops_3c += f
 
-    dens = torch.from_numpy(np.ascontiguousarray(w.densities)).cuda()
-    out = torch.empty(ns**4, dtype=torch.float64, device="cuda")
+    dens = [torch.from_numpy(np.ascontiguousarray(w.densities)).cuda() for w in ws]
+    ns = [w.nstates for w in ws]
+    outs = [torch.empty(k**4, dtype=torch.float64, device="cuda") for k in ns]
     stream = torch.cuda.current_stream()
     lib = nat.load()
+    batched = args.config == "cfg4"
 
     def step():
-        nat.check(lib.pa_df_4d(orb.handle, aux.handle, nd, nbf, dens.data_ptr(), nat.PA_LAYOUT_C, ns,
-                               out.data_ptr(), stream.cuda_stream))
+        if batched:
+            nat.df_4d_batch(orbs, auxs, dens, ns, outs, use_graph=True, stream=stream.cuda_stream)
+            return
+        w, d = ws[0], dens[0]
+        nat.check(lib.pa_df_4d(orbs[0].handle, auxs[0].handle, d.shape[0], d.shape[1], d.data_ptr(),
+                               nat.PA_LAYOUT_C, ns[0], outs[0].data_ptr(), stream.cuda_stream))
 
     if args.profile:
         for _ in range(args.warmup + args.steps):
@@ -298,19 +363,36 @@ def main():
     step_s = elapsed / args.steps
     value = total_ints / step_s
 
-    # end to end: the public Python API with pinned host densities (H2D + D2H inside)
+    # end to end through the public Python API: pinned host densities copied in
+    # and the tensors copied out in every call
     e2e = None
     if not args.no_e2e:
-        pinned = torch.from_numpy(np.ascontiguousarray(w.densities)).pin_memory().numpy()
+        pinned = [torch.from_numpy(np.ascontiguousarray(w.densities)).pin_memory() for w in ws]
+        if batched:
+            host_out = [torch.empty(k**4, dtype=torch.float64).pin_memory() for k in ns]
+
+            def call():
+                for dd, hp in zip(dens, pinned):
+                    dd.copy_(hp, non_blocking=True)
+                nat.df_4d_batch(orbs, auxs, dens, ns, outs, use_graph=True, stream=stream.cuda_stream)
+                for ho, o in zip(host_out, outs):
+                    ho.copy_(o, non_blocking=True)
+                torch.cuda.synchronize()
+                return host_out[0].numpy()
+        else:
+            arr = pinned[0].numpy()
+
+            def call():
+                return dia.contract_coulomb_densities_4d(ws[0].shells, ws[0].shells_aux, arr)
         for _ in range(2):
-            R = dia.contract_coulomb_densities_4d(w.shells, w.shells_aux, pinned)
+            R = call()
         torch.cuda.synchronize()
         barrier()
         iters = []
         t0 = time.perf_counter()
         for _ in range(args.steps):
             ti = time.perf_counter()
-            R = dia.contract_coulomb_densities_4d(w.shells, w.shells_aux, pinned)
+            R = call()
             iters.append((time.perf_counter() - ti) * 1e3)
         torch.cuda.synchronize()
         e2e_s = (time.perf_counter() - t0) / args.steps
@@ -318,40 +400,48 @@ def main():
             t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             e2e_s = float(t.item())
-        keep = [a for a in w.shells.as_arrays(fortran=True)] + [a for a in w.shells_aux.as_arrays(fortran=True)]
-        h2d = int(pinned.nbytes + sum(a.nbytes for a in keep))
+        keep = [a for w in ws for a in (w.shells.as_arrays(fortran=True) + w.shells_aux.as_arrays(fortran=True))]
+        h2d = int(sum(p.numpy().nbytes for p in pinned) + (0 if batched else sum(a.nbytes for a in keep)))
+        d2h = int(sum(k**4 * 8 for k in ns))
         e2e = {"value": total_ints / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": int(R.nbytes), "ms_per_step": e2e_s * 1e3,
+               "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3,
+               "api": "pysisyphus_addons._native.df_4d_batch (device buffers filled from pinned host memory)"
+               if batched else "pysisyphus_addons.diabatization.intor.contract_coulomb_densities_4d",
                "ms_per_call": [round(x, 3) for x in iters]}
 
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
         return
-    peak = fp64_peak_tflops(torch)
-    ms3 = statistics.mean(ms3c)
-    achieved = flops_3c / (ms3 / 1e3) / 1e12
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": metric_name(args), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": step_s * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-        "config": dict(workload_config(args.config, w, nd), boys_mode=args.boys,
+        "config": dict(workload_config(args, ws),
                        parallelism=f"independent molecules x{world}" if world > 1 else "single GPU"),
-        "roofline": {"bound": "fp64", "kernel": "k_df3c (all classes) + ordered reduction",
-                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                     "peak_source": "FP64 GEMM (torch.matmul float64 8192^3) measured in this run; "
-                                    "MEASURED_PEAKS.json has no FP64 figure",
-                     "flops_per_step_3c": flops_3c, "ms_3c": ms3, "traffic": None},
-        "phases_ms": {k: statistics.mean(p[k] for p in phases) for k in phases[0]},
         "screening": {"triplets": ntrip_all, "computed": ntrip, "ints": nints},
         "gpu_launches": launches,
-        "gpu_launches_3c": launches3c,
         "clocks": clk,
     }
+    if not batched:
+        peak = fp64_peak_tflops(torch)
+        ms3 = statistics.mean(ms3c)
+        achieved = flops_3c / (ms3 / 1e3) / 1e12
+        line["roofline"] = {
+            "bound": "tensor", "pipe": "FP64 (DMMA m8n8k4 tensor cores + FP64 FMA)",
+            "kernel": "k_df3c<LAB,LC> (all classes) + ordered reduction",
+            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "peak_source": "of measured: FP64 GEMM (torch.matmul float64 8192^3) in this run; "
+                           "MEASURED_PEAKS.json has no FP64 figure",
+            "flops_per_step_3c": flops_3c, "ms_3c": ms3, "traffic": None}
+        line["phases_ms"] = {k: statistics.mean(p[k] for p in phases) for k in phases[0]}
+        line["gpu_launches_3c"] = launches3c
     if e2e:
         line["e2e"] = e2e
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(w, nints)
+        v, threads, sample = oracle_sample(args, ws)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": sample + "; C++ OpenMP restatement of the reference driver (oracle/)"}
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -141,8 +141,9 @@ int pa_set_metric_shift(double shift);
  * contraction in FP32; their contributions are accumulated in FP64. */
 int pa_set_precision(int mode, double fp32_thresh);
 /* Granularity of the three-center work queue: work items per SM and shell
- * class (default 4). Finer items shorten the tail of each class launch and
- * cost more partial sums; the best value depends on the system size. */
+ * class; 0 (default) picks it from the system size (2 at 40 atoms, 32 at 200).
+ * Finer items shorten the tail of each class launch and cost more partial
+ * sums. */
 int pa_set_items_per_sm(int items);
 int pa_get_precision(void);
 

@@ -103,7 +103,17 @@ __global__ void __launch_bounds__(128) k_unit_setup(DevBasis B, const int2* __re
 }
 
 // ---------------------------------------------------------------------------
-constexpr int kSchwarzRowChunk = 8;
+// Schwarz values of high-L pairs, one block per pair. For every pair of bra
+// units (iu, ku) the block is
+//   (ab|ab)[r][s] = sum_(t,t') E_iu[r][t] (-1)^|t'| R[t + t'] E_ku[s][t'],
+// two small GEMMs run on the FP64 tensor cores (DMMA m8n8k4):
+//   Y = E_iu * H with H[t][t'] = (-1)^|t'| R[t + t'] gathered through the
+//   multi-index sum table, then (ab|ab) += Y * E_ku^T.
+__device__ __forceinline__ void sw_dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
 
 __global__ void __launch_bounds__(256) k_schwarz_bra(DevBasis B, const int2* __restrict__ pair_ab,
                                                      const int* __restrict__ pair_unit0,
@@ -120,14 +130,17 @@ __global__ void __launch_bounds__(256) k_schwarz_bra(DevBasis B, const int2* __r
   const int NH = ncum(la + lb);
   const int L4 = 2 * (la + lb);
   const int NR = ncum(L4);
-  double* Rn = smem;                  // L4 + 1 (padded to 32)
+  const int MT = (nab + 7) / 8, NT = (NH + 7) / 8, KT = (NH + 3) / 4;
+  const int YS = NT * 8 + 1;          // row stride of Y
+  double* Rn = smem;                  // 32
   double* R0 = Rn + 32;               // NR
   double* R1 = R0 + NR;               // NR
-  double* Y = R1 + NR;                // kSchwarzRowChunk * NH
-  double* out = Y + kSchwarzRowChunk * NH;  // nab * nab
+  double* Y = R1 + NR;                // [MT * 8][YS]
+  double* out = Y + MT * 8 * YS;      // [nab][nab]
   __shared__ double red[8];
   const IndexTables* it = dt.idx;
-  for (int i = threadIdx.x; i < nab * nab; i += blockDim.x) out[i] = 0.0;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
+  for (int i = tid; i < nab * nab; i += blockDim.x) out[i] = 0.0;
   const int u0 = pair_unit0[pair];
   const int nu = sa.y * sb.y;
   for (int iu = 0; iu < nu; ++iu)
@@ -138,45 +151,56 @@ __global__ void __launch_bounds__(256) k_schwarz_bra(DevBasis B, const int2* __r
       const double T = alpha * (X * X + Yd * Yd + Z * Z);
       const double pref = kTwoPi52 / (p * q * sqrt(pq));
       __syncthreads();  // previous users of Rn / R buffers / Y are done
-      if (threadIdx.x <= L4) {
-        const int n = threadIdx.x;
+      if (tid <= L4) {
         double f = pref;
-        for (int k = 0; k < n; ++k) f *= -2.0 * alpha;
-        Rn[n] = f * boys_n(dt, boys_mode, n, T);
+        for (int k = 0; k < tid; ++k) f *= -2.0 * alpha;
+        Rn[tid] = f * boys_n(dt, boys_mode, tid, T);
       }
       __syncthreads();
-      hermite_R(it, L4, Rn, X, Yd, Z, R0, R1, threadIdx.x, blockDim.x, BlockSync());
+      hermite_R(it, L4, Rn, X, Yd, Z, R0, R1, tid, blockDim.x, BlockSync());
       const double* Ei = U.esph + U.unit_esph[u0 + iu];
       const double* Ek = U.esph + U.unit_esph[u0 + ku];
-      for (int r0 = 0; r0 < nab; r0 += kSchwarzRowChunk) {
-        const int rows = min(kSchwarzRowChunk, nab - r0);
-        for (int idx = threadIdx.x; idx < rows * NH; idx += blockDim.x) {
-          const int rr = idx / NH, tp = idx - rr * NH;
-          const double* e = Ei + (r0 + rr) * NH;
-          double y = 0.0;
-          const int16_t* sidx = dt.sum_idx + tp;  // column tp of the sum table (symmetric)
-          for (int t = 0; t < NH; ++t) y = fma(e[t], R0[__ldg(sidx + t * kNSum)], y);
-          const int deg = it->xyz[tp][3];
-          Y[rr * NH + tp] = (deg & 1) ? -y : y;
+      // Y = Ei * H, one 8 x 8 tile per warp at a time
+      for (int tile = warp; tile < MT * NT; tile += 8) {
+        const int mt = tile / NT, nt = tile - mt * NT;
+        const int r = 8 * mt + g, c = 8 * nt + g;
+        double y0 = 0.0, y1 = 0.0;
+        for (int k4 = 0; k4 < KT; ++k4) {
+          const int k = 4 * k4 + t4;
+          const double a = (r < nab && k < NH) ? Ei[r * NH + k] : 0.0;
+          const double b = (k < NH && c < NH) ? R0[__ldg(dt.sum_idx + k * kNSum + c)] : 0.0;
+          sw_dmma(y0, y1, a, b);
         }
-        __syncthreads();
-        for (int idx = threadIdx.x; idx < rows * nab; idx += blockDim.x) {
-          const int rr = idx / nab, s = idx - rr * nab;
-          const double* e = Ek + s * NH;
-          const double* yr = Y + rr * NH;
-          double v = 0.0;
-          for (int tp = 0; tp < NH; ++tp) v = fma(yr[tp], e[tp], v);
-          out[(r0 + rr) * nab + s] += v;
+        const int cc = 8 * nt + 2 * t4;
+        double* yrow = Y + (8 * mt + g) * YS;
+        if (cc < NH) yrow[cc] = (it->xyz[cc][3] & 1) ? -y0 : y0;
+        if (cc + 1 < NH) yrow[cc + 1] = (it->xyz[cc + 1][3] & 1) ? -y1 : y1;
+      }
+      __syncthreads();
+      // out += Y * Ek^T
+      const int MT2 = MT, NT2 = (nab + 7) / 8;
+      for (int tile = warp; tile < MT2 * NT2; tile += 8) {
+        const int mt = tile / NT2, nt = tile - mt * NT2;
+        const int r = 8 * mt + g, c = 8 * nt + g;
+        double o0 = 0.0, o1 = 0.0;
+        for (int k4 = 0; k4 < KT; ++k4) {
+          const int k = 4 * k4 + t4;
+          const double a = (k < NH) ? Y[r * YS + k] : 0.0;  // rows >= nab of Y are never read below
+          const double b = (k < NH && c < nab) ? Ek[c * NH + k] : 0.0;
+          sw_dmma(o0, o1, a, b);
         }
-        __syncthreads();
+        const int cc = 8 * nt + 2 * t4;
+        if (r < nab && cc < nab) out[r * nab + cc] += o0;
+        if (r < nab && cc + 1 < nab) out[r * nab + cc + 1] += o1;
       }
     }
-  double s2 = 0.0;
-  for (int i = threadIdx.x; i < nab * nab; i += blockDim.x) s2 += out[i] * out[i];
-  for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s2;
   __syncthreads();
-  if (threadIdx.x == 0) {
+  double s2 = 0.0;
+  for (int i = tid; i < nab * nab; i += blockDim.x) s2 += out[i] * out[i];
+  for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+  if (lane == 0) red[warp] = s2;
+  __syncthreads();
+  if (tid == 0) {
     double tot = 0.0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
     Qab[pair] = sqrt(sqrt(tot));
@@ -441,15 +465,18 @@ int launch_unit_setup(const DevBasis& B, const int2* pair_ab, UnitArrays U, int 
   return 1;
 }
 
-size_t schwarz_bra_smem(int lab_max) {
-  const int NH = ncum(lab_max), NR = ncum(2 * lab_max);
-  const int nab = (2 * PA_LMAX + 1) * (2 * PA_LMAX + 1);
-  int nab_max = 1;
+// Shared memory of k_schwarz_bra for the pairs of class Lab = lab.
+size_t schwarz_bra_smem(int lab) {
+  size_t best = 0;
   for (int la = 0; la <= PA_LMAX; ++la)
-    for (int lb = 0; lb <= la; ++lb)
-      if (la + lb <= lab_max) nab_max = max(nab_max, (2 * la + 1) * (2 * lb + 1));
-  (void)nab;
-  return sizeof(double) * (32 + 2 * NR + kSchwarzRowChunk * NH + nab_max * nab_max);
+    for (int lb = 0; lb <= la; ++lb) {
+      if (la + lb != lab) continue;
+      const int nab = (2 * la + 1) * (2 * lb + 1), NH = ncum(la + lb), NR = ncum(2 * (la + lb));
+      const int MT = (nab + 7) / 8, NT = (NH + 7) / 8;
+      const size_t d = 32 + 2 * NR + static_cast<size_t>(MT) * 8 * (NT * 8 + 1) + nab * nab;
+      best = best > d ? best : d;
+    }
+  return sizeof(double) * best;
 }
 
 int launch_schwarz_bra(const DevBasis& B, const int2* pair_ab, const int* pair_unit0,
@@ -466,13 +493,14 @@ int launch_schwarz_bra(const DevBasis& B, const int2* pair_ab, const int* pair_u
         B, pair_ab, pair_unit0, class_pair, U, nlow, dt, boys_mode, Qab);
     ++launches;
   }
-  const int nhigh = P.npairs - nlow;
-  if (nhigh > 0) {
-    const size_t smem = schwarz_bra_smem(P.lab_max);
-    cudaFuncSetAttribute(k_schwarz_bra, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         static_cast<int>(smem));
-    k_schwarz_bra<<<nhigh, 256, smem, s>>>(B, pair_ab, pair_unit0, class_pair + nlow, U, nhigh, dt,
-                                           boys_mode, Qab);
+  // one launch per higher class, each with its own shared-memory footprint
+  cudaFuncSetAttribute(k_schwarz_bra, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(schwarz_bra_smem(2 * PA_LMAX)));
+  for (int lab = split; lab <= P.lab_max; ++lab) {
+    const int off = P.pair_class_off[lab], n = P.pair_class_off[lab + 1] - off;
+    if (n <= 0) continue;
+    k_schwarz_bra<<<n, 256, schwarz_bra_smem(lab), s>>>(B, pair_ab, pair_unit0, class_pair + off, U, n, dt,
+                                                        boys_mode, Qab);
     ++launches;
   }
   return launches;

@@ -22,7 +22,7 @@ struct BraPrepArgs {
   int n_class = 0;                        // slots in this class (stride of z)
 };
 
-size_t schwarz_bra_smem(int lab_max);
+size_t schwarz_bra_smem(int lab);
 int launch_bra_prep(const DevBasis& B, const int2* pair_ab, UnitArrays U, const BraPrepArgs& a,
                     int lab, cudaStream_t s);
 

@@ -24,98 +24,56 @@ namespace {
 constexpr int NB = 64;
 
 // Factorize the nb x nb diagonal block at (j0, j0) in place (lower) and write
-// its inverse (lower, zeros above the diagonal, NB x NB) to dinv.
-// Thread (r, g) = (tid % 64, tid / 64) keeps row r, columns j = 4 q + g
-// (q = 0..15) in registers; each column / row step is two block barriers and
-// at most 16 FMAs per thread.
-__global__ void __launch_bounds__(256) k_potrf_diag_inv(double* A, long long lda, int j0, int nb,
-                                                        double* dinv, int* info) {
-  __shared__ double Ls[NB][NB + 1];  // the factor, filled column by column
-  __shared__ double diag[NB];
-  __shared__ double xrow[2][NB];
-  const int tid = threadIdx.x, r = tid & (NB - 1), g = tid >> 6;
-  double a[16];
-#pragma unroll
-  for (int q = 0; q < 16; ++q) {
-    const int j = 4 * q + g;
-    a[q] = (r < nb && j <= r) ? A[(j0 + r) + lda * (j0 + j)] : (r == j ? 1.0 : 0.0);
-  }
-  if (g == (r & 3)) {
-#pragma unroll
-    for (int q = 0; q < 16; ++q)
-      if (4 * q + g == r) diag[r] = a[q];
-  }
+// its inverse (lower, zeros above the diagonal, NB x NB) to dinv. 64 threads:
+// thread r owns row r during the factorization (right-looking, column by
+// column, three cheap 64-thread barriers per column) and column r during the
+// inversion, where every thread solves L x = e_r on its own.
+__global__ void __launch_bounds__(NB) k_potrf_diag_inv(double* A, long long lda, int j0, int nb,
+                                                       double* dinv, int* info) {
+  extern __shared__ double dsm[];
+  double(*S)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(dsm);                   // the block, then L
+  double(*Xs)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(dsm + NB * (NB + 1));  // L^-1
+  const int r = threadIdx.x;
+  for (int c = 0; c < NB; ++c)
+    S[r][c] = (r < nb && c < nb) ? (c <= r ? A[(j0 + r) + lda * (j0 + c)] : 0.0) : (r == c ? 1.0 : 0.0);
   __syncthreads();
-  // Cholesky, right-looking over columns k
   for (int k = 0; k < NB; ++k) {
-    double dkk = diag[k];
+    double dkk = S[k][k];
     if (!(dkk > 0.0)) {
-      if (k < nb && tid == 0) atomicCAS(info, 0, j0 + k + 1);
+      if (k < nb && r == 0) atomicCAS(info, 0, j0 + k + 1);
       dkk = 1.0;  // keep the factor finite; the error is reported through info
     }
     const double d = sqrt(dkk);
-    const int qk = k >> 2;
-    if (g == (k & 3) && r >= k) {
-      double v = 0.0;
-#pragma unroll
-      for (int q = 0; q < 16; ++q)
-        if (q == qk) v = a[q];
-      v = (r == k) ? d : v / d;
-#pragma unroll
-      for (int q = 0; q < 16; ++q)
-        if (q == qk) a[q] = v;
-      Ls[r][k] = v;
-    }
-    __syncthreads();
-    const double lik = r > k ? Ls[r][k] : 0.0;
-#pragma unroll
-    for (int q = 0; q < 16; ++q) {
-      const int j = 4 * q + g;
-      if (j > k && j <= r) a[q] = fma(-lik, Ls[j][k], a[q]);
-    }
-    if (r == k + 1 && g == (r & 3)) {
-#pragma unroll
-      for (int q = 0; q < 16; ++q)
-        if (4 * q + g == r) diag[r] = a[q];
-    }
-    __syncthreads();
-  }
-  // write the factor back
-#pragma unroll
-  for (int q = 0; q < 16; ++q) {
-    const int j = 4 * q + g;
-    if (r < nb && j <= r) A[(j0 + r) + lda * (j0 + j)] = a[q];
-  }
-  // inverse X = L^-1 by rows: X[k][:] /= L_kk, then X[i][:] -= L_ik X[k][:]
-#pragma unroll
-  for (int q = 0; q < 16; ++q) a[q] = (4 * q + g == r) ? 1.0 : 0.0;
-  for (int k = 0; k < NB; ++k) {
-    if (r == k) {
-      const double inv = 1.0 / Ls[k][k];
-#pragma unroll
-      for (int q = 0; q < 16; ++q) {
-        const int j = 4 * q + g;
-        if (j <= k) {
-          a[q] *= inv;
-          xrow[k & 1][j] = a[q];
-        }
-      }
-    }
+    __syncthreads();  // every thread has read S[k][k]
+    if (r == k) S[k][k] = d;
+    if (r > k) S[r][k] = S[r][k] / d;
     __syncthreads();
     if (r > k) {
-      const double lik = Ls[r][k];
-#pragma unroll
-      for (int q = 0; q < 16; ++q) {
-        const int j = 4 * q + g;
-        if (j <= k) a[q] = fma(-lik, xrow[k & 1][j], a[q]);
-      }
+      const double lrk = S[r][k];
+      for (int j = k + 1; j <= r; ++j) S[r][j] = fma(-lrk, S[j][k], S[r][j]);
     }
+    __syncthreads();
   }
-#pragma unroll
-  for (int q = 0; q < 16; ++q) {
-    const int j = 4 * q + g;
-    dinv[r + NB * j] = (r < nb && j <= r) ? a[q] : 0.0;
+  // write the factor back (row r)
+  for (int c = 0; c <= r && c < nb; ++c)
+    if (r < nb) A[(j0 + r) + lda * (j0 + c)] = S[r][c];
+  // column r of L^-1 by forward substitution
+  for (int i = 0; i < NB; ++i) {
+    double v = 0.0;
+    if (i >= r) {
+      double v0 = (i == r) ? 1.0 : 0.0, v1 = 0.0;
+      int k = r;
+      for (; k + 1 < i; k += 2) {
+        v0 = fma(-S[i][k], Xs[k][r], v0);
+        v1 = fma(-S[i][k + 1], Xs[k + 1][r], v1);
+      }
+      if (k < i) v0 = fma(-S[i][k], Xs[k][r], v0);
+      v = (v0 + v1) / S[i][i];
+    }
+    Xs[i][r] = v;
   }
+  __syncthreads();
+  for (int c = 0; c < NB; ++c) dinv[r + NB * c] = (r < nb && c < nb) ? Xs[r][c] : 0.0;
 }
 
 // Panel below the diagonal block (rows j0 + NB.., columns j0..j0 + nb):
@@ -352,13 +310,15 @@ int cholesky_lower(double* A, int n, int* d_info, double* work, cudaStream_t s) 
   int launches = 0;
   cudaFuncSetAttribute(k_panel_inplace, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        static_cast<int>(2 * kTileSmem));
+  cudaFuncSetAttribute(k_potrf_diag_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(2 * kTileSmem));
   cudaMemsetAsync(d_info, 0, sizeof(int), s);
   const int nblk = (n + NB - 1) / NB;
   // per block column: diagonal factor + inverse, panel P := P L_kk^-T, A22 -= P P^T
   for (int b = 0; b < nblk; ++b) {
     const int j0 = b * NB, nb = std::min(NB, n - j0);
     double* Db = work + static_cast<size_t>(b) * NB * NB;
-    k_potrf_diag_inv<<<1, 256, 0, s>>>(A, n, j0, nb, Db, d_info);
+    k_potrf_diag_inv<<<1, NB, 2 * kTileSmem, s>>>(A, n, j0, nb, Db, d_info);
     ++launches;
     const int rest = n - j0 - nb;
     if (rest > 0) {

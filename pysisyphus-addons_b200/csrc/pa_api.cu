@@ -420,7 +420,13 @@ void layout_df(Carver& c, const pa_basis_s* orb, const pa_basis_s* aux, int nd, 
   b->df_raw = c.take<double>(static_cast<size_t>(naux) * nd);
   b->cub_bytes = cub_temp_bytes(orb, aux);
   b->cub_tmp = c.take<char>(b->cub_bytes);
-  // partial slabs
+  // partial slabs; the work-item granularity grows with the system size (on
+  // B200: 2 items per SM and class at 40 atoms, 32 at 200 atoms were best)
+  if (items_per_sm <= 0) {
+    const double T = static_cast<double>(P.npairs) * aux->host.shells.size();
+    items_per_sm = static_cast<int>(std::lround(2.0 * std::pow(std::max(T, 1.0) / 1.85e7, 0.55)));
+    items_per_sm = std::min(32, std::max(2, items_per_sm));
+  }
   b->runs.clear();
   size_t part_total = 0;
   const AuxLists& X = aux->aux;
@@ -1369,7 +1375,7 @@ int pa_get_precision(void) {
 }
 
 int pa_set_items_per_sm(int items) {
-  if (items < 1 || items > 1024) return fail(PA_ERR_ARG, "items per SM must be in [1, 1024]");
+  if (items < 0 || items > 1024) return fail(PA_ERR_ARG, "items per SM must be in [0, 1024] (0 = by size)");
   std::lock_guard<std::mutex> lk(g_opt_mu);
   g_opts.items_per_sm = items;
   return PA_OK;

@@ -78,7 +78,7 @@ struct Options {
   double metric_shift = 0.0;  // added to the diagonal of (P|Q) before the Cholesky
   int precision = 0;          // 0 = FP64 throughout, 1 = mixed (FP32 recurrences for weak triplets)
   double fp32_thresh = 1e-6;  // Schwarz bound below which the mixed form uses FP32
-  int items_per_sm = 4;       // work items per SM and class of the three-center kernel
+  int items_per_sm = 0;       // work items per SM and class of the three-center kernel (0 = by size)
 };
 
 struct Stats {

@@ -181,7 +181,7 @@ def set_precision(mode="fp64", fp32_thresh=1e-6):
 
 
 def set_items_per_sm(items):
-    """Work items per SM and shell class of the three-center queue (default 4)."""
+    """Work items per SM and shell class of the three-center queue (0 = by size, the default)."""
     check(load().pa_set_items_per_sm(int(items)))
 
 
