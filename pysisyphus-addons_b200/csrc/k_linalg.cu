@@ -1,9 +1,8 @@
 // Dense FP64 linear algebra of the density-fitting path (column-major):
 //  * blocked right-looking Cholesky of the metric, lower triangle
 //    (replaces dpotrf("L"), common/linalg.f90:78); each 64 x 64 diagonal block is
-//    factorized (and inverted, for the later solves) by one thread block, the
-//    panel below it solved against it in place and the trailing matrix updated
-//    by a lower GEMM;
+//    factorized and inverted by one thread block, the panel below it is
+//    scaled in place and the trailing matrix updated by a lower GEMM;
 //  * L^-1 df as a blocked forward substitution on the density columns, using
 //    the inverted diagonal blocks (replaces dtrtri("L","N"), common/linalg.f90:81,
 //    followed by dtrmm("L","L","N","N"), diabatization/intor.f90:198: the
@@ -24,89 +23,156 @@ namespace {
 constexpr int NB = 64;
 
 // Factorize the nb x nb diagonal block at (j0, j0) in place (lower) and write
-// its inverse (lower, zeros above the diagonal, NB x NB) to dinv. 64 threads:
-// thread r owns row r during the factorization (right-looking, column by
-// column, three cheap 64-thread barriers per column) and column r during the
-// inversion, where every thread solves L x = e_r on its own.
-__global__ void __launch_bounds__(NB) k_potrf_diag_inv(double* A, long long lda, int j0, int nb,
-                                                       double* dinv, int* info) {
+// its inverse (lower, zeros above the diagonal, NB x NB) to dinv. Both steps
+// use few barriers:
+//  * Cholesky: per sub-block column, one warp factors the 16 x 16 diagonal
+//    sub-block, one thread per row solves the 16-wide panel below it, and all
+//    threads update the trailing lower triangle;
+//  * inverse: elimination on the identity, one step (and one barrier) per
+//    row, the rows of X held in registers.
+constexpr int SB = 16;
+__global__ void __launch_bounds__(256) k_potrf_diag_inv(double* A, long long lda, int j0, int nb,
+                                                        double* dinv, int* info) {
   extern __shared__ double dsm[];
-  double(*S)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(dsm);                   // the block, then L
-  double(*Xs)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(dsm + NB * (NB + 1));  // L^-1
-  const int r = threadIdx.x;
-  for (int c = 0; c < NB; ++c)
+  double(*S)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(dsm);                       // the block, then L
+  double(*Xs)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(dsm + NB * (NB + 1));      // L^-1
+  double(*Ts)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(dsm + 2 * NB * (NB + 1));  // rows of X in flight
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int idx = tid; idx < NB * NB; idx += 256) {
+    const int r = idx & (NB - 1), c = idx >> 6;
     S[r][c] = (r < nb && c < nb) ? (c <= r ? A[(j0 + r) + lda * (j0 + c)] : 0.0) : (r == c ? 1.0 : 0.0);
-  __syncthreads();
-  for (int k = 0; k < NB; ++k) {
-    double dkk = S[k][k];
-    if (!(dkk > 0.0)) {
-      if (k < nb && r == 0) atomicCAS(info, 0, j0 + k + 1);
-      dkk = 1.0;  // keep the factor finite; the error is reported through info
-    }
-    const double d = sqrt(dkk);
-    __syncthreads();  // every thread has read S[k][k]
-    if (r == k) S[k][k] = d;
-    if (r > k) S[r][k] = S[r][k] / d;
-    __syncthreads();
-    if (r > k) {
-      const double lrk = S[r][k];
-      for (int j = k + 1; j <= r; ++j) S[r][j] = fma(-lrk, S[j][k], S[r][j]);
-    }
-    __syncthreads();
+    Xs[r][c] = 0.0;
   }
-  // write the factor back (row r)
-  for (int c = 0; c <= r && c < nb; ++c)
-    if (r < nb) A[(j0 + r) + lda * (j0 + c)] = S[r][c];
-  // column r of L^-1 by forward substitution
-  for (int i = 0; i < NB; ++i) {
-    double v = 0.0;
-    if (i >= r) {
-      double v0 = (i == r) ? 1.0 : 0.0, v1 = 0.0;
-      int k = r;
-      for (; k + 1 < i; k += 2) {
-        v0 = fma(-S[i][k], Xs[k][r], v0);
-        v1 = fma(-S[i][k + 1], Xs[k + 1][r], v1);
+  __syncthreads();
+  for (int k0 = 0; k0 < NB; k0 += SB) {
+    // 16 x 16 diagonal sub-block, lanes 0..15 own its rows
+    if (warp == 0) {
+      const int r = k0 + lane;
+      for (int k = k0; k < k0 + SB; ++k) {
+        double dkk = S[k][k];
+        if (!(dkk > 0.0)) {
+          if (k < nb && lane == 0) atomicCAS(info, 0, j0 + k + 1);
+          dkk = 1.0;  // keep the factor finite; the error is reported through info
+        }
+        const double d = sqrt(dkk);
+        __syncwarp();
+        if (lane < SB && r == k) S[k][k] = d;
+        if (lane < SB && r > k) S[r][k] = S[r][k] / d;
+        __syncwarp();
+        if (lane < SB && r > k) {
+          const double lrk = S[r][k];
+          for (int j = k + 1; j <= r; ++j) S[r][j] = fma(-lrk, S[j][k], S[r][j]);
+        }
+        __syncwarp();
       }
-      if (k < i) v0 = fma(-S[i][k], Xs[k][r], v0);
-      v = (v0 + v1) / S[i][i];
     }
-    Xs[i][r] = v;
+    __syncthreads();
+    // panel rows below: x L11^T = a by forward substitution, one thread per row
+    const int r = k0 + SB + tid;
+    if (r < NB) {
+      for (int j = k0; j < k0 + SB; ++j) {
+        double v = S[r][j];
+        for (int k = k0; k < j; ++k) v = fma(-S[r][k], S[j][k], v);
+        S[r][j] = v / S[j][j];
+      }
+    }
+    __syncthreads();
+    // trailing lower triangle: S[r][c] -= sum_k S[r][k] S[c][k], k in the sub-block
+    const int m = NB - k0 - SB;
+    for (int e = tid; e < m * m; e += 256) {
+      const int rr = k0 + SB + e / m, cc = k0 + SB + e % m;
+      if (cc > rr) continue;
+      double v = S[rr][cc];
+#pragma unroll
+      for (int k = 0; k < SB; ++k) v = fma(-S[rr][k0 + k], S[cc][k0 + k], v);
+      S[rr][cc] = v;
+    }
+    __syncthreads();
+  }
+  // write the factor back
+  for (int idx = tid; idx < NB * NB; idx += 256) {
+    const int r = idx & (NB - 1), c = idx >> 6;
+    if (r < nb && c <= r) A[(j0 + r) + lda * (j0 + c)] = S[r][c];
+  }
+  // inverse X = L^-1 by elimination on the identity, row k at step k:
+  // X[k][:] /= L_kk, then X[i][:] -= L_ik X[k][:] for i > k. Thread
+  // (r, g) = (tid % 64, tid / 64) keeps row r, columns 4 q + g, in registers.
+  {
+    const int r = tid & (NB - 1), g = tid >> 6;
+    double x[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) x[q] = (4 * q + g == r) ? 1.0 : 0.0;
+    for (int k = 0; k < NB; ++k) {
+      if (r == k) {
+        const double inv = 1.0 / S[k][k];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int j = 4 * q + g;
+          if (j <= k) {
+            x[q] *= inv;
+            Ts[k & 1][j] = x[q];
+          }
+        }
+      }
+      __syncthreads();
+      if (r > k) {
+        const double lik = S[r][k];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int j = 4 * q + g;
+          if (j <= k) x[q] = fma(-lik, Ts[k & 1][j], x[q]);
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 16; ++q) Xs[r][4 * q + g] = (4 * q + g <= r) ? x[q] : 0.0;
   }
   __syncthreads();
-  for (int c = 0; c < NB; ++c) dinv[r + NB * c] = (r < nb && c < nb) ? Xs[r][c] : 0.0;
+  for (int idx = tid; idx < NB * NB; idx += 256) {
+    const int r = idx & (NB - 1), c = idx >> 6;
+    dinv[r + NB * c] = (r < nb && c <= r) ? Xs[r][c] : 0.0;
+  }
 }
 
 // Panel below the diagonal block (rows j0 + NB.., columns j0..j0 + nb):
-// P := P L11^-T in place, by forward substitution against the factored
-// diagonal block L11 (what dtrsm does inside dpotrf). Multiplying by the
-// explicit inverse of L11 instead loses accuracy on the ill-conditioned
-// blocks of a nearly singular metric. One block of 64 threads per 64 rows;
-// thread r solves row r: x_j = (p_j - sum_(k<j) L_jk x_k) / L_jj.
-__global__ void __launch_bounds__(NB) k_panel_inplace(double* A, long long lda, int j0, int nb,
-                                                      int rows) {
+// P := P Dinv^T in place. One block per 64 rows; the whole row slice is read
+// into shared memory before it is overwritten.
+__global__ void __launch_bounds__(256) k_panel_inplace(double* A, long long lda, int j0, int nb,
+                                                       int rows, const double* __restrict__ dinv) {
   extern __shared__ double psm[];
-  double(*P)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(psm);                   // [row][p]
-  double(*Ls)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(psm + NB * (NB + 1));  // [j][k]
+  double(*P)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(psm);           // [row][p]
+  double(*D)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(psm + NB * (NB + 1));  // [j][p]
   const int tid = threadIdx.x;
   const int i0 = blockIdx.x * NB;
   double* base = A + (j0 + nb) + lda * j0;
-  for (int idx = tid; idx < NB * NB; idx += NB) {
-    const int i = idx & (NB - 1), c = idx >> 6;
-    P[i][c] = (i0 + i < rows && c < nb) ? base[(i0 + i) + lda * c] : 0.0;
-    Ls[i][c] = (i < nb && c <= i) ? A[(j0 + i) + lda * (j0 + c)] : 0.0;
+#pragma unroll
+  for (int idx = tid; idx < NB * NB; idx += 256) {
+    const int i = idx & (NB - 1), p = idx >> 6;
+    P[i][p] = (i0 + i < rows && p < nb) ? base[(i0 + i) + lda * p] : 0.0;
+    D[i][p] = dinv[i + NB * p];
   }
   __syncthreads();
-  const int r = tid;
-  for (int j = 0; j < nb; ++j) {
-    double v = P[r][j];
-    for (int k = 0; k < j; ++k) v = fma(-Ls[j][k], P[r][k], v);
-    P[r][j] = v / Ls[j][j];
+  const int tx = tid & 15, ty = tid >> 4;
+  double acc[4][4] = {};
+  for (int p = 0; p < NB; ++p) {
+    double x[4], y[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      x[u] = P[tx + 16 * u][p];
+      y[u] = D[ty + 16 * u][p];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) acc[u][v] = fma(x[u], y[v], acc[u][v]);
   }
-  __syncthreads();
-  for (int idx = tid; idx < NB * NB; idx += NB) {
-    const int i = idx & (NB - 1), c = idx >> 6;
-    if (i0 + i < rows && c < nb) base[(i0 + i) + lda * c] = P[i][c];
-  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int i = i0 + tx + 16 * u, j = ty + 16 * v;
+      if (i < rows && j < nb) base[i + lda * j] = acc[u][v];
+    }
 }
 
 // One step k of the blocked forward substitution B := L^-1 B (right-looking).
@@ -311,18 +377,18 @@ int cholesky_lower(double* A, int n, int* d_info, double* work, cudaStream_t s) 
   cudaFuncSetAttribute(k_panel_inplace, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        static_cast<int>(2 * kTileSmem));
   cudaFuncSetAttribute(k_potrf_diag_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       static_cast<int>(2 * kTileSmem));
+                       static_cast<int>(3 * kTileSmem));
   cudaMemsetAsync(d_info, 0, sizeof(int), s);
   const int nblk = (n + NB - 1) / NB;
   // per block column: diagonal factor + inverse, panel P := P L_kk^-T, A22 -= P P^T
   for (int b = 0; b < nblk; ++b) {
     const int j0 = b * NB, nb = std::min(NB, n - j0);
     double* Db = work + static_cast<size_t>(b) * NB * NB;
-    k_potrf_diag_inv<<<1, NB, 2 * kTileSmem, s>>>(A, n, j0, nb, Db, d_info);
+    k_potrf_diag_inv<<<1, 256, 3 * kTileSmem, s>>>(A, n, j0, nb, Db, d_info);
     ++launches;
     const int rest = n - j0 - nb;
     if (rest > 0) {
-      k_panel_inplace<<<(rest + NB - 1) / NB, NB, 2 * kTileSmem, s>>>(A, n, j0, nb, rest);
+      k_panel_inplace<<<(rest + NB - 1) / NB, 256, 2 * kTileSmem, s>>>(A, n, j0, nb, rest, Db);
       double* P = A + (j0 + nb) + static_cast<long long>(n) * j0;
       double* A22 = A + (j0 + nb) + static_cast<long long>(n) * (j0 + nb);
       launches += 1 + gemm_impl(false, true, rest, rest, nb, -1.0, P, n, P, n, 1.0, A22, n, true,
