@@ -66,6 +66,9 @@ def parse():
     ap.add_argument("--boys", default=None, choices=["reference", "exact"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--precision-report", action="store_true",
+                    help="per-tensor errors and times of the precision form against the FP64 path "
+                         "(and against the committed oracle fixture for the 40-atom workload)")
     ap.add_argument("--profile", action="store_true",
                     help="device steps only (for ncu): no e2e, CPU baseline, FP64 probe or clocks")
     a = ap.parse_args()
@@ -264,10 +267,74 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def precision_report(args):
+    """Raw contraction, df = L^-1 raw and the Coulomb tensor of the FP64 path
+    and of the precision form at several FP32 thresholds; max |difference| and
+    its ratio to the tensor's largest element, plus median device times."""
+    import torch
+
+    from pysisyphus_addons import _native as nat
+
+    torch.cuda.set_device(0)
+    nat.set_boys_mode(args.boys)
+    nat.set_metric_shift(SHIFTED.get(args.config, 0.0))
+    w = workloads(args)[0]
+    orb, aux = nat.Basis(w.shells, "orbital"), nat.Basis(w.shells_aux, "aux")
+    nd, ns, nbf, naux = len(w.densities), w.nstates, w.shells.sph_size, w.shells_aux.sph_size
+    dens = torch.from_numpy(np.ascontiguousarray(w.densities)).cuda()
+    lib, s = nat.load(), torch.cuda.current_stream()
+
+    def run(skip, tensor):
+        nat.set_skip_metric(skip)
+        try:
+            if tensor:
+                out = torch.empty(ns**4, dtype=torch.float64, device="cuda")
+                nat.check(lib.pa_df_4d(orb.handle, aux.handle, nd, nbf, dens.data_ptr(), nat.PA_LAYOUT_C, ns,
+                                       out.data_ptr(), s.cuda_stream))
+            else:
+                out = torch.empty(naux * nd, dtype=torch.float64, device="cuda")
+                nat.check(lib.pa_df_2d(orb.handle, aux.handle, nd, nbf, dens.data_ptr(), nat.PA_LAYOUT_C,
+                                       out.data_ptr(), s.cuda_stream))
+            return out.cpu().numpy(), nat.get_stats()
+        finally:
+            nat.set_skip_metric(0)
+
+    res = {}
+    for prec, thr in (("fp64", 0.0), ("mixed", 1e-8), ("mixed", 1e-6), ("mixed", 1e-4)):
+        nat.set_precision(prec, thr)
+        t = {"raw": run(1, False)[0], "df": run(0, False)[0], "R": run(0, True)[0]}
+        times = [run(0, True)[1] for _ in range(6)][2:]
+        t["ms_total"] = statistics.median(x["ms_total"] for x in times)
+        t["ms_3c"] = statistics.median(x["ms_3c"] for x in times)
+        res[f"{prec}@{thr:g}"] = t
+    nat.set_precision("fp64", 0.0)
+    base = res["fp64@0"]
+    fixture = None
+    if args.config == "cfg2" and args.boys == "reference":
+        fixture = np.load(ROOT / "tests" / "golden" / "oracle_cfg2_reference.npz")
+
+    def err(x, ref):
+        d = float(np.abs(x - ref).max())
+        return {"max_abs": d, "rel_of_max": d / float(np.abs(ref).max())}
+
+    out = {}
+    for k, t in res.items():
+        row = {"ms_total": t["ms_total"], "ms_3c": t["ms_3c"],
+               "vs_fp64_gpu": {n: err(t[n], base[n]) for n in ("raw", "df", "R")}}
+        if fixture is not None:
+            row["vs_fp64_oracle"] = {"raw": err(t["raw"].reshape(fixture["raw"].shape, order="F"), fixture["raw"]),
+                                     "R": err(t["R"].reshape(fixture["R"].shape, order="F"), fixture["R"])}
+        out[k] = row
+    print(json.dumps({"workload": workload_config(args, [w]), "results": out}), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.precision_report:
+        precision_report(args)
         return
     import torch
     import torch.distributed as dist
