@@ -199,6 +199,16 @@ def fp64_peak_tflops(torch):
     return 2 * n**3 / best / 1e12
 
 
+def aggregate_over_ranks(dist, torch, elapsed_s, nints, device):
+    """Whole-job figures of a multi-rank run: the slowest rank's time and the
+    integrals of all ranks (every rank evaluates its own molecule)."""
+    t = torch.tensor([float(elapsed_s)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    n = torch.tensor([float(nints)], dtype=torch.float64, device=device)
+    dist.all_reduce(n, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(n.item())
+
+
 def oracle_sample(args, ws, budget_s=20.0):
     """Time the oracle (C++ OpenMP restatement of the reference driver) on a
     bounded sample of the workload: whole tensors while they fit the budget,
@@ -419,12 +429,7 @@ def main():
     clk = clocks.stop()
     elapsed = t_start.elapsed_time(t_end) / 1e3
     if world > 1:
-        t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
-        n = torch.tensor([float(nints)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(n, op=dist.ReduceOp.SUM)
-        total_ints = float(n.item())
+        elapsed, total_ints = aggregate_over_ranks(dist, torch, elapsed, nints, "cuda")
     else:
         total_ints = float(nints)
     step_s = elapsed / args.steps
@@ -464,9 +469,7 @@ def main():
         torch.cuda.synchronize()
         e2e_s = (time.perf_counter() - t0) / args.steps
         if world > 1:
-            t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
+            e2e_s, _ = aggregate_over_ranks(dist, torch, e2e_s, 0, "cuda")
         keep = [a for w in ws for a in (w.shells.as_arrays(fortran=True) + w.shells_aux.as_arrays(fortran=True))]
         h2d = int(sum(p.numpy().nbytes for p in pinned) + (0 if batched else sum(a.nbytes for a in keep)))
         d2h = int(sum(k**4 * 8 for k in ns))
