@@ -39,32 +39,40 @@ def triple_flops(lab, lc, nd):
     return boys + R + X + G
 
 
-def model(shells: Shells, shells_aux: Shells, q_bra, q_aux, nd, thresh=float(np.float32(1e-10))):
-    """(flops of the 3c contraction, surviving shell triplets, spherical integrals)."""
+def model(shells: Shells, shells_aux: Shells, q_bra, q_aux, nd, thresh=float(np.float32(1e-10)),
+          chunk=20000):
+    """(flops of the 3c contraction, surviving shell triplets, spherical integrals).
+
+    Shell pairs are processed in chunks so that the pair x aux-shell test
+    arrays stay small at large systems."""
     n = len(shells)
     La = np.array([s.L for s in shells])
     Pa = np.array([s.nprims for s in shells])
     Lc = np.array([s.L for s in shells_aux])
     Pc = np.array([s.nprims for s in shells_aux])
     ia, ib = np.tril_indices(n)
-    qb = np.asarray(q_bra)  # packed a(a+1)/2 + b, which is tril order (row-major)
-    lab = La[ia] + La[ib]
-    units = Pa[ia] * Pa[ib]
-    nab = (2 * La[ia] + 1) * (2 * La[ib] + 1)
+    qb_all = np.asarray(q_bra)  # packed a(a+1)/2 + b, which is tril order (row-major)
+    qa = np.asarray(q_aux)
     flops = 0.0
     ntrip = 0
     nints = 0
-    qa = np.asarray(q_aux)
-    for lc in np.unique(Lc):
-        sel = Lc == lc
-        qc = qa[sel]
-        pc = Pc[sel]
-        surv = (qb[:, None] * qc[None, :]) >= thresh
-        per_pair_trip = surv.sum(axis=1)
-        per_pair_prim = (surv * pc[None, :]).sum(axis=1)
-        ntrip += int(per_pair_trip.sum())
-        nints += int((nab * per_pair_trip).sum() * (2 * lc + 1))
-        for l in np.unique(lab):
-            m = lab == l
-            flops += triple_flops(int(l), int(lc), nd) * float((units[m] * per_pair_prim[m]).sum())
+    for p0 in range(0, len(ia), chunk):
+        sl = slice(p0, p0 + chunk)
+        a_, b_ = ia[sl], ib[sl]
+        qb = qb_all[sl]
+        lab = La[a_] + La[b_]
+        units = Pa[a_] * Pa[b_]
+        nab = (2 * La[a_] + 1) * (2 * La[b_] + 1)
+        for lc in np.unique(Lc):
+            sel = Lc == lc
+            qc = qa[sel]
+            pc = Pc[sel]
+            surv = (qb[:, None] * qc[None, :]) >= thresh
+            per_pair_trip = surv.sum(axis=1)
+            per_pair_prim = (surv * pc[None, :]).sum(axis=1)
+            ntrip += int(per_pair_trip.sum())
+            nints += int((nab * per_pair_trip).sum() * (2 * lc + 1))
+            for l in np.unique(lab):
+                m = lab == l
+                flops += triple_flops(int(l), int(lc), nd) * float((units[m] * per_pair_prim[m]).sum())
     return flops, ntrip, nints
