@@ -261,6 +261,10 @@ struct Ctx {
   // same size do not map device memory again; the device's default pool and
   // other allocators in the process are untouched.
   cudaMemPool_t pool = nullptr;
+  // host-buffer path: the density upload runs on its own stream and only the
+  // density folding waits for it (screening and metric do not need it)
+  cudaStream_t scopy = nullptr;
+  cudaEvent_t ev_alloc = nullptr, ev_copied = nullptr;
   // batched form: metric chains of different molecules on their own streams
   cudaStream_t smet[kNs3c] = {};
   cudaEvent_t jmet[kNs3c] = {};
@@ -292,6 +296,9 @@ int current_ctx(Ctx** out, DeviceTables* dt) {
     PA_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
     PA_CUDA(cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, prio_hi));
     PA_CUDA(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
+    PA_CUDA(cudaStreamCreateWithFlags(&c->scopy, cudaStreamNonBlocking));
+    PA_CUDA(cudaEventCreateWithFlags(&c->ev_alloc, cudaEventDisableTiming));
+    PA_CUDA(cudaEventCreateWithFlags(&c->ev_copied, cudaEventDisableTiming));
     for (int i = 0; i < Ctx::kNs3c; ++i) {
       PA_CUDA(cudaStreamCreateWithFlags(&c->s3c[i], cudaStreamNonBlocking));
       PA_CUDA(cudaEventCreateWithFlags(&c->j3c[i], cudaEventDisableTiming));
@@ -619,7 +626,7 @@ int stage_solve(const pa_basis_s* aux, int nd, DfBuffers& b, const Options& o, d
 int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d_dens,
            long long sd, long long si, long long sj, double* d_df, DfBuffers& b,
            const DeviceTables& dt, const Options& o, cudaStream_t s, int* launches,
-           Ctx* ctx, int* launches_3c) {
+           Ctx* ctx, int* launches_3c, cudaEvent_t dens_ready) {
   cudaEvent_t* ph = ctx->ph;
   // metric (P|Q), its Cholesky factor and L^-1 on the second stream: independent
   // of everything until the final L^-1 df
@@ -632,6 +639,7 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
   int st = run_screening(orb, aux, dt, o, b, s, launches);
   if (st != PA_OK) return st;
   PA_CUDA(cudaEventRecord(ph[0], s));
+  if (dens_ready) PA_CUDA(cudaStreamWaitEvent(s, dens_ready, 0));
   stage_bra_prep(orb, aux, nd, d_dens, sd, si, sj, b, o, s, launches);
   PA_CUDA(cudaEventRecord(ph[1], s));
   // three-center contraction: one persistent launch per class, on four streams
@@ -743,7 +751,8 @@ int check_pair(pa_basis orb, pa_basis aux) {
 }
 
 int df_device(pa_basis orb, pa_basis aux, int ndens, int nbf, const double* d_dens, int layout,
-              double* d_df, int nstates, double* d_R, cudaStream_t user_stream) {
+              double* d_df, int nstates, double* d_R, cudaStream_t user_stream,
+              cudaEvent_t dens_ready = nullptr) {
   int st = check_pair(orb, aux);
   if (st != PA_OK) return st;
   if (ndens < 0 || nbf != orb->host.nsph)
@@ -780,7 +789,7 @@ int df_device(pa_basis orb, pa_basis aux, int ndens, int nbf, const double* d_de
   }
   PA_CUDA(cudaEventRecord(c->ev0, s));
   int launches = 0, launches_3c = 0;
-  st = run_df(orb, aux, ndens, d_dens, sd, si, sj, d_df, b, dt, o, s, &launches, c, &launches_3c);
+  st = run_df(orb, aux, ndens, d_dens, sd, si, sj, d_df, b, dt, o, s, &launches, c, &launches_3c, dens_ready);
   if (st != PA_OK) return st;
   g_stats.launches_3c = launches_3c;
   if (d_R) launches += coulomb_4d(d_df, aux->host.nsph, ndens, nstates, gram, d_R, s);
@@ -1116,8 +1125,16 @@ int df_host(pa_basis orb, pa_basis aux, int ndens, int nbf, const double* dens, 
   PA_CUDA(cudaMallocFromPoolAsync(&d_dens, std::max<size_t>(nd_bytes, 8), c->pool, c->stream));
   PA_CUDA(cudaMallocFromPoolAsync(&d_df, sizeof(double) * std::max<size_t>(df_count, 1), c->pool, c->stream));
   if (nstates > 0) PA_CUDA(cudaMallocFromPoolAsync(&d_R, sizeof(double) * out_count, c->pool, c->stream));
-  if (nd_bytes) PA_CUDA(cudaMemcpyAsync(d_dens, dens, nd_bytes, cudaMemcpyHostToDevice, c->stream));
-  st = df_device(orb, aux, ndens, nbf, d_dens, layout, d_df, nstates, d_R, c->stream);
+  cudaEvent_t ready = nullptr;
+  if (nd_bytes) {
+    PA_CUDA(cudaEventRecord(c->ev_alloc, c->stream));
+    PA_CUDA(cudaStreamWaitEvent(c->scopy, c->ev_alloc, 0));
+    PA_CUDA(cudaMemcpyAsync(d_dens, dens, nd_bytes, cudaMemcpyHostToDevice, c->scopy));
+    PA_CUDA(cudaEventRecord(c->ev_copied, c->scopy));
+    ready = c->ev_copied;
+  }
+  st = df_device(orb, aux, ndens, nbf, d_dens, layout, d_df, nstates, d_R, c->stream, ready);
+  if (st != PA_OK && ready) cudaStreamWaitEvent(c->stream, ready, 0);  // the copy ends before the free
   if (st == PA_OK) {
     cudaMemcpyAsync(out, nstates > 0 ? d_R : d_df, sizeof(double) * out_count, cudaMemcpyDeviceToHost,
                     c->stream);
