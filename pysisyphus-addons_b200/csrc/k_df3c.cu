@@ -261,7 +261,7 @@ __device__ __forceinline__ void x_triplet_thread(const Df3cArgs& a, double p, do
 // the lanes. Every lane of the warp calls this with the same Real (the caller
 // makes the precision choice warp-uniform), so the warp barriers pair up.
 template <int LAB, int LC, int TS, class Real>
-__device__ __forceinline__ void x_triplet_team(const Df3cArgs& a, const uchar4* txyz, const short4* tminus,
+__device__ __forceinline__ void x_triplet_team(const Df3cArgs& a, const uchar4* txyz, const int* rdesc,
                                                double* rbuf, int tl, bool active, int np, int po,
                                                int maxprim, double p, double X, double Y, double Z,
                                                double* xrow, int mpad) {
@@ -303,18 +303,11 @@ __device__ __forceinline__ void x_triplet_team(const Df3cArgs& a, const uchar4* 
           if (idx == 0) {
             v = Rn[n];
           } else {
-            const uchar4 e = txyz[idx];
-            const short4 mi = tminus[idx];
-            if (e.x) {
-              v = Xr * src[mi.x];
-              if (e.x > 1) v = fma(static_cast<Real>(e.x - 1), src[tminus[mi.x].x], v);
-            } else if (e.y) {
-              v = Yr * src[mi.y];
-              if (e.y > 1) v = fma(static_cast<Real>(e.y - 1), src[tminus[mi.y].y], v);
-            } else {
-              v = Zr * src[mi.z];
-              if (e.z > 1) v = fma(static_cast<Real>(e.z - 1), src[tminus[mi.z].z], v);
-            }
+            const int dsc = rdesc[idx];
+            const int d = rdesc_d(dsc), c = rdesc_c(dsc);
+            const Real xd = d == 0 ? Xr : (d == 1 ? Yr : Zr);
+            v = xd * src[rdesc_s1(dsc)];
+            if (c) v = fma(static_cast<Real>(c), src[rdesc_s2(dsc)], v);
           }
           dst[idx] = v;
         }
@@ -446,12 +439,11 @@ __device__ __forceinline__ void df3c_item(const Df3cArgs& a, int bx, int by, int
     } else {
       // team index tables (shared memory copies of the decoded multi-indices)
       uchar4* txyz = reinterpret_cast<uchar4*>(Rteam + C::NTRIP * (2 * C::NR + 16));
-      // short4 needs 8-byte alignment: start after an even number of uchar4 entries
-      short4* tminus = reinterpret_cast<short4*>(txyz + round_up(C::NR, 2));
+      int* rdesc = reinterpret_cast<int*>(txyz + C::NR);
       if (u0 == ub) {
         for (int i = tid; i < C::NR; i += kThreads) {
           txyz[i] = *reinterpret_cast<const uchar4*>(it->xyz[i]);
-          tminus[i] = make_short4(it->minus[i][0], it->minus[i][1], it->minus[i][2], 0);
+          rdesc[i] = a.dt.rdesc[i];
         }
         __syncthreads();
       }
@@ -469,10 +461,10 @@ __device__ __forceinline__ void df3c_item(const Df3cArgs& a, int bx, int by, int
       const bool weak = !active || u_Q[ui] * cc.w < a.thr32;
       const bool f32 = __all_sync(0xffffffffu, weak) && __any_sync(0xffffffffu, active);
       if (f32)
-        x_triplet_team<LAB, LC, C::TS, float>(a, txyz, tminus, rbuf, tl, active, np, po, maxprim, up.x, X, Y, Z,
+        x_triplet_team<LAB, LC, C::TS, float>(a, txyz, rdesc, rbuf, tl, active, np, po, maxprim, up.x, X, Y, Z,
                                               xrow, C::MPAD);
       else
-        x_triplet_team<LAB, LC, C::TS, double>(a, txyz, tminus, rbuf, tl, active, np, po, maxprim, up.x, X, Y,
+        x_triplet_team<LAB, LC, C::TS, double>(a, txyz, rdesc, rbuf, tl, active, np, po, maxprim, up.x, X, Y,
                                                Z, xrow, C::MPAD);
     }
     cp_async_commit_wait_all();

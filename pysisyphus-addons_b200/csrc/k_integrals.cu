@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(256) k_schwarz_bra(DevBasis B, const int2* __r
         Rn[tid] = f * boys_n(dt, boys_mode, tid, T);
       }
       __syncthreads();
-      hermite_R(it, L4, Rn, X, Yd, Z, R0, R1, tid, blockDim.x, BlockSync());
+      hermite_R(dt.rdesc, L4, Rn, X, Yd, Z, R0, R1, tid, blockDim.x, BlockSync());
       const double* Ei = U.esph + U.unit_esph[u0 + iu];
       const double* Ek = U.esph + U.unit_esph[u0 + ku];
       // Y = Ei * H, one 8 x 8 tile per warp at a time
@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(32 * kSwWarps) k_schwarz_bra_warp(
         Rn[lane] = f * boys_n(dt, boys_mode, lane, T);
       }
       __syncwarp();
-      hermite_R(it, L4, Rn, X, Yd, Z, R0, R1, lane, 32, WarpSync());
+      hermite_R(dt.rdesc, L4, Rn, X, Yd, Z, R0, R1, lane, 32, WarpSync());
       const double* Ei = U.esph + U.unit_esph[u0 + iu];
       const double* Ek = U.esph + U.unit_esph[u0 + ku];
       for (int idx = lane; idx < nab * NH; idx += 32) {
@@ -322,7 +322,7 @@ __device__ void twoc_block_warp(const DevBasis& X, int P, int Q, const DeviceTab
         s.Rn[lane] = f * boys_n(dt, boys_mode, lane, T);
       }
       __syncwarp();
-      hermite_R(it, L, s.Rn, Xd, Yd, Zd, s.R0, s.R1, lane, 32, WarpSync());
+      hermite_R(dt.rdesc, L, s.Rn, Xd, Yd, Zd, s.R0, s.R1, lane, 32, WarpSync());
       for (int idx = lane; idx < nsP * ncQ; idx += 32) {
         const int m = idx / ncQ, sg = idx - m * ncQ;
         const int row = sph_row(lP, m);

@@ -103,7 +103,7 @@ __device__ void block_3c(const StdArgs& a, int pair, int c, Blk3cScratch s) {
         s.Rn[tid] = f * boys_n(a.dt, a.boys_mode, tid, alpha * RPC2);
       }
       __syncthreads();
-      hermite_R(it, L, s.Rn, X, Y, Z, s.R0, s.R1, tid, nthr, BlockSync());
+      hermite_R(a.dt.rdesc, L, s.Rn, X, Y, Z, s.R0, s.R1, tid, nthr, BlockSync());
       for (int idx = tid; idx < NH * NC; idx += nthr) {
         const int t = idx / NC, m = idx - t * NC;
         const int row = lc * lc + m;

@@ -22,10 +22,9 @@ namespace pa {
 // is called between levels by every participating thread (also by threads
 // with no entries to compute in a level).
 template <class Sync>
-__device__ __forceinline__ void hermite_R(const IndexTables* __restrict__ it, int L,
-                                          const double* Rn, double X, double Y, double Z,
-                                          double* b0, double* b1, int lane, int nlanes,
-                                          Sync sync) {
+__device__ __forceinline__ void hermite_R(const int* __restrict__ rdesc, int L, const double* Rn,
+                                          double X, double Y, double Z, double* b0, double* b1,
+                                          int lane, int nlanes, Sync sync) {
   // Threads with lane >= nlanes (e.g. nlanes == 0 for an inactive team) only
   // take part in the synchronization.
   const bool works = lane < nlanes;
@@ -41,26 +40,11 @@ __device__ __forceinline__ void hermite_R(const IndexTables* __restrict__ it, in
       if (idx == 0) {
         v = Rn[n];
       } else {
-        const uchar4 e = *reinterpret_cast<const uchar4*>(it->xyz[idx]);
-        int d;
-        double Xd;
-        int ed;
-        if (e.x) {
-          d = 0;
-          Xd = X;
-          ed = e.x;
-        } else if (e.y) {
-          d = 1;
-          Xd = Y;
-          ed = e.y;
-        } else {
-          d = 2;
-          Xd = Z;
-          ed = e.z;
-        }
-        const int i1 = it->minus[idx][d];
-        v = Xd * src[i1];
-        if (ed > 1) v = fma(static_cast<double>(ed - 1), src[it->minus[i1][d]], v);
+        const int dsc = __ldg(rdesc + idx);
+        const int d = rdesc_d(dsc), c = rdesc_c(dsc);
+        const double xd = d == 0 ? X : (d == 1 ? Y : Z);
+        v = xd * src[rdesc_s1(dsc)];
+        if (c) v = fma(static_cast<double>(c), src[rdesc_s2(dsc)], v);
       }
       dst[idx] = v;
     }

@@ -55,7 +55,17 @@ struct DeviceTables {
   // sum_idx[i * kNSum + j] = index of the multi-index sum (i) + (j) for
   // components i, j of degree <= 2 * PA_LMAX
   const int16_t* sum_idx;
+  // Hermite recursion descriptor of every component idx > 0 (kNCumMax
+  // entries): s1 | s2 << 10 | d << 20 | c << 22, where d is the first
+  // direction with a nonzero exponent e_d, s1 = idx - 1_d, s2 = idx - 2_d and
+  // c = e_d - 1, so R(idx) = X_d R'(s1) + c R'(s2).
+  const int* rdesc;
 };
+
+__device__ __forceinline__ int rdesc_s1(int dsc) { return dsc & 1023; }
+__device__ __forceinline__ int rdesc_s2(int dsc) { return (dsc >> 10) & 1023; }
+__device__ __forceinline__ int rdesc_d(int dsc) { return (dsc >> 20) & 3; }
+__device__ __forceinline__ int rdesc_c(int dsc) { return dsc >> 22; }
 
 constexpr int kNSum = ncum(2 * PA_LMAX);  // 165
 

@@ -179,6 +179,16 @@ int build_tables(TablesOnDevice* out, std::string* err) {
     for (int j = 0; j < kNSum; ++j)
       sum_idx[static_cast<size_t>(i) * kNSum + j] = static_cast<int16_t>(
           cidx(h_idx.xyz[i][0] + h_idx.xyz[j][0], h_idx.xyz[i][1] + h_idx.xyz[j][1], h_idx.xyz[i][2] + h_idx.xyz[j][2]));
+  // Hermite recursion descriptors
+  std::vector<int> rdesc(kNCumMax, 0);
+  for (int idx = 1; idx < kNCumMax; ++idx) {
+    const int e[3] = {h_idx.xyz[idx][0], h_idx.xyz[idx][1], h_idx.xyz[idx][2]};
+    const int d = e[0] ? 0 : (e[1] ? 1 : 2);
+    const int s1 = h_idx.minus[idx][d];
+    const int c = e[d] - 1;
+    const int s2 = c > 0 ? h_idx.minus[s1][d] : 0;
+    rdesc[idx] = s1 | (s2 << 10) | (d << 20) | (c << 22);
+  }
   if (dense.size() > 1024) {
     *err = "solid-harmonic table exceeds its constant-memory slot";
     return PA_ERR_ARG;
@@ -186,7 +196,7 @@ int build_tables(TablesOnDevice* out, std::string* err) {
   // upload
   const size_t bytes = sizeof(IndexTables) + sizeof(double) * (taylor.size() + ref.size() + val.size()) +
                        sizeof(int) * start.size() + sizeof(int16_t) * col.size() +
-                       sizeof(int16_t) * sum_idx.size() + 7 * 256;
+                       sizeof(int16_t) * sum_idx.size() + sizeof(int) * rdesc.size() + 8 * 256;
   char* base = nullptr;
   cudaError_t e = cudaMalloc(&base, bytes);
   if (e != cudaSuccess) {
@@ -208,6 +218,7 @@ int build_tables(TablesOnDevice* out, std::string* err) {
   dt.sph_col = reinterpret_cast<const int16_t*>(put(col.data(), sizeof(int16_t) * col.size()));
   dt.sph_val = reinterpret_cast<const double*>(put(val.data(), sizeof(double) * val.size()));
   dt.sum_idx = reinterpret_cast<const int16_t*>(put(sum_idx.data(), sizeof(int16_t) * sum_idx.size()));
+  dt.rdesc = reinterpret_cast<const int*>(put(rdesc.data(), sizeof(int) * rdesc.size()));
   e = upload_sph_dense(dense.data(), static_cast<int>(dense.size()), dense_off.data(), rownorm.data(), 0);
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
