@@ -28,15 +28,16 @@ constexpr int NB = 64;
 //  * Cholesky: per sub-block column, one warp factors the 16 x 16 diagonal
 //    sub-block, one thread per row solves the 16-wide panel below it, and all
 //    threads update the trailing lower triangle;
-//  * inverse: elimination on the identity, one step (and one barrier) per
-//    row, the rows of X held in registers.
+//  * inverse: four warps invert the diagonal sub-blocks by forward
+//    substitution (one lane per column), then block rows i = 1..3 follow from
+//    X_ij = -X_ii sum_(j <= k < i) L_ik X_kj.
 constexpr int SB = 16;
 __global__ void __launch_bounds__(256) k_potrf_diag_inv(double* A, long long lda, int j0, int nb,
                                                         double* dinv, int* info) {
   extern __shared__ double dsm[];
   double(*S)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(dsm);                       // the block, then L
   double(*Xs)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(dsm + NB * (NB + 1));      // L^-1
-  double(*Ts)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(dsm + 2 * NB * (NB + 1));  // rows of X in flight
+  double(*Ts)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(dsm + 2 * NB * (NB + 1));  // block-row sums
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   for (int idx = tid; idx < NB * NB; idx += 256) {
     const int r = idx & (NB - 1), c = idx >> 6;
@@ -94,40 +95,40 @@ __global__ void __launch_bounds__(256) k_potrf_diag_inv(double* A, long long lda
     const int r = idx & (NB - 1), c = idx >> 6;
     if (r < nb && c <= r) A[(j0 + r) + lda * (j0 + c)] = S[r][c];
   }
-  // inverse X = L^-1 by elimination on the identity, row k at step k:
-  // X[k][:] /= L_kk, then X[i][:] -= L_ik X[k][:] for i > k. Thread
-  // (r, g) = (tid % 64, tid / 64) keeps row r, columns 4 q + g, in registers.
-  {
-    const int r = tid & (NB - 1), g = tid >> 6;
-    double x[16];
-#pragma unroll
-    for (int q = 0; q < 16; ++q) x[q] = (4 * q + g == r) ? 1.0 : 0.0;
-    for (int k = 0; k < NB; ++k) {
-      if (r == k) {
-        const double inv = 1.0 / S[k][k];
-#pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const int j = 4 * q + g;
-          if (j <= k) {
-            x[q] *= inv;
-            Ts[k & 1][j] = x[q];
-          }
-        }
+  // diagonal sub-blocks of the inverse: warp w < 4 inverts sub-block w by
+  // forward substitution, lane c solving for column c
+  if (warp < NB / SB && lane < SB) {
+    const int o = warp * SB, c = lane;
+    for (int i = 0; i < SB; ++i) {
+      double v = 0.0;
+      if (i >= c) {
+        v = (i == c) ? 1.0 : 0.0;
+        for (int k = c; k < i; ++k) v = fma(-S[o + i][o + k], Xs[o + k][o + c], v);
+        v /= S[o + i][o + i];
       }
-      __syncthreads();
-      if (r > k) {
-        const double lik = S[r][k];
-#pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const int j = 4 * q + g;
-          if (j <= k) x[q] = fma(-lik, Ts[k & 1][j], x[q]);
-        }
-      }
+      Xs[o + i][o + c] = v;
     }
-#pragma unroll
-    for (int q = 0; q < 16; ++q) Xs[r][4 * q + g] = (4 * q + g <= r) ? x[q] : 0.0;
   }
   __syncthreads();
+  // block rows i = 1..3: T_j = sum_(j <= k < i) L_ik X_kj, then X_ij = -X_ii T_j
+  for (int bi = 1; bi < NB / SB; ++bi) {
+    const int ro = bi * SB, ncol = bi * SB;  // columns 0 .. ro - 1
+    for (int e = tid; e < SB * ncol; e += 256) {
+      const int i = e / ncol, c = e % ncol;
+      const int bj = c / SB;
+      double v = 0.0;
+      for (int k = bj * SB; k < ro; ++k) v = fma(S[ro + i][k], Xs[k][c], v);
+      Ts[ro + i][c] = v;
+    }
+    __syncthreads();
+    for (int e = tid; e < SB * ncol; e += 256) {
+      const int i = e / ncol, c = e % ncol;
+      double v = 0.0;
+      for (int k = 0; k <= i; ++k) v = fma(Xs[ro + i][ro + k], Ts[ro + k][c], v);
+      Xs[ro + i][c] = -v;
+    }
+    __syncthreads();
+  }
   for (int idx = tid; idx < NB * NB; idx += 256) {
     const int r = idx & (NB - 1), c = idx >> 6;
     dinv[r + NB * c] = (r < nb && c <= r) ? Xs[r][c] : 0.0;
