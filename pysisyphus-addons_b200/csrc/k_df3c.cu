@@ -377,23 +377,30 @@ __device__ __forceinline__ void df3c_item(const Df3cArgs& a, int bx, int by, int
 #pragma unroll
     for (int n = 0; n < 5; ++n) acc[j][n][0] = acc[j][n][1] = 0.0;
 
+  // unit data of the next step, loaded one step ahead by threads tid < UB
+  double nq = 0.0;
+  double4 npP = make_double4(1.0, 0.0, 0.0, 0.0);
+  if (tid < C::UB && ub + tid < ue) {
+    nq = a.unit_Q[a.unit_slot0 + ub + tid];
+    npP = a.slot_pP[a.unit_slot0 + ub + tid];
+  }
   for (int u0 = ub; u0 < ue && tile_n > 0; u0 += C::UB) {
-    if (a.unit_Q[a.unit_slot0 + u0] * qc_max < thr) break;  // sorted: nothing below survives
     __syncthreads();  // previous step's GEMM is done with Xs / Gs / unit data
-    // units of this step that can meet the tile (a prefix, units are sorted)
-    int nvalid = 0;
-    for (int i = 0; i < C::UB; ++i) {
-      const int s = u0 + i;
-      if (s < ue && a.unit_Q[a.unit_slot0 + s] * qc_max >= thr) nvalid = i + 1;
-    }
+    // units of this step that can meet the tile: a prefix, units are sorted
+    bool valid = false;
     if (tid < C::UB) {
-      const int s = u0 + tid;
-      if (tid < nvalid) {
-        u_pP[tid] = a.slot_pP[a.unit_slot0 + s];
-        u_Q[tid] = a.unit_Q[a.unit_slot0 + s];
-      } else {
-        u_pP[tid] = make_double4(1.0, 0.0, 0.0, 0.0);
-        u_Q[tid] = 0.0;
+      valid = u0 + tid < ue && nq * qc_max >= thr;
+      u_pP[tid] = valid ? npP : make_double4(1.0, 0.0, 0.0, 0.0);
+      u_Q[tid] = valid ? nq : 0.0;
+    }
+    const int nvalid = __syncthreads_count(valid);
+    if (nvalid == 0) break;  // sorted: nothing below survives
+    if (tid < C::UB) {
+      const int s = u0 + C::UB + tid;
+      nq = 0.0;
+      if (s < ue) {
+        nq = a.unit_Q[a.unit_slot0 + s];
+        npP = a.slot_pP[a.unit_slot0 + s];
       }
     }
     // 1. G of the valid units: rows k = ui * NH + t, dw doubles each (16-byte chunks)

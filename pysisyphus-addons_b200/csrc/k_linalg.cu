@@ -7,9 +7,9 @@
 //    the inverted diagonal blocks (replaces dtrtri("L","N"), common/linalg.f90:81,
 //    followed by dtrmm("L","L","N","N"), diabatization/intor.f90:198: the
 //    explicit inverse is never formed);
-//  * a tiled FP64 GEMM C := beta C + alpha op(A) op(B) with optional lower
-//    triangular A, used by all of the above and by the Coulomb-tensor Gram
-//    matrix;
+//  * a tiled FP64 GEMM C := beta C + alpha op(A) op(B) on the FP64 tensor
+//    cores with optional lower triangular A, used by all of the above and by
+//    the Coulomb-tensor Gram matrix;
 //  * the 8-fold-symmetric scatter of the Coulomb tensor
 //    (diabatization/intor.f90:241-269).
 #include <algorithm>
@@ -23,13 +23,15 @@ namespace {
 constexpr int NB = 64;
 
 // Factorize the nb x nb diagonal block at (j0, j0) in place (lower) and write
-// its inverse (lower, zeros above the diagonal, NB x NB) to dinv. Both steps
-// use few barriers:
-//  * Cholesky: per sub-block column, one warp factors the 16 x 16 diagonal
-//    sub-block, one thread per row solves the 16-wide panel below it, and all
-//    threads update the trailing lower triangle;
-//  * inverse: four warps invert the diagonal sub-blocks by forward
-//    substitution (one lane per column), then block rows i = 1..3 follow from
+// its inverse (lower, zeros above the diagonal, NB x NB) to dinv. The serial
+// part is kept short: one square root and one reciprocal per pivot, the
+// columns scaled by the reciprocal (as dpotf2 does), rows held in registers.
+//  * Cholesky, per 16-column sub-block: warp 0 factors the 16 x 16 diagonal
+//    sub-block (lane r holds row r, pivots and L(j, k) move by shuffles); one
+//    thread per row below solves x L11^T = a in registers; all threads update
+//    the trailing lower triangle;
+//  * inverse: four warps invert the diagonal sub-blocks (lane c holds column c
+//    in registers), then block rows i = 1..3 follow from
 //    X_ij = -X_ii sum_(j <= k < i) L_ik X_kj.
 constexpr int SB = 16;
 __global__ void __launch_bounds__(256) k_potrf_diag_inv(double* A, long long lda, int j0, int nb,
@@ -38,6 +40,7 @@ __global__ void __launch_bounds__(256) k_potrf_diag_inv(double* A, long long lda
   double(*S)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(dsm);                       // the block, then L
   double(*Xs)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(dsm + NB * (NB + 1));      // L^-1
   double(*Ts)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(dsm + 2 * NB * (NB + 1));  // block-row sums
+  __shared__ double invd[NB];                                                           // 1 / L(j, j)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   for (int idx = tid; idx < NB * NB; idx += 256) {
     const int r = idx & (NB - 1), c = idx >> 6;
@@ -46,36 +49,53 @@ __global__ void __launch_bounds__(256) k_potrf_diag_inv(double* A, long long lda
   }
   __syncthreads();
   for (int k0 = 0; k0 < NB; k0 += SB) {
-    // 16 x 16 diagonal sub-block, lanes 0..15 own its rows
     if (warp == 0) {
-      const int r = k0 + lane;
-      for (int k = k0; k < k0 + SB; ++k) {
-        double dkk = S[k][k];
+      // lanes 16..31 repeat lanes 0..15 (they only feed the shuffles)
+      const int r = lane & (SB - 1);
+      double v[SB];
+#pragma unroll
+      for (int j = 0; j < SB; ++j) v[j] = (j <= r) ? S[k0 + r][k0 + j] : 0.0;
+#pragma unroll
+      for (int k = 0; k < SB; ++k) {
+        double dkk = __shfl_sync(0xffffffffu, v[k], k);
         if (!(dkk > 0.0)) {
-          if (k < nb && lane == 0) atomicCAS(info, 0, j0 + k + 1);
+          if (lane == 0 && k0 + k < nb) atomicCAS(info, 0, j0 + k0 + k + 1);
           dkk = 1.0;  // keep the factor finite; the error is reported through info
         }
         const double d = sqrt(dkk);
-        __syncwarp();
-        if (lane < SB && r == k) S[k][k] = d;
-        if (lane < SB && r > k) S[r][k] = S[r][k] / d;
-        __syncwarp();
-        if (lane < SB && r > k) {
-          const double lrk = S[r][k];
-          for (int j = k + 1; j <= r; ++j) S[r][j] = fma(-lrk, S[j][k], S[r][j]);
+        const double id = 1.0 / d;
+        if (r == k) v[k] = d;
+        if (r > k) v[k] *= id;  // L(r, k)
+#pragma unroll
+        for (int j = 1; j < SB; ++j) {  // fixed trip count: j > k folds once k is unrolled
+          if (j <= k) continue;
+          const double ljk = __shfl_sync(0xffffffffu, v[k], j);  // L(j, k) from lane j
+          if (r >= j) v[j] = fma(-v[k], ljk, v[j]);
         }
-        __syncwarp();
+        if (lane == k) invd[k0 + k] = id;
+      }
+      if (lane < SB) {
+#pragma unroll
+        for (int j = 0; j < SB; ++j)
+          if (j <= r) S[k0 + r][k0 + j] = v[j];
       }
     }
     __syncthreads();
-    // panel rows below: x L11^T = a by forward substitution, one thread per row
-    const int r = k0 + SB + tid;
-    if (r < NB) {
-      for (int j = k0; j < k0 + SB; ++j) {
-        double v = S[r][j];
-        for (int k = k0; k < j; ++k) v = fma(-S[r][k], S[j][k], v);
-        S[r][j] = v / S[j][j];
+    // panel rows below: x L11^T = a, right-looking in registers, one thread per row
+    const int pr = k0 + SB + tid;
+    if (pr < NB) {
+      double v[SB];
+#pragma unroll
+      for (int j = 0; j < SB; ++j) v[j] = S[pr][k0 + j];
+#pragma unroll
+      for (int j = 0; j < SB; ++j) {
+        v[j] *= invd[k0 + j];
+#pragma unroll
+        for (int jj = 1; jj < SB; ++jj)
+          if (jj > j) v[jj] = fma(-v[j], S[k0 + jj][k0 + j], v[jj]);
       }
+#pragma unroll
+      for (int j = 0; j < SB; ++j) S[pr][k0 + j] = v[j];
     }
     __syncthreads();
     // trailing lower triangle: S[r][c] -= sum_k S[r][k] S[c][k], k in the sub-block
@@ -96,17 +116,21 @@ __global__ void __launch_bounds__(256) k_potrf_diag_inv(double* A, long long lda
     if (r < nb && c <= r) A[(j0 + r) + lda * (j0 + c)] = S[r][c];
   }
   // diagonal sub-blocks of the inverse: warp w < 4 inverts sub-block w by
-  // forward substitution, lane c solving for column c
-  if (warp < NB / SB && lane < SB) {
-    const int o = warp * SB, c = lane;
+  // forward substitution, lane c holding column c
+  if (warp < NB / SB) {
+    const int o = warp * SB, c = lane & (SB - 1);
+    double x[SB];
+#pragma unroll
     for (int i = 0; i < SB; ++i) {
-      double v = 0.0;
-      if (i >= c) {
-        v = (i == c) ? 1.0 : 0.0;
-        for (int k = c; k < i; ++k) v = fma(-S[o + i][o + k], Xs[o + k][o + c], v);
-        v /= S[o + i][o + i];
-      }
-      Xs[o + i][o + c] = v;
+      double v = (i == c) ? 1.0 : 0.0;
+#pragma unroll
+      for (int k = 0; k < SB - 1; ++k)
+        if (k < i) v = fma(-S[o + i][o + k], x[k], v);
+      x[i] = (i >= c) ? v * invd[o + i] : 0.0;
+    }
+    if (lane < SB) {
+#pragma unroll
+      for (int i = 0; i < SB; ++i) Xs[o + i][o + c] = x[i];
     }
   }
   __syncthreads();
@@ -241,8 +265,16 @@ __global__ void __launch_bounds__(256) k_trsm_step(const double* __restrict__ L,
   }
 }
 
+__device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
 // C[m x n] := beta C + alpha op(A) op(B); op(A) is m x k, op(B) is k x n.
-// 64 x 64 tiles, k-steps of 16, 256 threads with 4 x 4 outputs each.
+// 64 x 64 tiles, k-steps of 16 staged in shared memory, products on the FP64
+// tensor cores (mma.sync m8n8k4): warp w owns rows 16 (w % 4) .. + 16 and
+// columns 32 (w / 4) .. + 32 of the tile.
 // lower_c: skip output tiles strictly above the diagonal (and entries above it).
 // lower_a: A (not transposed) is lower triangular; entries above its diagonal
 //          are treated as zero whatever the storage holds.
@@ -257,9 +289,11 @@ __global__ void __launch_bounds__(256) k_gemm(int m, int n, int k, double alpha,
   if (lower_c && bj > bi) return;
   __shared__ double As[TK][TM + 1];
   __shared__ double Bs[TK][TN + 1];
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t4 = lane & 3;
+  const int wm = (warp & 3) * 16, wn = (warp >> 2) * 32;
   const int i0 = bi * TM, j0 = bj * TN;
-  double acc[4][4] = {};
+  double acc[2][4][2] = {};
   // with a lower triangular A, columns k > i0 + TM - 1 contribute nothing
   const int kend = (lower_a && !TA) ? min(k, i0 + TM) : k;
   for (int kk = 0; kk < kend; kk += TK) {
@@ -293,29 +327,31 @@ __global__ void __launch_bounds__(256) k_gemm(int m, int n, int k, double alpha,
     }
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < TK; ++q) {
-      double a[4], b[4];
+    for (int q = 0; q < TK; q += 4) {
+      double a[2], b[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[q][tx + 16 * i];
+      for (int mt = 0; mt < 2; ++mt) a[mt] = As[q + t4][wm + 8 * mt + g];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[q][ty + 16 * j];
+      for (int nt = 0; nt < 4; ++nt) b[nt] = Bs[q + t4][wn + 8 * nt + g];
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        for (int nt = 0; nt < 4; ++nt) dmma_m8n8k4(acc[mt][nt][0], acc[mt][nt][1], a[mt], b[nt]);
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int gi = i0 + tx + 16 * i, gj = j0 + ty + 16 * j;
-      if (gi < m && gj < n && (!lower_c || gi >= gj)) {
-        double* c = C + gi + ldc * gj;
-        *c = (beta == 0.0 ? 0.0 : beta * *c) + alpha * acc[i][j];
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int gi = i0 + wm + 8 * mt + g, gj = j0 + wn + 8 * nt + 2 * t4 + i;
+        if (gi < m && gj < n && (!lower_c || gi >= gj)) {
+          double* c = C + gi + ldc * gj;
+          *c = (beta == 0.0 ? 0.0 : beta * *c) + alpha * acc[mt][nt][i];
+        }
       }
-    }
 }
 
 // R(i,j,k,l) = Gram[pair(i,j)][pair(k,l)], pair(i,j) = max(max+1)/2 + min.
@@ -373,7 +409,8 @@ size_t linalg_workspace_doubles(int n) {
   return static_cast<size_t>(nblk) * NB * NB;
 }
 
-int cholesky_lower(double* A, int n, int* d_info, double* work, cudaStream_t s) {
+int cholesky_lower(double* A, int n, int* d_info, double* work, cudaStream_t s,
+                   const CholLookahead* la) {
   int launches = 0;
   cudaFuncSetAttribute(k_panel_inplace, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        static_cast<int>(2 * kTileSmem));
@@ -381,21 +418,39 @@ int cholesky_lower(double* A, int n, int* d_info, double* work, cudaStream_t s) 
                        static_cast<int>(3 * kTileSmem));
   cudaMemsetAsync(d_info, 0, sizeof(int), s);
   const int nblk = (n + NB - 1) / NB;
-  // per block column: diagonal factor + inverse, panel P := P L_kk^-T, A22 -= P P^T
+  bool rest_pending = false;  // a trailing update of the previous step is queued on la->aux
+  // per block column b: diagonal factor + inverse, panel P := P L_bb^-T, then
+  // A22 -= P P^T, split (with lookahead) into the next block column (main
+  // stream, on the path to the next diagonal block) and the rest (aux stream)
   for (int b = 0; b < nblk; ++b) {
     const int j0 = b * NB, nb = std::min(NB, n - j0);
     double* Db = work + static_cast<size_t>(b) * NB * NB;
     k_potrf_diag_inv<<<1, 256, 3 * kTileSmem, s>>>(A, n, j0, nb, Db, d_info);
     ++launches;
     const int rest = n - j0 - nb;
-    if (rest > 0) {
-      k_panel_inplace<<<(rest + NB - 1) / NB, 256, 2 * kTileSmem, s>>>(A, n, j0, nb, rest, Db);
-      double* P = A + (j0 + nb) + static_cast<long long>(n) * j0;
-      double* A22 = A + (j0 + nb) + static_cast<long long>(n) * (j0 + nb);
-      launches += 1 + gemm_impl(false, true, rest, rest, nb, -1.0, P, n, P, n, 1.0, A22, n, true,
-                                false, s);
+    if (rest <= 0) continue;
+    k_panel_inplace<<<(rest + NB - 1) / NB, 256, 2 * kTileSmem, s>>>(A, n, j0, nb, rest, Db);
+    ++launches;
+    double* P = A + (j0 + nb) + static_cast<long long>(n) * j0;
+    double* A22 = A + (j0 + nb) + static_cast<long long>(n) * (j0 + nb);
+    if (!la) {
+      launches += gemm_impl(false, true, rest, rest, nb, -1.0, P, n, P, n, 1.0, A22, n, true, false, s);
+      continue;
+    }
+    const int nb1 = std::min(NB, rest), rest2 = rest - nb1;
+    cudaEventRecord(la->ev_panel, s);
+    // the previous step's remainder also updated this next block column
+    if (rest_pending) cudaStreamWaitEvent(s, la->ev_rest, 0);
+    launches += gemm_impl(false, true, rest, nb1, nb, -1.0, P, n, P, n, 1.0, A22, n, true, false, s);
+    rest_pending = rest2 > 0;
+    if (rest_pending) {
+      cudaStreamWaitEvent(la->aux, la->ev_panel, 0);
+      launches += gemm_impl(false, true, rest2, rest2, nb, -1.0, P + nb1, n, P + nb1, n, 1.0,
+                            A22 + nb1 + static_cast<long long>(n) * nb1, n, true, false, la->aux);
+      cudaEventRecord(la->ev_rest, la->aux);
     }
   }
+  if (rest_pending) cudaStreamWaitEvent(s, la->ev_rest, 0);
   return launches;
 }
 

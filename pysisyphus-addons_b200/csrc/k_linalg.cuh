@@ -14,10 +14,21 @@ int gemm(bool ta, bool tb, int m, int n, int k, double alpha, const double* A, l
 // Doubles of scratch cholesky_lower needs for an n x n matrix (the inverted
 // 64 x 64 diagonal blocks, kept for trsm_lower_left).
 size_t linalg_workspace_doubles(int n);
+// Second stream of the Cholesky factorization: with it, the trailing update
+// beyond the next block column runs there while the next diagonal block is
+// factorized on the main stream (one step of lookahead). The events order the
+// two streams; all three are owned by the caller.
+struct CholLookahead {
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_panel = nullptr, ev_rest = nullptr;
+};
 // In place: the lower triangle of A (n x n, lda = n) becomes L with A = L L^T
 // (dpotrf); work receives the inverses of L's diagonal blocks. *d_info
 // (device) receives 0 or the 1-based column of the first non-positive pivot.
-int cholesky_lower(double* A, int n, int* d_info, double* work, cudaStream_t s);
+// Without la every launch goes to s; with it the work is complete on s when
+// the last launch enqueued on s completes.
+int cholesky_lower(double* A, int n, int* d_info, double* work, cudaStream_t s,
+                   const CholLookahead* la = nullptr);
 // C := L^-1 B (n x nrhs) for the factor and work of cholesky_lower. B is
 // overwritten (used as scratch).
 int trsm_lower_left(const double* L, int n, const double* dinv, double* B, long long ldb, int nrhs,

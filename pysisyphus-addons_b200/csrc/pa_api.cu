@@ -268,6 +268,10 @@ struct Ctx {
   // batched form: metric chains of different molecules on their own streams
   cudaStream_t smet[kNs3c] = {};
   cudaEvent_t jmet[kNs3c] = {};
+  // lookahead streams of the Cholesky factorization: la2 for the chains on
+  // stream2 and for pa_cholesky_solve, la_met[i] for the chain on smet[i]
+  CholLookahead la2;
+  CholLookahead la_met[kNs3c];
   struct BatchPlan* plan = nullptr;  // the last batch, kept for replay
 };
 
@@ -304,6 +308,12 @@ int current_ctx(Ctx** out, DeviceTables* dt) {
       PA_CUDA(cudaEventCreateWithFlags(&c->j3c[i], cudaEventDisableTiming));
       PA_CUDA(cudaStreamCreateWithPriority(&c->smet[i], cudaStreamNonBlocking, prio_hi));
       PA_CUDA(cudaEventCreateWithFlags(&c->jmet[i], cudaEventDisableTiming));
+    }
+    for (int i = 0; i <= Ctx::kNs3c; ++i) {
+      CholLookahead& la = i < Ctx::kNs3c ? c->la_met[i] : c->la2;
+      PA_CUDA(cudaStreamCreateWithPriority(&la.aux, cudaStreamNonBlocking, prio_hi));
+      PA_CUDA(cudaEventCreateWithFlags(&la.ev_panel, cudaEventDisableTiming));
+      PA_CUDA(cudaEventCreateWithFlags(&la.ev_rest, cudaEventDisableTiming));
     }
     PA_CUDA(cudaEventCreate(&c->m0));
     PA_CUDA(cudaEventCreate(&c->m1));
@@ -522,11 +532,11 @@ int run_screening(const pa_basis_s* orb, const pa_basis_s* aux, const DeviceTabl
 
 // (P|Q) [+ shift], its Cholesky factor and the inverted diagonal blocks.
 void stage_metric(const pa_basis_s* aux, DfBuffers& b, const DeviceTables& dt, const Options& o,
-                  cudaStream_t s2, int* launches) {
+                  cudaStream_t s2, const CholLookahead* la, int* launches) {
   const int naux = aux->host.nsph;
   *launches += launch_metric(aux->dev, dt, o.boys_mode, b.M, s2);
   *launches += add_diagonal(b.M, naux, o.metric_shift, s2);
-  *launches += cholesky_lower(b.M, naux, b.info, b.lawork, s2);
+  *launches += cholesky_lower(b.M, naux, b.info, b.lawork, s2, la);
 }
 
 // Density folding of the sorted bra units, per L_ab class.
@@ -634,7 +644,7 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
   PA_CUDA(cudaEventRecord(ctx->fork, s));
   PA_CUDA(cudaStreamWaitEvent(s2, ctx->fork, 0));
   PA_CUDA(cudaEventRecord(ctx->m0, s2));
-  stage_metric(aux, b, dt, o, s2, launches);
+  stage_metric(aux, b, dt, o, s2, &ctx->la2, launches);
   PA_CUDA(cudaEventRecord(ctx->m1, s2));
   int st = run_screening(orb, aux, dt, o, b, s, launches);
   if (st != PA_OK) return st;
@@ -849,7 +859,7 @@ int record_batch(Ctx* c, BatchPlan& plan, const std::vector<BatchMol>& mols, con
   for (int m = 0; m < nmol; ++m) {
     const BatchMol& M = mols[m];
     DfBuffers& b = plan.bufs[m];
-    stage_metric(M.aux, b, dt, o, c->smet[m % W], launches);
+    stage_metric(M.aux, b, dt, o, c->smet[m % W], &c->la_met[m % W], launches);
     const int st = run_screening(M.orb, M.aux, dt, o, b, c->s3c[m % W], launches);
     if (st != PA_OK) return st;
     stage_bra_prep(M.orb, M.aux, M.nd, M.dens, M.sd, M.si, M.sj, b, o, c->s3c[m % W], launches);
@@ -1227,7 +1237,7 @@ int std_device(pa_basis orb, pa_basis aux, int kind, int nmos, const double* d_m
   PA_CUDA(cudaEventRecord(c->m0, s2));
   launches += launch_metric(aux->dev, dt, o.boys_mode, b.M, s2);
   launches += add_diagonal(b.M, naux, o.metric_shift, s2);
-  launches += cholesky_lower(b.M, naux, b.info, b.lawork, s2);
+  launches += cholesky_lower(b.M, naux, b.info, b.lawork, s2, &c->la2);
   PA_CUDA(cudaEventRecord(c->m1, s2));
   // Schwarz vectors (screener%init, common/screening.f90:101-163)
   UnitArrays U;
@@ -1762,7 +1772,7 @@ int pa_cholesky_solve(int n, double* A, int nrhs, double* B) {
   double* work = cv.take<double>(linalg_workspace_doubles(n));
   double* dC = cv.take<double>(nb);
   PA_CUDA(cudaEventRecord(c->ev0, c->stream));
-  int launches = cholesky_lower(dA, n, info, work, c->stream);
+  int launches = cholesky_lower(dA, n, info, work, c->stream, &c->la2);
   if (nb) launches += trsm_lower_left(dA, n, work, dB, n, nrhs, dC, n, c->stream);
   PA_CUDA(cudaGetLastError());
   PA_CUDA(cudaEventRecord(c->ev1, c->stream));

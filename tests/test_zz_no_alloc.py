@@ -88,3 +88,22 @@ def test_noalloc_cholesky_reports_non_spd():
     # a later good call starts from a cleared status word
     L, Y = _noalloc(torch, np.diag([4.0, 1.0, 2.0, 3.0]), np.ones((4, 1)))
     np.testing.assert_allclose(Y[:, 0], 1.0 / np.sqrt([4.0, 1.0, 2.0, 3.0]), rtol=1e-15)
+
+
+def test_lookahead_factor_is_bitwise_the_plain_order():
+    """pa_cholesky_solve runs the factorization with one step of lookahead: the
+    trailing update of each step is split into the next block column (main
+    stream) and the rest (second stream). pa_cholesky_solve_noalloc keeps one
+    update per step on one stream. Both tile the update into the same 64 x 64
+    blocks with the same k order, so the factors and solutions agree bit for
+    bit."""
+    torch = pytest.importorskip("torch")
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(5)
+    n, nrhs = 900, 9  # 15 block columns: lookahead active for 13 steps
+    A = _spd(rng, n)
+    B = rng.normal(size=(n, nrhs))
+    L, Y = _noalloc(torch, A, B)
+    Lref, Yref = nat.cholesky_solve(A, B)
+    np.testing.assert_array_equal(np.tril(L), np.tril(Lref))
+    np.testing.assert_array_equal(Y, Yref)
