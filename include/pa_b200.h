@@ -50,6 +50,10 @@ extern "C" {
 #define PA_PRECISION_FP64 0  /* FP64 throughout (default)                          */
 #define PA_PRECISION_MIXED 1 /* FP32 recurrences for triplets below a Schwarz bound */
 
+/* Triplet estimates of the density-fitting screening. */
+#define PA_SCREEN_SCHWARZ 0 /* Q_ab Q_c (schwarz_estimate, default)                */
+#define PA_SCREEN_QVL 1     /* qvl_estimate, common/screening.f90:267-299          */
+
 /* Density layouts for the pa_* entry points. */
 #define PA_LAYOUT_FORTRAN 0 /* (ndens, nbf, nbf) column-major: d fastest          */
 #define PA_LAYOUT_C 1       /* (ndens, nbf, nbf) row-major: last index fastest    */
@@ -146,6 +150,17 @@ int pa_set_precision(int mode, double fp32_thresh);
  * sums. */
 int pa_set_items_per_sm(int items);
 int pa_get_precision(void);
+/* Triplet estimate of the density-fitting contraction (process-wide):
+ * PA_SCREEN_SCHWARZ (default) is schwarz_estimate, the reference's active line
+ * (diabatization/intor.f90:138); PA_SCREEN_QVL is qvl_estimate
+ * (common/screening.f90:267-299), the commented-out alternative at :137:
+ * beyond the sum of the extents of the bra distribution and the auxiliary
+ * shell, Q_ab pi sqrt(2) beta_c / ((zeta_a + zeta_b)^(1/4) R^(L_c + 1))
+ * replaces Q_ab Q_c. Applies to the Coulomb-tensor entry points and
+ * pa_count_triplets; the std tensors always use the Schwarz estimate, as the
+ * reference does. */
+int pa_set_screening(int mode);
+int pa_get_screening(void);
 
 /* Statistics of the last density-fitting call on this process. */
 typedef struct {

@@ -31,6 +31,10 @@ const double DF2C_SKIP2 = 1e-10;
 
 int g_boys_mode = 0;
 int g_skip_metric = 0;
+// Triplet estimate of contract_coulomb_densities_2d: 0 = schwarz_estimate (the
+// reference's active line, diabatization/intor.f90:138), 1 = qvl_estimate (its
+// commented-out alternative at :137, common/screening.f90:267-299).
+int g_screening = 0;
 // Optional diagonal shift of (P|Q) before the factorization (0 = the reference).
 double g_metric_shift = 0.0;
 OracleStats g_stats{};
@@ -707,6 +711,84 @@ void trmm_right_lower_trans(const std::vector<double>& L, int n, double* Bm, int
   }
 }
 
+// QVL screener data (t_df_screener%init, common/screening.f90:101-163) and
+// qvl_estimate (:267-299). thresh_ws = 1d-4 at every call site
+// (diabatization/intor.f90:84); the auxiliary extents use prec = 1d-8 and the
+// default min_extent 0.01 (:168-196).
+struct QvlScreener {
+  std::vector<double> cx, cy, cz, ext_bra, den_bra;  // per bra pair a >= b, index a(a+1)/2 + b
+  std::vector<double> ext_aux, beta_aux;             // per auxiliary shell
+};
+
+double auxiliary_extent(const std::vector<double>& exps, double prec, double min_extent) {
+  double ext = 0.0;
+  const double prec_term = -std::log(prec);
+  for (double e : exps) {
+    const double arg = (prec_term + 0.5 * std::log(e)) / e;
+    ext = std::max(ext, arg < 0.0 ? min_extent : std::sqrt(arg));
+  }
+  return ext;
+}
+
+QvlScreener qvl_screener(const OBasis& B, const OBasis& X) {
+  QvlScreener q;
+  const double erfi = oracle_erfinv(1.0 - 1e-4);
+  const int nsh = static_cast<int>(B.shells.size());
+  std::vector<double> effexp(nsh);
+  for (int i = 0; i < nsh; ++i)
+    effexp[i] = *std::min_element(B.shells[i].exps.begin(), B.shells[i].exps.end());
+  const size_t np = static_cast<size_t>(nsh) * (nsh + 1) / 2;
+  q.cx.resize(np);
+  q.cy.resize(np);
+  q.cz.resize(np);
+  q.ext_bra.resize(np);
+  q.den_bra.resize(np);
+  for (int a = 0; a < nsh; ++a)
+    for (int b = 0; b <= a; ++b) {
+      const OShell& sa = B.shells[a];
+      const OShell& sb = B.shells[b];
+      const size_t k = static_cast<size_t>(a) * (a + 1) / 2 + b;
+      double R[3];
+      oracle_contracted_center(static_cast<int>(sa.exps.size()), sa.exps.data(), sa.coefs.data(), sa.A,
+                               static_cast<int>(sb.exps.size()), sb.exps.data(), sb.coefs.data(), sb.A, R);
+      // contracted_extent (:198-232)
+      double ext = 0.0;
+      for (double ax : sa.exps)
+        for (double bx : sb.exps) {
+          const double px = ax + bx;
+          double d2 = 0.0;
+          for (int d = 0; d < 3; ++d) {
+            const double P = (ax * sa.A[d] + bx * sb.A[d]) / px;
+            d2 += (R[d] - P) * (R[d] - P);
+          }
+          ext = std::max(ext, std::sqrt(2.0 / px) * erfi + std::sqrt(d2));
+        }
+      q.cx[k] = R[0];
+      q.cy[k] = R[1];
+      q.cz[k] = R[2];
+      q.ext_bra[k] = ext;
+      q.den_bra[k] = std::pow(effexp[a] + effexp[b], 0.25);
+    }
+  for (const OShell& c : X.shells) {
+    q.ext_aux.push_back(auxiliary_extent(c.exps, 1e-8, 0.01));
+    const double eff = *std::min_element(c.exps.begin(), c.exps.end());
+    q.beta_aux.push_back(std::pow(eff, -(2.0 * c.L + 3.0) / 4.0) * std::sqrt(double_factorial(2 * c.L - 1)));
+  }
+  return q;
+}
+
+double qvl_estimate(const QvlScreener& q, const OBasis& X, const std::vector<double>& sbra,
+                    const std::vector<double>& saux, int a, int b, int c) {
+  const size_t k = static_cast<size_t>(a) * (a + 1) / 2 + b;
+  const OShell& sc = X.shells[c];
+  const double dx = q.cx[k] - sc.A[0], dy = q.cy[k] - sc.A[1], dz = q.cz[k] - sc.A[2];
+  const double R = std::sqrt(dx * dx + dy * dy + dz * dz);
+  if (R <= q.ext_bra[k] + q.ext_aux[c]) return sbra[k] * saux[c];
+  double RL = R;
+  for (int l = 0; l < sc.L; ++l) RL *= R;
+  return sbra[k] * PI * std::sqrt(2.0) * q.beta_aux[c] / (q.den_bra[k] * RL);
+}
+
 // contract_coulomb_densities_2d (diabatization/intor.f90:28-200).
 void df_contract_2d(const OBasis& B, const OBasis& X, int ndens, int nbf, const double* D,
                     double* df) {
@@ -714,9 +796,10 @@ void df_contract_2d(const OBasis& B, const OBasis& X, int ndens, int nbf, const 
   const int naux = X.nsph;
   const int nsh = static_cast<int>(B.shells.size());
   const int nsx = static_cast<int>(X.shells.size());
-  // screener (common/screening.f90:101-163; only the Schwarz part is used)
+  // screener (common/screening.f90:101-163)
   const std::vector<double> sbra = schwarz_bra(B);
   const std::vector<double> saux = schwarz_aux(X);
+  const QvlScreener qvl = g_screening ? qvl_screener(B, X) : QvlScreener{};
   const double t1 = now();
   std::vector<double> metric = metric_2c2e(X);
   const double t2 = now();
@@ -739,7 +822,8 @@ void df_contract_2d(const OBasis& B, const OBasis& X, int ndens, int nbf, const 
         for (int b = 0; b <= a; ++b) {
           const OShell& sb = B.shells[b];
           const int nb = 2 * sb.L + 1;
-          const double est = sbra[static_cast<size_t>(a) * (a + 1) / 2 + b] * saux[c];
+          const double est = g_screening ? qvl_estimate(qvl, X, sbra, saux, a, b, c)
+                                         : sbra[static_cast<size_t>(a) * (a + 1) / 2 + b] * saux[c];
           if (est < SCREEN_THRESH) {
             ++skipped;
             continue;
@@ -954,6 +1038,7 @@ void oracle_set_boys_mode(int mode) { g_boys_mode = mode; }
 int oracle_get_boys_mode(void) { return g_boys_mode; }
 void oracle_set_skip_metric(int skip) { g_skip_metric = skip ? 1 : 0; }
 void oracle_set_metric_shift(double shift) { g_metric_shift = shift; }
+void oracle_set_screening(int mode) { g_screening = mode ? 1 : 0; }
 void oracle_set_threads(int nthreads) {
   if (nthreads > 0) omp_set_num_threads(nthreads);
 }

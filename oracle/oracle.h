@@ -34,6 +34,8 @@ void oracle_set_skip_metric(int skip);
  * reference's behaviour). For auxiliary bases that are linearly dependent to
  * machine precision, where dpotrf fails. */
 void oracle_set_metric_shift(double shift);
+// 0: schwarz_estimate (default), 1: qvl_estimate in the Coulomb contraction.
+void oracle_set_screening(int mode);
 int oracle_get_threads(void);
 /* Optional BLAS/LAPACK (Fortran calling convention) used by inv_chol / dtrmm /
  * dgemm, exactly as the reference calls them; naive loops when unset. */

@@ -85,6 +85,7 @@ def lib():
     L.oracle_set_threads.argtypes = [_i]
     L.oracle_set_skip_metric.argtypes = [_i]
     L.oracle_set_metric_shift.argtypes = [_d]
+    L.oracle_set_screening.argtypes = [_i]
     L.oracle_get_threads.restype = _i
     L.oracle_register_lapack.argtypes = [ctypes.c_void_p] * 4
     L.oracle_last_stats.argtypes = [ctypes.POINTER(OracleStats)]
@@ -132,6 +133,12 @@ def set_skip_metric(skip):
 
 def set_metric_shift(shift):
     lib().oracle_set_metric_shift(float(shift))
+
+
+def set_screening(mode):
+    """'schwarz' (default) or 'qvl': the triplet estimate of the Coulomb
+    contraction (diabatization/intor.f90:137-138)."""
+    lib().oracle_set_screening({"schwarz": 0, "qvl": 1}[mode])
 
 
 def set_threads(n):

@@ -326,6 +326,26 @@ __device__ __forceinline__ void x_triplet_team(const Df3cArgs& a, const uchar4* 
   }
 }
 
+// Screening estimate of triplet (unit slot us, auxiliary slot cs), unit Schwarz
+// value uq, auxiliary center cc.xyz: schwarz_estimate Q_ab Q_c
+// (common/screening.f90:301-313; cc.w = Q_c) or, with QVL screening,
+// qvl_estimate (:267-299): Q_ab Q_c within the sum of the extents, beyond it
+// Q_ab pi sqrt(2) beta_c / ((zeta_a + zeta_b)^(1/4) R^(L_c + 1)).
+template <int LC>
+__device__ __forceinline__ double triplet_estimate(const Df3cArgs& a, int us, int cs, double uq,
+                                                   const double4& cc) {
+  if (!a.qvl) return uq * cc.w;
+  const double4 aq = a.aux_qvl[a.aux_slot0 + cs];   // (Q_c, extent, beta, 0)
+  const double4 pq = a.slot_qvl[a.unit_slot0 + us];  // (contracted center, extent)
+  const double dx = pq.x - cc.x, dy = pq.y - cc.y, dz = pq.z - cc.z;
+  const double R = sqrt(dx * dx + dy * dy + dz * dz);
+  if (R <= pq.w + aq.y) return uq * aq.x;
+  double RL = R;
+#pragma unroll
+  for (int l = 0; l < LC; ++l) RL *= R;
+  return uq * kPi * 1.4142135623730951 * aq.z / (a.slot_den[a.unit_slot0 + us] * RL);
+}
+
 // One work item: aux tile bx (TC shells), bra-unit chunk by, density chunk bz.
 template <int LAB, int LC>
 __device__ __forceinline__ void df3c_item(const Df3cArgs& a, int bx, int by, int bz, double* smem) {
@@ -432,13 +452,14 @@ __device__ __forceinline__ void df3c_item(const Df3cArgs& a, int bx, int by, int
         const int ui = tr / C::TC, ci = tr - ui * C::TC;
         if (ci >= tile_n || ui >= nvalid) continue;
         const double4 cc = c_C[ci];
-        if (u_Q[ui] * cc.w < thr) continue;
+        const double est = triplet_estimate<LC>(a, u0 + ui, c0 + ci, u_Q[ui], cc);
+        if (est < thr) continue;
         const double4 up = u_pP[ui];
         const double p = up.x;
         const double X = up.y - cc.x, Y = up.z - cc.y, Z = up.w - cc.z;
         const int np = c_info[2 * ci], po = c_info[2 * ci + 1];
         double* xrow0 = Xs + (ui * C::NH) * C::MPAD + ci * C::NC;
-        if (u_Q[ui] * cc.w < a.thr32)
+        if (est < a.thr32)
           x_triplet_thread<LAB, LC, C::NR, C::MPAD, C::TPT, float>(a, p, X, Y, Z, np, po, xrow0, part);
         else
           x_triplet_thread<LAB, LC, C::NR, C::MPAD, C::TPT, double>(a, p, X, Y, Z, np, po, xrow0, part);
@@ -459,13 +480,15 @@ __device__ __forceinline__ void df3c_item(const Df3cArgs& a, int bx, int by, int
       const int ui = in_team ? team / C::TC : 0, ci = in_team ? team - ui * C::TC : 0;
       double* rbuf = Rteam + (in_team ? team : 0) * (2 * C::NR + 16);
       const double4 cc = c_C[ci];
-      const bool active = in_team && ci < tile_n && ui < nvalid && (u_Q[ui] * cc.w >= thr);
+      const bool valid = in_team && ci < tile_n && ui < nvalid;
+      const double est = valid ? triplet_estimate<LC>(a, u0 + ui, c0 + ci, u_Q[ui], cc) : 0.0;
+      const bool active = valid && est >= thr;
       const double4 up = u_pP[ui];
       const double X = up.y - cc.x, Y = up.z - cc.y, Z = up.w - cc.z;
       const int np = active ? c_info[2 * ci] : 0, po = c_info[2 * ci + 1];
       double* xrow = Xs + (ui * C::NH) * C::MPAD + ci * C::NC;
       // FP32 recurrences only when every active team of the warp has a weak triplet
-      const bool weak = !active || u_Q[ui] * cc.w < a.thr32;
+      const bool weak = !active || est < a.thr32;
       const bool f32 = __all_sync(0xffffffffu, weak) && __any_sync(0xffffffffu, active);
       if (f32)
         x_triplet_team<LAB, LC, C::TS, float>(a, txyz, rdesc, rbuf, tl, active, np, po, maxprim, up.x, X, Y, Z,

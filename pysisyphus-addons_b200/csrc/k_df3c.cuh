@@ -28,6 +28,13 @@ struct Df3cArgs {
   const double* aux_Q = nullptr;     // [slot]
   int nd = 0;
   double* partial = nullptr;         // [chunk][n_aux * NC][nd]
+  // QVL screening (qvl = 1): aux_Q then holds the sort keys (bounds of the
+  // estimate / Q_ab); per unit slot (contracted center, extent) and
+  // (zeta_a + zeta_b)^(1/4); per auxiliary slot (Q_c, extent, beta, 0)
+  int qvl = 0;
+  const double4* slot_qvl = nullptr;
+  const double* slot_den = nullptr;
+  const double4* aux_qvl = nullptr;
   // persistent scheduling (filled in by launch_df3c_class): work items are
   // (aux tile, bra chunk, density chunk), pulled from *counter (zeroed before
   // the launch)

@@ -427,7 +427,14 @@ __global__ void __launch_bounds__(256) k_bra_prep(DevBasis B, const int2* __rest
     if (ab.x != ab.y) v += a.dens[d * a.sd + j * a.si + i * a.sj];
     Ds[idx] = v;
   }
-  if (threadIdx.x == 0) a.slot_pP[slot] = U.unit_pP[u];
+  if (threadIdx.x == 0) {
+    a.slot_pP[slot] = U.unit_pP[u];
+    if (a.slot_qvl) {
+      const int pr = U.unit_pair[u];
+      a.slot_qvl[slot] = a.pair_qvl[pr];
+      a.slot_den[slot] = a.pair_den[pr];
+    }
+  }
   const double* E = U.esph + U.unit_esph[u];
   // G layout: [z][slot in class][t][dw], density d = z * dw + column, zero padded
   const int dw = a.dw;

@@ -20,6 +20,12 @@ struct BraPrepArgs {
   long long g_base = 0;                   // offset of this class's first slot
   int dw = 8;                             // density chunk width (multiple of 8, <= 40)
   int n_class = 0;                        // slots in this class (stride of z)
+  // QVL screening (null otherwise): per pair (center, extent) and
+  // (zeta_a + zeta_b)^(1/4), copied to the unit's slot
+  const double4* pair_qvl = nullptr;
+  const double* pair_den = nullptr;
+  double4* slot_qvl = nullptr;
+  double* slot_den = nullptr;
 };
 
 size_t schwarz_bra_smem(int lab);

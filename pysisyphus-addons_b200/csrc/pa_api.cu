@@ -12,6 +12,7 @@
 #include <cub/device/device_segmented_radix_sort.cuh>
 
 #include <algorithm>
+#include <limits>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -191,6 +192,91 @@ void build_aux_lists(const HostBasis& b, AuxLists* out) {
   *out = std::move(x);
 }
 
+// erf^-1(y) for 0 <= y < 1 by Newton's method on erf(x) - y
+// (d/dx erf = 2/sqrt(pi) exp(-x^2)), started from x = 1 and clipped to
+// stay positive; converges to full double precision in a few steps.
+double erfinv_newton(double y) {
+  double x = 1.0;
+  for (int it = 0; it < 100; ++it) {
+    const double f = std::erf(x) - y;
+    const double step = f / (2.0 / std::sqrt(kPi) * std::exp(-x * x));
+    double xn = x - step;
+    if (xn <= 0.0) xn = 0.5 * x;
+    if (std::fabs(xn - x) <= 1e-16 * std::fabs(xn)) return xn;
+    x = xn;
+  }
+  return x;
+}
+
+void build_qvl_pairs(const HostBasis& b, const PairLists& P, std::vector<double4>* cen_ext,
+                     std::vector<double>* den, double* den_min) {
+  // thresh_ws = 1d-4 at every call site (diabatization/intor.f90:84,
+  // std/intor.f90:60,201); contracted_extent uses erf^-1(1 - thresh_ws)
+  const double erfi = erfinv_newton(1.0 - 1e-4);
+  const int n = static_cast<int>(b.shells.size());
+  std::vector<double> effexp(n);
+  for (int i = 0; i < n; ++i) {
+    const HostShell& s = b.shells[i];
+    effexp[i] = *std::min_element(b.exps.begin() + s.prim_off, b.exps.begin() + s.prim_off + s.nprim);
+  }
+  cen_ext->resize(P.pair_ab.size());
+  den->resize(P.pair_ab.size());
+  double dmin = std::numeric_limits<double>::infinity();
+  for (size_t q = 0; q < P.pair_ab.size(); ++q) {
+    const HostShell& sa = b.shells[P.pair_ab[q].x];
+    const HostShell& sb = b.shells[P.pair_ab[q].y];
+    // contracted_center (common/screening.f90:235-265): |d_a d_b|-weighted
+    // mean of the primitive product centers
+    double R[3] = {0.0, 0.0, 0.0}, wsum = 0.0;
+    for (int i = 0; i < sa.nprim; ++i)
+      for (int j = 0; j < sb.nprim; ++j) {
+        const double ax = b.exps[sa.prim_off + i], bx = b.exps[sb.prim_off + j];
+        const double w = std::fabs(b.coefs[sa.prim_off + i] * b.coefs[sb.prim_off + j]);
+        const double px = ax + bx;
+        for (int d = 0; d < 3; ++d) R[d] += w * (ax * sa.A[d] + bx * sb.A[d]) / px;
+        wsum += w;
+      }
+    for (int d = 0; d < 3; ++d) R[d] /= wsum;
+    // contracted_extent (:198-232): max over primitive pairs of
+    // sqrt(2 / p) erf^-1(1 - thresh_ws) + |R - P|
+    double ext = 0.0;
+    for (int i = 0; i < sa.nprim; ++i)
+      for (int j = 0; j < sb.nprim; ++j) {
+        const double ax = b.exps[sa.prim_off + i], bx = b.exps[sb.prim_off + j];
+        const double px = ax + bx;
+        double d2 = 0.0;
+        for (int d = 0; d < 3; ++d) {
+          const double Pd = (ax * sa.A[d] + bx * sb.A[d]) / px;
+          d2 += (R[d] - Pd) * (R[d] - Pd);
+        }
+        ext = std::max(ext, std::sqrt(2.0 / px) * erfi + std::sqrt(d2));
+      }
+    (*cen_ext)[q] = make_double4(R[0], R[1], R[2], ext);
+    const double dn = std::pow(effexp[P.pair_ab[q].x] + effexp[P.pair_ab[q].y], 0.25);
+    (*den)[q] = dn;
+    dmin = std::min(dmin, dn);
+  }
+  *den_min = P.pair_ab.empty() ? 1.0 : dmin;
+}
+
+void build_qvl_aux(const HostBasis& b, std::vector<double2>* ext_beta) {
+  ext_beta->resize(b.shells.size());
+  const double prec_term = -std::log(1e-8);  // auxiliary_extent(exps, 1d-8), min_extent 0.01
+  for (size_t i = 0; i < b.shells.size(); ++i) {
+    const HostShell& s = b.shells[i];
+    double ext = 0.0, emin = std::numeric_limits<double>::infinity();
+    for (int k = 0; k < s.nprim; ++k) {
+      const double e = b.exps[s.prim_off + k];
+      const double arg = (prec_term + 0.5 * std::log(e)) / e;
+      ext = std::max(ext, arg < 0.0 ? 0.01 : std::sqrt(arg));
+      emin = std::min(emin, e);
+    }
+    double dfact = 1.0;  // (2L - 1)!!
+    for (int k = 2 * s.L - 1; k > 1; k -= 2) dfact *= k;
+    (*ext_beta)[i] = make_double2(ext, std::pow(emin, -(2.0 * s.L + 3.0) / 4.0) * std::sqrt(dfact));
+  }
+}
+
 cudaError_t Arena::reserve(size_t bytes) {
   if (bytes <= cap) return cudaSuccess;
   if (base) {
@@ -237,6 +323,15 @@ struct pa_basis_s {
   int* d_class_pair = nullptr;   // pairs grouped by Lab
   int* d_aux_shell = nullptr;    // aux shells grouped by L
   int* d_aux_off = nullptr;      // [lc_max + 2]
+  // QVL screener data: per shell (as an auxiliary basis) and per shell pair
+  // (as an orbital basis, built with the pair lists)
+  std::vector<double2> aux_qvl;  // (extent, beta)
+  double2* d_aux_qvl = nullptr;
+  std::vector<double4> pair_qvl;  // (contracted center, extent)
+  std::vector<double> pair_den;   // (zeta_a + zeta_b)^(1/4)
+  double qvl_den_min = 1.0;
+  double4* d_pair_qvl = nullptr;
+  double* d_pair_den = nullptr;
 };
 
 namespace pa {
@@ -354,13 +449,35 @@ __global__ void k_gather_unit_keys(int n, const int* __restrict__ class_unit,
   vals[i] = u;
 }
 
+// Sort keys of the auxiliary shells: Q_c, or with QVL screening (qvl != null)
+// the bound max(Q_c, pi sqrt(2) beta_c / (den_min ext_c^(L_c + 1))) of
+// qvl_estimate / Q_ab: beyond the distance ext_ab + ext_c > ext_c the QVL
+// estimate is below Q_ab times the second term, inside it equals Q_ab Q_c. With
+// these keys the staircase of sorted units and shells stays a valid bound.
 __global__ void k_gather_aux_keys(int n, const int* __restrict__ shells, const double* __restrict__ Qc,
-                                  double* keys, int* vals) {
+                                  const int4* __restrict__ shell_info, const double2* __restrict__ qvl,
+                                  double den_min, double* keys, int* vals) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int s = shells[i];
-  keys[i] = Qc[s];
+  double key = Qc[s];
+  if (qvl) {
+    const double2 eb = qvl[s];
+    double rl = eb.x;
+    for (int l = 0; l < shell_info[s].x; ++l) rl *= eb.x;
+    key = fmax(key, kPi * sqrt(2.0) * eb.y / (den_min * rl));
+  }
+  keys[i] = key;
   vals[i] = s;
+}
+
+// Per auxiliary slot: (Q_c, extent, beta, 0) of the sorted shell (QVL screening).
+__global__ void k_aux_slot_qvl(int n, const int* __restrict__ sorted_aux, const double* __restrict__ Qc,
+                               const double2* __restrict__ qvl, double4* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int s = sorted_aux[i];
+  out[i] = make_double4(Qc[s], qvl[s].x, qvl[s].y, 0.0);
 }
 
 __global__ void k_boys_eval(DeviceTables dt, int mode, int nmax, int n, const double* T, double* out) {
@@ -375,6 +492,10 @@ struct DfBuffers {
   double *Qab, *Qc, *qmax, *esph, *ukeys, *slot_Q, *akeys, *aux_Q, *G, *M, *partial, *lawork,
       *df_raw;
   double4 *unit_pP, *slot_pP;
+  // QVL screening: per unit slot (contracted center, extent of its pair) and
+  // (zeta_a + zeta_b)^(1/4); per auxiliary slot (Q_c, extent, beta, 0)
+  double4 *slot_qvl, *aux_slot_qvl;
+  double* slot_den;
   int *uvals, *sorted_unit, *avals, *sorted_aux, *info;
   int* counters = nullptr;  // one work counter per class run
   void* cub_tmp;
@@ -419,6 +540,9 @@ void layout_df(Carver& c, const pa_basis_s* orb, const pa_basis_s* aux, int nd, 
   b->slot_Q = c.take<double>(P.nunits);
   b->sorted_unit = c.take<int>(P.nunits);
   b->slot_pP = c.take<double4>(P.nunits);
+  b->slot_qvl = c.take<double4>(P.nunits);
+  b->slot_den = c.take<double>(P.nunits);
+  b->aux_slot_qvl = c.take<double4>(nx);
   b->akeys = c.take<double>(nx);
   b->avals = c.take<int>(nx);
   b->aux_Q = c.take<double>(nx);
@@ -499,9 +623,14 @@ int run_screening(const pa_basis_s* orb, const pa_basis_s* aux, const DeviceTabl
   *launches += launch_schwarz_bra(orb->dev, orb->d_pair_ab, orb->d_pair_unit0, orb->d_class_pair, P, U, dt,
                                   o.boys_mode, b.Qab, s);
   *launches += launch_schwarz_aux(aux->dev, dt, o.boys_mode, b.Qc, s);
+  const bool qvl = o.screening == PA_SCREEN_QVL;
   if (nx > 0) {
+    k_gather_aux_keys<<<(nx + 255) / 256, 256, 0, s>>>(nx, aux->d_aux_shell, b.Qc, aux->dev.shell,
+                                                       qvl ? aux->d_aux_qvl : nullptr, orb->qvl_den_min,
+                                                       b.akeys, b.avals);
+    ++*launches;
     size_t bytes = b.cub_bytes;
-    PA_CUDA(cub::DeviceReduce::Max(b.cub_tmp, bytes, b.Qc, b.qmax, nx, s));
+    PA_CUDA(cub::DeviceReduce::Max(b.cub_tmp, bytes, b.akeys, b.qmax, nx, s));  // largest key
     ++*launches;
   }
   if (P.nunits > 0) {
@@ -515,13 +644,15 @@ int run_screening(const pa_basis_s* orb, const pa_basis_s* aux, const DeviceTabl
     *launches += 2;
   }
   if (nx > 0) {
-    k_gather_aux_keys<<<(nx + 255) / 256, 256, 0, s>>>(nx, aux->d_aux_shell, b.Qc, b.akeys, b.avals);
-    ++*launches;
     size_t bytes = b.cub_bytes;
     PA_CUDA(cub::DeviceSegmentedRadixSort::SortPairsDescending(
         b.cub_tmp, bytes, b.akeys, b.aux_Q, b.avals, b.sorted_aux, nx, aux->aux.lc_max + 1,
         aux->d_aux_off, aux->d_aux_off + 1, 0, 64, s));
     *launches += 2;
+    if (qvl) {
+      k_aux_slot_qvl<<<(nx + 255) / 256, 256, 0, s>>>(nx, b.sorted_aux, b.Qc, aux->d_aux_qvl, b.aux_slot_qvl);
+      ++*launches;
+    }
   }
   return PA_OK;
 }
@@ -564,6 +695,12 @@ void stage_bra_prep(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const 
     a.g_base = b.g_off[lab];
     a.dw = b.dw;
     a.n_class = a.slot_end - a.slot0;
+    if (o.screening == PA_SCREEN_QVL) {
+      a.pair_qvl = orb->d_pair_qvl;
+      a.pair_den = orb->d_pair_den;
+      a.slot_qvl = b.slot_qvl;
+      a.slot_den = b.slot_den;
+    }
     *launches += launch_bra_prep(orb->dev, orb->d_pair_ab, U, a, lab, s);
   }
 }
@@ -592,6 +729,12 @@ Df3cArgs class_args(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const 
   a.aux_Q = b.aux_Q;
   a.nd = nd;
   a.partial = r.partial;
+  if (o.screening == PA_SCREEN_QVL) {
+    a.qvl = 1;
+    a.slot_qvl = b.slot_qvl;
+    a.slot_den = b.slot_den;
+    a.aux_qvl = b.aux_slot_qvl;
+  }
   return a;
 }
 
@@ -710,6 +853,10 @@ int ensure_pairs(pa_basis b) {
   if (b->host.lmax > PA_LMAX) return fail(PA_ERR_LMAX, "orbital basis L above the compiled maximum");
   PairLists P;
   build_pair_lists(b->host, &P);
+  std::vector<double4> pair_qvl;
+  std::vector<double> pair_den;
+  double den_min = 1.0;
+  build_qvl_pairs(b->host, P, &pair_qvl, &pair_den, &den_min);
   Carver cnt;
   char* dpair = nullptr;
   for (int pass = 0; pass < 2; ++pass) {
@@ -727,6 +874,8 @@ int ensure_pairs(pa_basis b) {
     b->d_class_unit = cnt.take<int>(P.class_unit.size());
     b->d_class_off = cnt.take<int>(P.class_off.size());
     b->d_class_pair = cnt.take<int>(P.class_pair.size());
+    b->d_pair_qvl = cnt.take<double4>(pair_qvl.size());
+    b->d_pair_den = cnt.take<double>(pair_den.size());
   }
   std::vector<char> stage(cnt.used);
   auto put = [&](const void* dst, const void* src, size_t bytes) {
@@ -740,12 +889,17 @@ int ensure_pairs(pa_basis b) {
   put(b->d_class_unit, P.class_unit.data(), sizeof(int) * P.class_unit.size());
   put(b->d_class_off, P.class_off.data(), sizeof(int) * P.class_off.size());
   put(b->d_class_pair, P.class_pair.data(), sizeof(int) * P.class_pair.size());
+  put(b->d_pair_qvl, pair_qvl.data(), sizeof(double4) * pair_qvl.size());
+  put(b->d_pair_den, pair_den.data(), sizeof(double) * pair_den.size());
   const cudaError_t e = cudaMemcpy(dpair, stage.data(), cnt.used, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     cudaFree(dpair);
     return fail(PA_ERR_CUDA, std::string("pair-list upload: ") + cudaGetErrorString(e));
   }
   b->pairs = std::move(P);
+  b->pair_qvl = std::move(pair_qvl);
+  b->pair_den = std::move(pair_den);
+  b->qvl_den_min = den_min;
   b->dpair = dpair;
   b->pairs_ready = true;
   return PA_OK;
@@ -1401,6 +1555,18 @@ int pa_get_precision(void) {
   return g_opts.precision;
 }
 
+int pa_set_screening(int mode) {
+  if (mode != PA_SCREEN_SCHWARZ && mode != PA_SCREEN_QVL) return fail(PA_ERR_ARG, "unknown screening mode");
+  std::lock_guard<std::mutex> lk(g_opt_mu);
+  g_opts.screening = mode;
+  return PA_OK;
+}
+
+int pa_get_screening(void) {
+  std::lock_guard<std::mutex> lk(g_opt_mu);
+  return g_opts.screening;
+}
+
 int pa_set_items_per_sm(int items) {
   if (items < 0 || items > 1024) return fail(PA_ERR_ARG, "items per SM must be in [0, 1024] (0 = by size)");
   std::lock_guard<std::mutex> lk(g_opt_mu);
@@ -1456,6 +1622,7 @@ int pa_basis_create(int nshells, int ndata, const int* bas_centers, const int* b
     return fail(st, err);
   }
   build_aux_lists(b->host, &b->aux);
+  build_qvl_aux(b->host, &b->aux_qvl);
   const HostBasis& h = b->host;
   const int ns = static_cast<int>(h.shells.size());
   Carver cnt;
@@ -1474,6 +1641,7 @@ int pa_basis_create(int nshells, int ndata, const int* bas_centers, const int* b
     b->dev.prim = cv.take<double2>(h.exps.size());
     b->d_aux_shell = cv.take<int>(b->aux.class_shell.size());
     b->d_aux_off = cv.take<int>(b->aux.class_off.size());
+    b->d_aux_qvl = cv.take<double2>(b->aux_qvl.size());
   }
   std::vector<int4> shell(ns);
   std::vector<double4> center(ns);
@@ -1494,6 +1662,7 @@ int pa_basis_create(int nshells, int ndata, const int* bas_centers, const int* b
   put(b->dev.prim, prim.data(), sizeof(double2) * prim.size());
   put(b->d_aux_shell, b->aux.class_shell.data(), sizeof(int) * b->aux.class_shell.size());
   put(b->d_aux_off, b->aux.class_off.data(), sizeof(int) * b->aux.class_off.size());
+  put(b->d_aux_qvl, b->aux_qvl.data(), sizeof(double2) * b->aux_qvl.size());
   const cudaError_t e = cnt.used ? cudaMemcpy(b->dmem, stage.data(), cnt.used, cudaMemcpyHostToDevice) : cudaSuccess;
   if (e != cudaSuccess) {
     cudaFree(b->dmem);
@@ -1671,7 +1840,44 @@ int pa_count_triplets(pa_basis orbital, pa_basis aux, long long* ntriplets, long
   std::vector<double> qb(orbital->pairs.npairs), qc(aux->host.shells.size());
   st = schwarz_impl(orbital, aux, qb.data(), qc.data());
   if (st != PA_OK) return st;
-  const double thr = options().screen_thresh;
+  const Options o = options();
+  const double thr = o.screen_thresh;
+  if (o.screening == PA_SCREEN_QVL) {
+    // every (pair, shell) with the estimate of the kernels (qvl_estimate)
+    long long ncomp = 0, ni = 0;
+    const HostBasis& X = aux->host;
+    for (int p = 0; p < orbital->pairs.npairs; ++p) {
+      const int2 ab = orbital->pairs.pair_ab[p];
+      const long long nab = static_cast<long long>(2 * orbital->host.shells[ab.x].L + 1) *
+                            (2 * orbital->host.shells[ab.y].L + 1);
+      const double4 pq = orbital->pair_qvl[p];
+      for (size_t c = 0; c < X.shells.size(); ++c) {
+        const HostShell& sc = X.shells[c];
+        const double dx = pq.x - sc.A[0], dy = pq.y - sc.A[1], dz = pq.z - sc.A[2];
+        const double R = std::sqrt(dx * dx + dy * dy + dz * dz);
+        double est;
+        if (R <= pq.w + aux->aux_qvl[c].x) {
+          est = qb[p] * qc[c];
+        } else {
+          double RL = R;
+          for (int l = 0; l < sc.L; ++l) RL *= R;
+          est = qb[p] * kPi * 1.4142135623730951 * aux->aux_qvl[c].y / (orbital->pair_den[p] * RL);
+        }
+        if (est >= thr) {
+          ++ncomp;
+          ni += nab * (2 * sc.L + 1);
+        }
+      }
+    }
+    const long long all = static_cast<long long>(orbital->pairs.npairs) * qc.size();
+    if (ntriplets) *ntriplets = all;
+    if (ncomputed) *ncomputed = ncomp;
+    if (nints) *nints = ni;
+    g_stats.ntriplets = all;
+    g_stats.nskipped = all - ncomp;
+    g_stats.nints = ni;
+    return PA_OK;
+  }
   std::vector<std::pair<double, int>> sc;
   for (size_t i = 0; i < qc.size(); ++i) sc.push_back({qc[i], 2 * aux->host.shells[i].L + 1});
   std::sort(sc.begin(), sc.end(), [](const auto& x, const auto& y) { return x.first > y.first; });

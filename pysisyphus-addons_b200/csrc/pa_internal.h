@@ -68,6 +68,16 @@ struct AuxLists {
 void build_pair_lists(const HostBasis& b, PairLists* out);
 void build_aux_lists(const HostBasis& b, AuxLists* out);
 
+// QVL screener data of t_df_screener%init (common/screening.f90:101-163):
+// per shell pair (order of PairLists::pair_ab) the contracted center and
+// extent (x, y, z, extent) and (zeta_a,min + zeta_b,min)^(1/4); the smallest of
+// the latter in *den_min.
+void build_qvl_pairs(const HostBasis& b, const PairLists& P, std::vector<double4>* cen_ext,
+                     std::vector<double>* den, double* den_min);
+// Per auxiliary shell: (extent, beta) of auxiliary_extent(exps, 1d-8) and
+// beta = zeta_min^(-(2L+3)/4) sqrt((2L-1)!!).
+void build_qvl_aux(const HostBasis& b, std::vector<double2>* ext_beta);
+
 // ---------------------------------------------------------------------------
 // Options and statistics.
 struct Options {
@@ -79,6 +89,7 @@ struct Options {
   int precision = 0;          // 0 = FP64 throughout, 1 = mixed (FP32 recurrences for weak triplets)
   double fp32_thresh = 1e-6;  // Schwarz bound below which the mixed form uses FP32
   int items_per_sm = 0;       // work items per SM and class of the three-center kernel (0 = by size)
+  int screening = 0;          // triplet estimate: 0 = Schwarz (reference), 1 = QVL
 };
 
 struct Stats {

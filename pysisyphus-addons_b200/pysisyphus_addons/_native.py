@@ -27,6 +27,8 @@ PA_BOYS_EXACT = 0
 PA_BOYS_REFERENCE = 1
 PA_PRECISION_FP64 = 0
 PA_PRECISION_MIXED = 1
+PA_SCREEN_SCHWARZ = 0
+PA_SCREEN_QVL = 1
 PA_LAYOUT_FORTRAN = 0
 PA_LAYOUT_C = 1
 PA_LMAX_ORBITAL = 4
@@ -92,6 +94,8 @@ SIGNATURES = {
     "pa_set_precision": [_i, _d],
     "pa_set_items_per_sm": [_i],
     "pa_get_precision": [],
+    "pa_set_screening": [_i],
+    "pa_get_screening": [],
     "pa_get_stats": [ctypes.POINTER(PaStats)],
     "pa_basis_create": [_i, _i, _pi, _pi, _pd, _i, ctypes.POINTER(_vp)],
     "pa_basis_destroy": [_vp],
@@ -187,6 +191,17 @@ def set_items_per_sm(items):
 
 def get_precision():
     return {PA_PRECISION_FP64: "fp64", PA_PRECISION_MIXED: "mixed"}[load().pa_get_precision()]
+
+
+def set_screening(mode="schwarz"):
+    """'schwarz' (default, the reference's schwarz_estimate) or 'qvl'
+    (qvl_estimate, common/screening.f90:267-299) for the Coulomb-tensor path."""
+    code = {"schwarz": PA_SCREEN_SCHWARZ, "qvl": PA_SCREEN_QVL}.get(mode, mode)
+    check(load().pa_set_screening(int(code)))
+
+
+def get_screening():
+    return {PA_SCREEN_SCHWARZ: "schwarz", PA_SCREEN_QVL: "qvl"}[load().pa_get_screening()]
 
 
 def set_metric_shift(shift):

@@ -143,3 +143,67 @@ def test_eri_symmetries():
     pq = oracle.eri_block(sh[2], None, sh[0], None)[:, 0, :, 0]
     qp = oracle.eri_block(sh[0], None, sh[2], None)[:, 0, :, 0]
     np.testing.assert_allclose(pq, qp.T, atol=1e-14)
+
+
+def _qvl_count_numpy(shells, shells_aux, qb, qa, thresh):
+    """Independent numpy restatement of t_df_screener%init
+    (common/screening.f90:101-163) and qvl_estimate (:267-299): the number of
+    triplets a >= b, c whose estimate reaches the threshold."""
+    erfi = oracle.erfinv(1.0 - 1e-4)
+
+    def norm_coeffs(s):
+        e, c, lp = np.asarray(s.exps, float), np.asarray(s.coeffs, float), s.L + 1.5
+        N = (c[:, None] * c[None, :] * (e[:, None] * e[None, :]) ** (lp / 2) / (e[:, None] + e[None, :]) ** lp).sum()
+        return c * np.sqrt(e**lp / (np.pi**1.5 / 2**s.L * N))
+
+    orb = list(shells)
+    coefs = [norm_coeffs(s) for s in orb]
+    cen = np.array([s.center for s in orb], float)
+    count = 0
+    for a in range(len(orb)):
+        for b in range(a + 1):
+            ea, eb = np.asarray(orb[a].exps, float), np.asarray(orb[b].exps, float)
+            px = ea[:, None] + eb[None, :]
+            P = (ea[:, None, None] * cen[a] + eb[None, :, None] * cen[b]) / px[:, :, None]
+            w = np.abs(coefs[a][:, None] * coefs[b][None, :])
+            R = (w[:, :, None] * P).sum(axis=(0, 1)) / w.sum()
+            ext = (np.sqrt(2.0 / px) * erfi + np.linalg.norm(R - P, axis=2)).max()
+            den = (ea.min() + eb.min()) ** 0.25
+            q = qb[a * (a + 1) // 2 + b]
+            for c, sc in enumerate(shells_aux):
+                ec = np.asarray(sc.exps, float)
+                arg = (-np.log(1e-8) + 0.5 * np.log(ec)) / ec
+                ext_c = np.where(arg < 0, 0.01, np.sqrt(np.maximum(arg, 0))).max()
+                beta = ec.min() ** (-(2 * sc.L + 3) / 4) * np.sqrt(float(np.prod(np.arange(2 * sc.L - 1, 0, -2))))
+                dist = np.linalg.norm(R - np.asarray(sc.center, float))
+                est = q * qa[c] if dist <= ext + ext_c else q * np.pi * np.sqrt(2.0) * beta / (den * dist ** (sc.L + 1))
+                count += est >= thresh
+    return count
+
+
+def test_oracle_qvl_screening_cfg1():
+    """qvl_estimate in the oracle's Coulomb contraction (the commented-out line
+    diabatization/intor.f90:137): the computed triplet set matches an
+    independent numpy restatement of the screener, differs from the Schwarz
+    set, and moves the raw contraction by little (the skipped triplets are
+    distant ones)."""
+    from pysisyphus_addons.common.synthetic import config_workload
+
+    w = config_workload("cfg1")
+    oracle.set_skip_metric(1)
+    try:
+        ref = oracle.contract_coulomb_densities_2d(w.shells, w.shells_aux, w.densities)
+        st_s = oracle.last_stats()
+        oracle.set_screening("qvl")
+        got = oracle.contract_coulomb_densities_2d(w.shells, w.shells_aux, w.densities)
+        st_q = oracle.last_stats()
+    finally:
+        oracle.set_screening("schwarz")
+        oracle.set_skip_metric(0)
+    qb = oracle.int_schwarz_bra(w.shells)
+    qa = oracle.int_schwarz_aux(w.shells_aux)
+    n_np = _qvl_count_numpy(w.shells, w.shells_aux, qb, qa, float(np.float32(1e-10)))
+    assert st_q["ntriplets"] - st_q["nskipped"] == n_np
+    assert st_q["nskipped"] != st_s["nskipped"]
+    diff = np.abs(got - ref).max()
+    assert 0.0 < diff < 1e-9 * np.abs(ref).max()
