@@ -52,6 +52,10 @@ SHIFTED = {"cfg5": 1e-7, "cfg4": 1e-7}
 def metric_name(args):
     form = "mixed precision" if args.precision == "mixed" else "FP64 plain"
     path = "batched Coulomb tensors" if args.config == "cfg4" else "Coulomb tensor"
+    if args.config == "cfg4" and args.sequential:
+        path = "Coulomb tensors of the batch, one call per molecule"
+    if args.screening == "qvl":
+        form += ", QVL screening"
     return f"3c2e ints/s ({path}, {form} path)"
 
 
@@ -69,6 +73,12 @@ def parse():
     ap.add_argument("--precision-report", action="store_true",
                     help="per-tensor errors and times of the precision form against the FP64 path "
                          "(and against the committed oracle fixture for the 40-atom workload)")
+    ap.add_argument("--screening", default="schwarz", choices=["schwarz", "qvl"],
+                    help="triplet estimate: schwarz (the reference's) or qvl (qvl_estimate); with qvl the "
+                         "integral count follows the QVL set and the Schwarz-based flops model (roofline) "
+                         "is not reported")
+    ap.add_argument("--sequential", action="store_true",
+                    help="cfg4: one pa_df_4d call per molecule (the reference's way) instead of the batched form")
     ap.add_argument("--profile", action="store_true",
                     help="device steps only (for ncu): no e2e, CPU baseline, FP64 probe or clocks")
     a = ap.parse_args()
@@ -90,7 +100,7 @@ def workload_config(args, ws):
 
     shift = SHIFTED.get(args.config, 0.0)
     base = {"boys_mode": args.boys, "precision": args.precision, "screen_thresh": "float32(1e-10)",
-            "metric_shift": shift}
+            "screening": args.screening, "metric_shift": shift}
     if shift:
         base["metric_shift_reason"] = ("auxiliary metric numerically singular for this workload "
                                        "(smallest eigenvalues ~ -1e-13 with exact Boys)")
@@ -98,6 +108,7 @@ def workload_config(args, ws):
     base["l2"] = (f"inputs larger than L2 (densities {dens_mb:.0f} MB > 126 MB)" if dens_mb > 126 else
                   f"inputs smaller than L2 (densities {dens_mb:.1f} MB): not flushed between steps")
     if args.config == "cfg4":
+        base["form"] = "one call per molecule" if args.sequential else "batched (pa_df_4d_batch, CUDA graph)"
         return dict(base, workload="df_coulomb_tensor_batch_64molecules_5to60atoms_lmax3_lauxmax4_4to16states",
                     nmol=len(ws), natoms_total=int(sum(len(w.mol.atomic_nums) for w in ws)),
                     nbf_total=int(sum(w.shells.sph_size for w in ws)),
@@ -220,6 +231,7 @@ def oracle_sample(args, ws, budget_s=20.0):
 
     oracle.set_boys_mode(args.boys)
     oracle.set_metric_shift(SHIFTED.get(args.config, 0.0))
+    oracle.set_screening(args.screening)
     threads = os.cpu_count() or 1
     oracle.set_threads(threads)
     if args.config in ("cfg1", "cfg2"):
@@ -370,6 +382,7 @@ def main():
     nat.set_boys_mode(args.boys)
     nat.set_metric_shift(SHIFTED.get(args.config, 0.0))
     nat.set_precision(args.precision, 1e-6)
+    nat.set_screening(args.screening)
     ws = workloads(args, rank)
     orbs = [nat.Basis(w.shells, "orbital") for w in ws]
     auxs = [nat.Basis(w.shells_aux, "aux") for w in ws]
@@ -379,7 +392,7 @@ def main():
         nints += n_i
         ntrip_all += t_all
         ntrip += t_c
-        if len(ws) == 1:
+        if len(ws) == 1 and args.screening == "schwarz":
             qb = sch.int_schwarz_bra(w.shells)
             qa = sch.int_schwarz_aux(w.shells_aux)
             f, tm, im = fl.model(w.shells, w.shells_aux, qb, qa, len(w.densities))
@@ -395,15 +408,19 @@ def main():
     outs = [torch.empty(k**4, dtype=torch.float64, device="cuda") for k in ns]
     stream = torch.cuda.current_stream()
     lib = nat.load()
-    batched = args.config == "cfg4"
+    batched = args.config == "cfg4" and not args.sequential
+    step_stats = []  # statistics of every call of the last step
 
     def step():
+        step_stats.clear()
         if batched:
             nat.df_4d_batch(orbs, auxs, dens, ns, outs, use_graph=True, stream=stream.cuda_stream)
+            step_stats.append(nat.get_stats())
             return
-        w, d = ws[0], dens[0]
-        nat.check(lib.pa_df_4d(orbs[0].handle, auxs[0].handle, d.shape[0], d.shape[1], d.data_ptr(),
-                               nat.PA_LAYOUT_C, ns[0], outs[0].data_ptr(), stream.cuda_stream))
+        for o, a, d, k, out in zip(orbs, auxs, dens, ns, outs):
+            nat.check(lib.pa_df_4d(o.handle, a.handle, d.shape[0], d.shape[1], d.data_ptr(),
+                                   nat.PA_LAYOUT_C, k, out.data_ptr(), stream.cuda_stream))
+            step_stats.append(nat.get_stats())
 
     if args.profile:
         for _ in range(args.warmup + args.steps):
@@ -422,11 +439,11 @@ def main():
     t_start.record(stream)
     for _ in range(args.steps):
         step()
-        st = nat.get_stats()
-        ms3c.append(st["ms_3c"])
-        phases.append({k: st[k] for k in ("ms_screen", "ms_bra", "ms_metric", "ms_3c", "ms_solve")})
-        launches += st["kernel_launches"]
-        launches3c += st["launches_3c"]
+        ms3c.append(sum(st["ms_3c"] for st in step_stats))
+        phases.append({k: sum(st[k] for st in step_stats)
+                       for k in ("ms_screen", "ms_bra", "ms_metric", "ms_3c", "ms_solve")})
+        launches += sum(st["kernel_launches"] for st in step_stats)
+        launches3c += sum(st["launches_3c"] for st in step_stats)
     t_end.record(stream)
     torch.cuda.synchronize()
     barrier()
@@ -456,10 +473,13 @@ def main():
                 torch.cuda.synchronize()
                 return host_out[0].numpy()
         else:
-            arr = pinned[0].numpy()
+            arrs = [p.numpy() for p in pinned]
 
             def call():
-                return dia.contract_coulomb_densities_4d(ws[0].shells, ws[0].shells_aux, arr)
+                R = None
+                for w, arr in zip(ws, arrs):
+                    R = dia.contract_coulomb_densities_4d(w.shells, w.shells_aux, arr)
+                return R
         for _ in range(2):
             R = call()
         torch.cuda.synchronize()
@@ -497,7 +517,7 @@ def main():
         "gpu_launches": launches,
         "clocks": clk,
     }
-    if not batched:
+    if len(ws) == 1 and args.screening == "schwarz":
         peak = fp64_peak_tflops(torch)
         ms3 = statistics.mean(ms3c)
         achieved = flops_3c / (ms3 / 1e3) / 1e12
@@ -508,6 +528,7 @@ def main():
             "peak_source": "of measured: FP64 GEMM (torch.matmul float64 8192^3) in this run; "
                            "MEASURED_PEAKS.json has no FP64 figure",
             "flops_per_step_3c": flops_3c, "ms_3c": ms3, "traffic": None}
+    if len(ws) == 1:
         line["phases_ms"] = {k: statistics.mean(p[k] for p in phases) for k in phases[0]}
         line["gpu_launches_3c"] = launches3c
     if e2e:
