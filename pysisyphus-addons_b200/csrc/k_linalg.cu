@@ -354,6 +354,25 @@ __global__ void __launch_bounds__(256) k_gemm(int m, int n, int k, double alpha,
       }
 }
 
+// Gram matrix G[i + nd j] = sum_k df[k + naux i] df[k + naux j] of the fitted
+// densities, one warp per entry: lanes stride over k (contiguous columns),
+// then a fixed-order shuffle reduction. Used for nd <= kGramWarpMax, where the
+// tiled GEMM would run as a single block over the whole k range.
+constexpr int kGramWarpMax = 128;
+__global__ void __launch_bounds__(256) k_gram_warp(const double* __restrict__ df, int naux, int nd,
+                                                   double* G) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= nd * nd) return;
+  const int i = w % nd, j = w / nd;
+  const double* a = df + static_cast<long long>(naux) * i;
+  const double* b = df + static_cast<long long>(naux) * j;
+  double s = 0.0;
+  for (int k = lane; k < naux; k += 32) s = fma(a[k], b[k], s);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) G[i + static_cast<long long>(nd) * j] = s;
+}
+
 // R(i,j,k,l) = Gram[pair(i,j)][pair(k,l)], pair(i,j) = max(max+1)/2 + min.
 __global__ void k_coulomb4d(const double* __restrict__ gram, int ndens, int ns, double* R) {
   const long long total = static_cast<long long>(ns) * ns * ns * ns;
@@ -472,8 +491,15 @@ int add_diagonal(double* A, int n, double shift, cudaStream_t s) {
 
 int coulomb_4d(const double* df, int naux, int ndens, int nstates, double* gram_scratch,
                double* R, cudaStream_t s) {
-  int launches = gemm(true, false, ndens, ndens, naux, 1.0, df, naux, df, naux, 0.0, gram_scratch,
-                      ndens, false, s);
+  int launches = 0;
+  if (ndens <= kGramWarpMax) {
+    const long long threads = 32LL * ndens * ndens;
+    k_gram_warp<<<static_cast<int>((threads + 255) / 256), 256, 0, s>>>(df, naux, ndens, gram_scratch);
+    launches = 1;
+  } else {
+    launches = gemm(true, false, ndens, ndens, naux, 1.0, df, naux, df, naux, 0.0, gram_scratch, ndens,
+                    false, s);
+  }
   const long long total = static_cast<long long>(nstates) * nstates * nstates * nstates;
   const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 4096));
   k_coulomb4d<<<std::max(blocks, 1), 256, 0, s>>>(gram_scratch, ndens, nstates, R);

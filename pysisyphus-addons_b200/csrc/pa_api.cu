@@ -1096,7 +1096,7 @@ int batch_4d(int nmol, const pa_basis* orbs, const pa_basis* auxs, const int* nd
   const Options o = options();
   // signature of the batch: options, then per molecule handles, sizes, pointers
   std::vector<long long> sig{nmol, layout, use_graph ? 1 : 0, o.boys_mode, o.skip_metric, o.precision,
-                             o.items_per_sm};
+                             o.items_per_sm, o.screening};
   for (double v : {o.screen_thresh, o.fp32_thresh, o.metric_shift}) {
     long long bits;
     std::memcpy(&bits, &v, sizeof bits);

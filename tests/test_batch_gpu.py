@@ -54,6 +54,29 @@ def test_batch_matches_single_molecule_path(small_batch, use_graph):
             np.testing.assert_array_equal(o.cpu().numpy(), f)
 
 
+def test_batch_graph_follows_the_screening_mode(small_batch):
+    """The recorded graph is keyed on the options: after a switch to QVL
+    screening the next batch call records anew and equals the single-molecule
+    QVL path. QVL changes the triplet set of every molecule of this batch, so a
+    stale replay of the Schwarz graph would be caught."""
+    import torch
+
+    ws, orbs, auxs, dens = small_batch
+    ns = [w.nstates for w in ws]
+    outs = [torch.full((k**4,), np.nan, dtype=torch.float64, device="cuda") for k in ns]
+    nat.df_4d_batch(orbs, auxs, dens, ns, outs, use_graph=True)
+    schwarz = [o.cpu().numpy().copy() for o in outs]
+    nat.set_screening("qvl")
+    try:
+        nat.df_4d_batch(orbs, auxs, dens, ns, outs, use_graph=True)
+        for w, o, b, a, d, s0 in zip(ws, outs, orbs, auxs, dens, schwarz):
+            ref = single(torch, b, a, d, w.nstates)
+            np.testing.assert_array_equal(o.cpu().numpy(), ref)
+            assert not np.array_equal(ref, s0)
+    finally:
+        nat.set_screening("schwarz")
+
+
 def test_batch_errors(small_batch):
     import torch
 
