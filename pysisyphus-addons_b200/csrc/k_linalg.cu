@@ -200,68 +200,111 @@ __global__ void __launch_bounds__(256) k_panel_inplace(double* A, long long lda,
     }
 }
 
-// One step k of the blocked forward substitution B := L^-1 B (right-looking).
-// Block (it, jt), it = k.., jt over 16-column tiles of B: Xk = Dinv_k B_k
-// (recomputed by every block; B_k is not written in this step); block it = k
-// stores Xk in C, the others update B_it -= L_(it,k) Xk. Thread (r, g) =
-// (tid % 64, tid / 64) owns row r, columns 4 g .. 4 g + 3 of the tile.
+// Super-step of the blocked forward substitution B := L^-1 B (right-looking)
+// over the diagonal blocks k0 .. k0 + ns - 1 (ns <= kTrsmSuper). Block
+// (it, jt), it = k0.., jt over 16-column tiles of B, first solves the
+// super-step's blocks itself, in the order of the one-block-per-launch scheme:
+// for j = 0 .. ns-1, B_(k0+j) -= L_(k0+j, k0+l) X_l for l < j, then
+// X_j = Dinv_(k0+j) B_(k0+j). Every product is sum_p M[r][p] X[p][c] with p
+// ascending and each update one subtraction, so the results are those of one
+// launch per diagonal block, in a quarter of the launches. Blocks with it in
+// the super-step store X_(it-k0) in C; the others update
+// B_it -= L_(it, k0+j) X_j for j = 0 .. ns-1 (B itself is only written by
+// these, and B_(k0..) is read before any block of this launch writes). Thread
+// (r, g) = (tid % 64, tid / 64) owns row r, columns 4 g .. 4 g + 3 of the tile.
 constexpr int kTrsmCols = 16;
-__global__ void __launch_bounds__(256) k_trsm_step(const double* __restrict__ L, long long lda, int n,
-                                                   int k, const double* __restrict__ dinv_k,
-                                                   double* B, long long ldb, int nrhs, double* C,
-                                                   long long ldc) {
-  __shared__ double M[NB][NB + 1];            // Dinv_k, then L_(it,k)   [i][p]
-  __shared__ double Xs[NB][kTrsmCols + 1];    // B_k, then Xk            [p][c]
+constexpr int kTrsmSuper = 4;
+constexpr size_t kTrsmSmem = sizeof(double) * (NB * (NB + 1) + kTrsmSuper * NB * (kTrsmCols + 1));
+__global__ void __launch_bounds__(256) k_trsm_super(const double* __restrict__ L, long long lda, int n,
+                                                    int k0, int ns, const double* __restrict__ dinv,
+                                                    const double* B, long long ldb, int nrhs, double* Bw,
+                                                    double* C, long long ldc) {
+  extern __shared__ double tsm[];
+  double(*M)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(tsm);  // Dinv or an L block   [i][p]
+  double(*Xs)[NB][kTrsmCols + 1] =
+      reinterpret_cast<double(*)[NB][kTrsmCols + 1]>(tsm + NB * (NB + 1));  // X_j     [j][p][c]
   const int tid = threadIdx.x, r = tid & (NB - 1), g = tid >> 6;
-  const int it = k + blockIdx.x, c0 = blockIdx.y * kTrsmCols;
-  const int r0 = k * NB, nbk = min(NB, n - r0);
+  const int it = k0 + blockIdx.x, c0 = blockIdx.y * kTrsmCols;
+  auto load_M = [&](const double* src, long long ld, int rows, int cols) {
+    __syncthreads();  // every thread is done with M
 #pragma unroll
-  for (int idx = tid; idx < NB * NB; idx += 256) {
-    const int i = idx & (NB - 1), p = idx >> 6;
-    M[i][p] = dinv_k[i + NB * p];
-  }
-#pragma unroll
-  for (int idx = tid; idx < NB * kTrsmCols; idx += 256) {
-    const int i = idx & (NB - 1), c = idx >> 6;
-    Xs[i][c] = (i < nbk && c0 + c < nrhs) ? B[(r0 + i) + ldb * (c0 + c)] : 0.0;
-  }
-  __syncthreads();
-  double acc[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll 8
-  for (int p = 0; p < NB; ++p) {
-    const double m = M[r][p];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) acc[c] = fma(m, Xs[p][4 * g + c], acc[c]);
-  }
-  if (it == k) {
+    for (int idx = tid; idx < NB * NB; idx += 256) {
+      const int i = idx & (NB - 1), q = idx >> 6;
+      M[i][q] = (i < rows && q < cols) ? src[i + ld * q] : 0.0;
+    }
+    __syncthreads();
+  };
+  // the super-step's solutions X_0 .. X_(ns-1), kept in shared memory
+  for (int j = 0; j < ns; ++j) {
+    const int rj = (k0 + j) * NB, nbj = min(NB, n - rj);
+    double t[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       const int col = c0 + 4 * g + c;
-      if (r < nbk && col < nrhs) C[(r0 + r) + ldc * col] = acc[c];
+      t[c] = (r < nbj && col < nrhs) ? B[(rj + r) + ldb * col] : 0.0;
+    }
+    for (int l = 0; l < j; ++l) {
+      const int rl = (k0 + l) * NB, nbl = min(NB, n - rl);
+      load_M(L + rj + lda * rl, lda, nbj, nbl);
+      double upd[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 8
+      for (int p = 0; p < NB; ++p) {
+        const double m = M[r][p];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) upd[c] = fma(m, Xs[l][p][4 * g + c], upd[c]);
+      }
+#pragma unroll
+      for (int c = 0; c < 4; ++c) t[c] -= upd[c];
+    }
+    // X_j = Dinv_j t: t goes through shared memory (row r of the tile)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) Xs[j][r][4 * g + c] = (r < nbj) ? t[c] : 0.0;
+    load_M(dinv + static_cast<size_t>(k0 + j) * NB * NB, NB, NB, NB);
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 8
+    for (int p = 0; p < NB; ++p) {
+      const double m = M[r][p];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[c] = fma(m, Xs[j][p][4 * g + c], acc[c]);
+    }
+    __syncthreads();  // every thread has read Xs[j] as B_j
+#pragma unroll
+    for (int c = 0; c < 4; ++c) Xs[j][r][4 * g + c] = acc[c];
+  }
+  if (it < k0 + ns) {
+    __syncthreads();
+    const int j = it - k0, rj = it * NB, nbj = min(NB, n - rj);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int col = c0 + 4 * g + c;
+      if (r < nbj && col < nrhs) C[(rj + r) + ldc * col] = Xs[j][r][4 * g + c];
     }
     return;
   }
   const int ri = it * NB, nbi = min(NB, n - ri);
-  __syncthreads();  // every thread is done with M and Xs
+  double bv[4];
 #pragma unroll
-  for (int c = 0; c < 4; ++c) Xs[r][4 * g + c] = acc[c];
-#pragma unroll
-  for (int idx = tid; idx < NB * NB; idx += 256) {
-    const int i = idx & (NB - 1), p = idx >> 6;
-    M[i][p] = (i < nbi && p < nbk) ? L[(ri + i) + lda * (r0 + p)] : 0.0;
+  for (int c = 0; c < 4; ++c) {
+    const int col = c0 + 4 * g + c;
+    bv[c] = (r < nbi && col < nrhs) ? B[(ri + r) + ldb * col] : 0.0;
   }
-  __syncthreads();
-  double upd[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int j = 0; j < ns; ++j) {
+    const int rj = (k0 + j) * NB, nbj = min(NB, n - rj);
+    load_M(L + ri + lda * rj, lda, nbi, nbj);
+    double upd[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll 8
-  for (int p = 0; p < NB; ++p) {
-    const double m = M[r][p];
+    for (int p = 0; p < NB; ++p) {
+      const double m = M[r][p];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) upd[c] = fma(m, Xs[p][4 * g + c], upd[c]);
+      for (int c = 0; c < 4; ++c) upd[c] = fma(m, Xs[j][p][4 * g + c], upd[c]);
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) bv[c] -= upd[c];
   }
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
     const int col = c0 + 4 * g + c;
-    if (r < nbi && col < nrhs) B[(ri + r) + ldb * col] -= upd[c];
+    if (r < nbi && col < nrhs) Bw[(ri + r) + ldb * col] = bv[c];
   }
 }
 
@@ -476,11 +519,14 @@ int cholesky_lower(double* A, int n, int* d_info, double* work, cudaStream_t s,
 int trsm_lower_left(const double* L, int n, const double* dinv, double* B, long long ldb, int nrhs,
                     double* C, long long ldc, cudaStream_t s) {
   if (n <= 0 || nrhs <= 0) return 0;
+  cudaFuncSetAttribute(k_trsm_super, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kTrsmSmem));
   const int nblk = (n + NB - 1) / NB, ct = (nrhs + kTrsmCols - 1) / kTrsmCols;
-  for (int k = 0; k < nblk; ++k)
-    k_trsm_step<<<dim3(nblk - k, ct), 256, 0, s>>>(L, n, n, k, dinv + static_cast<size_t>(k) * NB * NB, B,
-                                                   ldb, nrhs, C, ldc);
-  return nblk;
+  int launches = 0;
+  for (int k0 = 0; k0 < nblk; k0 += kTrsmSuper, ++launches) {
+    const int ns = std::min(kTrsmSuper, nblk - k0);
+    k_trsm_super<<<dim3(nblk - k0, ct), 256, kTrsmSmem, s>>>(L, n, n, k0, ns, dinv, B, ldb, nrhs, B, C, ldc);
+  }
+  return launches;
 }
 
 int add_diagonal(double* A, int n, double shift, cudaStream_t s) {
