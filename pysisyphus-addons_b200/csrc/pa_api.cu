@@ -571,12 +571,14 @@ void layout_df(Carver& c, const pa_basis_s* orb, const pa_basis_s* aux, int nd, 
   b->runs.clear();
   size_t part_total = 0;
   const AuxLists& X = aux->aux;
-  for (int lab = 0; lab <= P.lab_max && nd > 0; ++lab) {
-    const int nu = P.class_off[lab + 1] - P.class_off[lab];
-    if (nu == 0) continue;
-    for (int lc = 0; lc <= X.lc_max; ++lc) {
-      const int nxc = X.class_off[lc + 1] - X.class_off[lc];
-      if (nxc == 0) continue;
+  // class runs grouped by L_c, highest first (light L_c = 0 classes last, so
+  // the cheapest reduction closes the phase), L_ab ascending within a group
+  for (int lc = X.lc_max; lc >= 0 && nd > 0; --lc) {
+    const int nxc = X.class_off[lc + 1] - X.class_off[lc];
+    if (nxc == 0) continue;
+    for (int lab = 0; lab <= P.lab_max; ++lab) {
+      const int nu = P.class_off[lab + 1] - P.class_off[lab];
+      if (nu == 0) continue;
       Df3cClassInfo ci;
       df3c_class_info(lab, lc, &ci);
       const int bx = (nxc + ci.tc - 1) / ci.tc;
@@ -738,15 +740,16 @@ Df3cArgs class_args(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const 
   return a;
 }
 
-// Ordered sum of the partial slabs into df_raw.
-void stage_reduce(const pa_basis_s* aux, int nd, DfBuffers& b, cudaStream_t s, int* launches) {
+// Ordered sum of the partial slabs of auxiliary class lc into df_raw (the
+// classes in L_ab order, as they appear in b.runs).
+void stage_reduce_lc(const pa_basis_s* aux, int nd, DfBuffers& b, int lc, cudaStream_t s, int* launches) {
   const AuxLists& X = aux->aux;
-  for (int lc = 0; lc <= X.lc_max && nd > 0; ++lc) {
+  {
     Df3cReduceArgs ra;
     ra.X = aux->dev;
     ra.aux_slot0 = X.class_off[lc];
     ra.n_aux = X.class_off[lc + 1] - X.class_off[lc];
-    if (ra.n_aux == 0) continue;
+    if (ra.n_aux == 0 || nd <= 0) return;
     ra.nc = 2 * lc + 1;
     ra.nd = nd;
     ra.naux = aux->host.nsph;
@@ -761,6 +764,11 @@ void stage_reduce(const pa_basis_s* aux, int nd, DfBuffers& b, cudaStream_t s, i
     ra.df = b.df_raw;
     *launches += launch_df3c_reduce(ra, s);
   }
+}
+
+// All auxiliary classes, after every class run is done.
+void stage_reduce(const pa_basis_s* aux, int nd, DfBuffers& b, cudaStream_t s, int* launches) {
+  for (int lc = 0; lc <= aux->aux.lc_max; ++lc) stage_reduce_lc(aux, nd, b, lc, s, launches);
 }
 
 // d_df = L^-1 df_raw (or df_raw itself when the metric is skipped).
@@ -801,18 +809,23 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
     PA_CUDA(cudaMemsetAsync(b.counters, 0, sizeof(int) * b.runs.size(), s));
     PA_CUDA(cudaEventRecord(ctx->fork, s));
     for (int i = 0; i < Ctx::kNs3c; ++i) PA_CUDA(cudaStreamWaitEvent(ctx->s3c[i], ctx->fork, 0));
-    int ri = 0;
-    for (const auto& r : b.runs) {
-      const int run_index = ri++;
+    // the runs come grouped by L_c: once a group is enqueued, the main stream
+    // waits for the class streams and reduces that group while the next
+    // groups run
+    const int nr = static_cast<int>(b.runs.size());
+    for (int ri = 0; ri < nr; ++ri) {
+      const auto& r = b.runs[ri];
       Df3cArgs a = class_args(orb, aux, nd, b, dt, o, r);
-      a.counter = b.counters + run_index;
-      *launches += launch_df3c_class(r.lab, r.lc, a, r.ny, ctx->s3c[run_index % Ctx::kNs3c]);
+      a.counter = b.counters + ri;
+      *launches += launch_df3c_class(r.lab, r.lc, a, r.ny, ctx->s3c[ri % Ctx::kNs3c]);
+      if (ri + 1 == nr || b.runs[ri + 1].lc != r.lc) {
+        for (int i = 0; i < Ctx::kNs3c; ++i) {
+          PA_CUDA(cudaEventRecord(ctx->j3c[i], ctx->s3c[i]));
+          PA_CUDA(cudaStreamWaitEvent(s, ctx->j3c[i], 0));
+        }
+        stage_reduce_lc(aux, nd, b, r.lc, s, launches);
+      }
     }
-    for (int i = 0; i < Ctx::kNs3c; ++i) {
-      PA_CUDA(cudaEventRecord(ctx->j3c[i], ctx->s3c[i]));
-      PA_CUDA(cudaStreamWaitEvent(s, ctx->j3c[i], 0));
-    }
-    stage_reduce(aux, nd, b, s, launches);
   }
   *launches_3c = *launches - before3c;
   PA_CUDA(cudaEventRecord(ph[2], s));
