@@ -327,9 +327,12 @@ struct pa_basis_s {
   // (as an orbital basis, built with the pair lists)
   std::vector<double2> aux_qvl;  // (extent, beta)
   double2* d_aux_qvl = nullptr;
+  // (the pair data only once QVL screening is used with this basis)
+  bool qvl_ready = false;
   std::vector<double4> pair_qvl;  // (contracted center, extent)
   std::vector<double> pair_den;   // (zeta_a + zeta_b)^(1/4)
   double qvl_den_min = 1.0;
+  char* dqvl = nullptr;
   double4* d_pair_qvl = nullptr;
   double* d_pair_den = nullptr;
 };
@@ -866,10 +869,6 @@ int ensure_pairs(pa_basis b) {
   if (b->host.lmax > PA_LMAX) return fail(PA_ERR_LMAX, "orbital basis L above the compiled maximum");
   PairLists P;
   build_pair_lists(b->host, &P);
-  std::vector<double4> pair_qvl;
-  std::vector<double> pair_den;
-  double den_min = 1.0;
-  build_qvl_pairs(b->host, P, &pair_qvl, &pair_den, &den_min);
   Carver cnt;
   char* dpair = nullptr;
   for (int pass = 0; pass < 2; ++pass) {
@@ -887,8 +886,6 @@ int ensure_pairs(pa_basis b) {
     b->d_class_unit = cnt.take<int>(P.class_unit.size());
     b->d_class_off = cnt.take<int>(P.class_off.size());
     b->d_class_pair = cnt.take<int>(P.class_pair.size());
-    b->d_pair_qvl = cnt.take<double4>(pair_qvl.size());
-    b->d_pair_den = cnt.take<double>(pair_den.size());
   }
   std::vector<char> stage(cnt.used);
   auto put = [&](const void* dst, const void* src, size_t bytes) {
@@ -902,19 +899,51 @@ int ensure_pairs(pa_basis b) {
   put(b->d_class_unit, P.class_unit.data(), sizeof(int) * P.class_unit.size());
   put(b->d_class_off, P.class_off.data(), sizeof(int) * P.class_off.size());
   put(b->d_class_pair, P.class_pair.data(), sizeof(int) * P.class_pair.size());
-  put(b->d_pair_qvl, pair_qvl.data(), sizeof(double4) * pair_qvl.size());
-  put(b->d_pair_den, pair_den.data(), sizeof(double) * pair_den.size());
   const cudaError_t e = cudaMemcpy(dpair, stage.data(), cnt.used, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
     cudaFree(dpair);
     return fail(PA_ERR_CUDA, std::string("pair-list upload: ") + cudaGetErrorString(e));
   }
   b->pairs = std::move(P);
+  b->dpair = dpair;
+  b->pairs_ready = true;
+  return PA_OK;
+}
+
+// QVL pair data of an orbital basis (pair lists built), once, on first use of
+// QVL screening with it.
+int ensure_qvl(pa_basis b) {
+  std::lock_guard<std::mutex> lk(b->pair_mu);
+  if (b->qvl_ready) return PA_OK;
+  std::vector<double4> pair_qvl;
+  std::vector<double> pair_den;
+  double den_min = 1.0;
+  build_qvl_pairs(b->host, b->pairs, &pair_qvl, &pair_den, &den_min);
+  Carver cnt;
+  char* d = nullptr;
+  for (int pass = 0; pass < 2; ++pass) {
+    if (pass == 1) {
+      if (cudaMalloc(&d, std::max<size_t>(cnt.used, 256)) != cudaSuccess)
+        return fail(PA_ERR_CUDA, "cudaMalloc(QVL pair data) failed");
+      cnt = Carver();
+      cnt.base = d;
+    }
+    b->d_pair_qvl = cnt.take<double4>(pair_qvl.size());
+    b->d_pair_den = cnt.take<double>(pair_den.size());
+  }
+  cudaError_t e = cudaMemcpy(b->d_pair_qvl, pair_qvl.data(), sizeof(double4) * pair_qvl.size(),
+                             cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(b->d_pair_den, pair_den.data(), sizeof(double) * pair_den.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(d);
+    return fail(PA_ERR_CUDA, std::string("QVL pair data upload: ") + cudaGetErrorString(e));
+  }
   b->pair_qvl = std::move(pair_qvl);
   b->pair_den = std::move(pair_den);
   b->qvl_den_min = den_min;
-  b->dpair = dpair;
-  b->pairs_ready = true;
+  b->dqvl = d;
+  b->qvl_ready = true;
   return PA_OK;
 }
 
@@ -924,7 +953,9 @@ int check_pair(pa_basis orb, pa_basis aux) {
   cudaGetDevice(&dev);
   if (orb->device != dev || aux->device != dev)
     return fail(PA_ERR_ARG, "basis handle belongs to another device");
-  return ensure_pairs(orb);
+  const int st = ensure_pairs(orb);
+  if (st != PA_OK || options().screening != PA_SCREEN_QVL) return st;
+  return ensure_qvl(orb);
 }
 
 int df_device(pa_basis orb, pa_basis aux, int ndens, int nbf, const double* d_dens, int layout,
@@ -1694,6 +1725,7 @@ int pa_basis_destroy(pa_basis basis) {
   if (!basis) return PA_OK;
   if (basis->dmem) cudaFree(basis->dmem);
   if (basis->dpair) cudaFree(basis->dpair);
+  if (basis->dqvl) cudaFree(basis->dqvl);
   delete basis;
   return PA_OK;
 }
