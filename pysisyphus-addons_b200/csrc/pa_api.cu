@@ -348,6 +348,7 @@ struct Ctx {
   cudaEvent_t ph[5] = {};  // phase boundaries on the main stream: screen | bra | 3c | solve
   cudaStream_t stream2 = nullptr;     // metric + Cholesky + inverse, overlapped with the 3c work
   cudaEvent_t fork = nullptr, m0 = nullptr, m1 = nullptr;
+  cudaEvent_t ev_bra[2 * PA_LMAX + 1] = {};  // density folding of each L_ab class done
   // streams of the three-center class launches: the tail of one class overlaps
   // the start of the next
   static constexpr int kNs3c = 4;
@@ -398,6 +399,7 @@ int current_ctx(Ctx** out, DeviceTables* dt) {
     PA_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
     PA_CUDA(cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, prio_hi));
     PA_CUDA(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
+    for (auto& e : c->ev_bra) PA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     PA_CUDA(cudaStreamCreateWithFlags(&c->scopy, cudaStreamNonBlocking));
     PA_CUDA(cudaEventCreateWithFlags(&c->ev_alloc, cudaEventDisableTiming));
     PA_CUDA(cudaEventCreateWithFlags(&c->ev_copied, cudaEventDisableTiming));
@@ -676,16 +678,21 @@ void stage_metric(const pa_basis_s* aux, DfBuffers& b, const DeviceTables& dt, c
 }
 
 // Density folding of the sorted bra units, per L_ab class.
+// With ev_lab, ev_lab[lab] is recorded on s once class lab is folded (also for
+// empty classes), so that three-center launches can wait for their class alone.
 void stage_bra_prep(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d_dens,
                     long long sd, long long si, long long sj, DfBuffers& b, const Options& o,
-                    cudaStream_t s, int* launches) {
+                    cudaStream_t s, int* launches, cudaEvent_t* ev_lab = nullptr) {
   const PairLists& P = orb->pairs;
   UnitArrays U = unit_arrays(orb, b);
   for (int lab = 0; lab <= P.lab_max; ++lab) {
     BraPrepArgs a;
     a.slot0 = P.class_off[lab];
     a.slot_end = P.class_off[lab + 1];
-    if (a.slot_end <= a.slot0 || nd == 0 || aux->host.shells.empty()) continue;
+    if (a.slot_end <= a.slot0 || nd == 0 || aux->host.shells.empty()) {
+      if (ev_lab) cudaEventRecord(ev_lab[lab], s);
+      continue;
+    }
     a.slot_Q = b.slot_Q;
     a.qmax_aux = b.qmax;
     a.thresh = o.screen_thresh;
@@ -707,6 +714,7 @@ void stage_bra_prep(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const 
       a.slot_den = b.slot_den;
     }
     *launches += launch_bra_prep(orb->dev, orb->d_pair_ab, U, a, lab, s);
+    if (ev_lab) cudaEventRecord(ev_lab[lab], s);
   }
 }
 
@@ -804,14 +812,19 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
   if (st != PA_OK) return st;
   PA_CUDA(cudaEventRecord(ph[0], s));
   if (dens_ready) PA_CUDA(cudaStreamWaitEvent(s, dens_ready, 0));
-  stage_bra_prep(orb, aux, nd, d_dens, sd, si, sj, b, o, s, launches);
-  PA_CUDA(cudaEventRecord(ph[1], s));
-  // three-center contraction: one persistent launch per class, on four streams
-  const int before3c = *launches;
-  if (nd > 0 && !b.runs.empty()) {
+  // the class streams start after the screening; each class launch then waits
+  // only for the folding of its own L_ab class
+  const bool run3c = nd > 0 && !b.runs.empty();
+  if (run3c) {
     PA_CUDA(cudaMemsetAsync(b.counters, 0, sizeof(int) * b.runs.size(), s));
     PA_CUDA(cudaEventRecord(ctx->fork, s));
     for (int i = 0; i < Ctx::kNs3c; ++i) PA_CUDA(cudaStreamWaitEvent(ctx->s3c[i], ctx->fork, 0));
+  }
+  stage_bra_prep(orb, aux, nd, d_dens, sd, si, sj, b, o, s, launches, ctx->ev_bra);
+  PA_CUDA(cudaEventRecord(ph[1], s));
+  // three-center contraction: one persistent launch per class, on four streams
+  const int before3c = *launches;
+  if (run3c) {
     // the runs come grouped by L_c: once a group is enqueued, the main stream
     // waits for the class streams and reduces that group while the next
     // groups run
@@ -820,6 +833,7 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
       const auto& r = b.runs[ri];
       Df3cArgs a = class_args(orb, aux, nd, b, dt, o, r);
       a.counter = b.counters + ri;
+      PA_CUDA(cudaStreamWaitEvent(ctx->s3c[ri % Ctx::kNs3c], ctx->ev_bra[r.lab], 0));
       *launches += launch_df3c_class(r.lab, r.lc, a, r.ny, ctx->s3c[ri % Ctx::kNs3c]);
       if (ri + 1 == nr || b.runs[ri + 1].lc != r.lc) {
         for (int i = 0; i < Ctx::kNs3c; ++i) {
