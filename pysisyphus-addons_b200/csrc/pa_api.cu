@@ -347,6 +347,8 @@ struct Ctx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t ph[5] = {};  // phase boundaries on the main stream: screen | bra | 3c | solve
   cudaStream_t stream2 = nullptr;     // metric + Cholesky + inverse, overlapped with the 3c work
+  cudaStream_t sscr = nullptr;        // screening of the single-molecule path (highest priority)
+  cudaEvent_t ev_scr0 = nullptr, ev_scr1 = nullptr;
   cudaEvent_t fork = nullptr, m0 = nullptr, m1 = nullptr;
   cudaEvent_t ev_bra[2 * PA_LMAX + 1] = {};  // density folding of each L_ab class done
   // streams of the three-center class launches: the tail of one class overlaps
@@ -397,7 +399,14 @@ int current_ctx(Ctx** out, DeviceTables* dt) {
     // that a 3c block frees instead of queueing behind the whole 3c grid.
     int prio_lo = 0, prio_hi = 0;
     PA_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
-    PA_CUDA(cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, prio_hi));
+    // The screening is on the critical path and the metric chain has slack:
+    // screening at the highest priority, the metric chain one level below
+    // (still above the three-center kernels at the default level).
+    const int prio_met = prio_hi < prio_lo ? prio_hi + 1 : prio_hi;
+    PA_CUDA(cudaStreamCreateWithPriority(&c->sscr, cudaStreamNonBlocking, prio_hi));
+    PA_CUDA(cudaEventCreateWithFlags(&c->ev_scr0, cudaEventDisableTiming));
+    PA_CUDA(cudaEventCreateWithFlags(&c->ev_scr1, cudaEventDisableTiming));
+    PA_CUDA(cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, prio_met));
     PA_CUDA(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
     for (auto& e : c->ev_bra) PA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     PA_CUDA(cudaStreamCreateWithFlags(&c->scopy, cudaStreamNonBlocking));
@@ -411,7 +420,7 @@ int current_ctx(Ctx** out, DeviceTables* dt) {
     }
     for (int i = 0; i <= Ctx::kNs3c; ++i) {
       CholLookahead& la = i < Ctx::kNs3c ? c->la_met[i] : c->la2;
-      PA_CUDA(cudaStreamCreateWithPriority(&la.aux, cudaStreamNonBlocking, prio_hi));
+      PA_CUDA(cudaStreamCreateWithPriority(&la.aux, cudaStreamNonBlocking, i < Ctx::kNs3c ? prio_hi : prio_met));
       PA_CUDA(cudaEventCreateWithFlags(&la.ev_panel, cudaEventDisableTiming));
       PA_CUDA(cudaEventCreateWithFlags(&la.ev_rest, cudaEventDisableTiming));
     }
@@ -808,8 +817,12 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
   PA_CUDA(cudaEventRecord(ctx->m0, s2));
   stage_metric(aux, b, dt, o, s2, &ctx->la2, launches);
   PA_CUDA(cudaEventRecord(ctx->m1, s2));
-  int st = run_screening(orb, aux, dt, o, b, s, launches);
+  PA_CUDA(cudaEventRecord(ctx->ev_scr0, s));
+  PA_CUDA(cudaStreamWaitEvent(ctx->sscr, ctx->ev_scr0, 0));
+  int st = run_screening(orb, aux, dt, o, b, ctx->sscr, launches);
   if (st != PA_OK) return st;
+  PA_CUDA(cudaEventRecord(ctx->ev_scr1, ctx->sscr));
+  PA_CUDA(cudaStreamWaitEvent(s, ctx->ev_scr1, 0));
   PA_CUDA(cudaEventRecord(ph[0], s));
   if (dens_ready) PA_CUDA(cudaStreamWaitEvent(s, dens_ready, 0));
   // the class streams start after the screening; each class launch then waits
