@@ -35,27 +35,18 @@ __device__ __forceinline__ int cidx_sum(const IndexTables* __restrict__ it, int 
 }
 
 // ---------------------------------------------------------------------------
-// Per bra unit (primitive pair of a shell pair): the Gaussian product center
-// and exponent, and the spherical Hermite expansion
-// E_sph[(ma, mb)][tuv] = c_a c_b exp(-ab/p AB^2) sum S_la,ma S_lb,mb E_x E_y E_z.
-// One warp per unit: most units are low-L with a handful of entries.
-constexpr int kUnitWarps = 4;  // bra units per block, one warp each
-constexpr int kUnitE = (PA_LMAX + 1) * (PA_LMAX + 1) * (2 * PA_LMAX + 1);
-__global__ void __launch_bounds__(32 * kUnitWarps) k_unit_setup(DevBasis B, const int2* __restrict__ pair_ab,
-                                                                UnitArrays U, int nunits, DeviceTables dt) {
-  __shared__ double E_all[kUnitWarps][3][kUnitE];
-  __shared__ double sh_all[kUnitWarps][8];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int u = blockIdx.x * kUnitWarps + warp;
-  if (u >= nunits) return;  // warp-uniform
-  double(*E)[kUnitE] = E_all[warp];
-  double* sh = sh_all[warp];
+__global__ void __launch_bounds__(128) k_unit_setup(DevBasis B, const int2* __restrict__ pair_ab,
+                                                    UnitArrays U, int nunits, DeviceTables dt) {
+  const int u = blockIdx.x;
+  if (u >= nunits) return;
+  __shared__ double E[3][(PA_LMAX + 1) * (PA_LMAX + 1) * (2 * PA_LMAX + 1)];
+  __shared__ double sh[8];
   const int pair = U.unit_pair[u];
   const int2 ab = pair_ab[pair];
   const int4 sa = B.shell[ab.x], sb = B.shell[ab.y];
   const int la = sa.x, lb = sb.x;
   const int2 pr = U.unit_prims[u];
-  if (lane == 0) {
+  if (threadIdx.x == 0) {
     const double4 A = B.center[ab.x], Bc = B.center[ab.y];
     const double2 pa_ = B.prim[pr.x], pb_ = B.prim[pr.y];
     const double p = pa_.x + pb_.x;
@@ -74,15 +65,15 @@ __global__ void __launch_bounds__(32 * kUnitWarps) k_unit_setup(DevBasis B, cons
     sh[7] = Pz - A.z;
     U.unit_pP[u] = make_double4(p, Px, Py, Pz);
   }
-  __syncwarp();
-  if (lane < 3) {
-    const int d = lane;
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    const int d = threadIdx.x;
     const double4 Bc = B.center[ab.y];
     const double Pd = sh[1 + d];
     const double PB = Pd - (d == 0 ? Bc.x : (d == 1 ? Bc.y : Bc.z));
     hermite_E_1d(la, lb, sh[5 + d], PB, 0.5 / sh[0], E[d]);
   }
-  __syncwarp();
+  __syncthreads();
   const IndexTables* it = dt.idx;
   const int nsb = 2 * lb + 1;
   const int nab = (2 * la + 1) * nsb;
@@ -91,7 +82,7 @@ __global__ void __launch_bounds__(32 * kUnitWarps) k_unit_setup(DevBasis B, cons
   const int offa = ncum(la - 1 < 0 ? -1 : la - 1), offb = ncum(lb - 1 < 0 ? -1 : lb - 1);
   const double pref = sh[4];
   double* out = U.esph + U.unit_esph[u];
-  for (int idx = lane; idx < nab * NH; idx += 32) {
+  for (int idx = threadIdx.x; idx < nab * NH; idx += blockDim.x) {
     const int r = idx / NH, t = idx - r * NH;
     const int ma = r / nsb, mb = r - ma * nsb;
     const uchar4 tt = *reinterpret_cast<const uchar4*>(it->xyz[t]);
@@ -477,7 +468,7 @@ __global__ void __launch_bounds__(256) k_bra_prep(DevBasis B, const int2* __rest
 int launch_unit_setup(const DevBasis& B, const int2* pair_ab, UnitArrays U, int nunits,
                       const DeviceTables& dt, cudaStream_t s) {
   if (nunits == 0) return 0;
-  k_unit_setup<<<(nunits + kUnitWarps - 1) / kUnitWarps, 32 * kUnitWarps, 0, s>>>(B, pair_ab, U, nunits, dt);
+  k_unit_setup<<<nunits, 128, 0, s>>>(B, pair_ab, U, nunits, dt);
   return 1;
 }
 
