@@ -91,21 +91,27 @@ class Shells:
         """
         offset = 1 if fortran else 0
         nshells = len(self.shells)
-        bas_centers = np.zeros((nshells, 3), dtype=np.int32)
-        bas_spec = np.zeros((nshells, 5), dtype=np.int32)
+        # rows are collected in Python lists and converted once (per-row numpy
+        # assignment dominates the cost otherwise)
         data = []
         center_ptrs = {}
-        for i, shell in enumerate(self.shells):
-            key = (shell.center_ind, *shell.center.tolist())
-            if key not in center_ptrs:
-                center_ptrs[key] = len(data)
-                data.extend(shell.center.tolist())
-            bas_centers[i] = (shell.center_ind, shell.atomic_num, center_ptrs[key] + offset)
+        cen_rows = []
+        for shell in self.shells:
+            xyz = shell.center.tolist()
+            key = (shell.center_ind, *xyz)
+            ptr = center_ptrs.get(key)
+            if ptr is None:
+                ptr = center_ptrs[key] = len(data)
+                data.extend(xyz)
+            cen_rows.append((shell.center_ind, shell.atomic_num, ptr + offset))
+        spec_rows = []
         for i, shell in enumerate(self.shells):
             ptr = len(data)
             data.extend(shell.coeffs.tolist())
             data.extend(shell.exps.tolist())
-            bas_spec[i] = (i, shell.L, shell.nprims, 1, ptr + offset)
+            spec_rows.append((i, shell.L, len(shell.exps), 1, ptr + offset))
+        bas_centers = np.array(cen_rows, dtype=np.int32).reshape(nshells, 3)
+        bas_spec = np.array(spec_rows, dtype=np.int32).reshape(nshells, 5)
         bas_data = np.array(data, dtype=np.float64)
         return bas_centers, bas_spec, bas_data
 
