@@ -811,16 +811,18 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
   cudaEvent_t* ph = ctx->ph;
   // metric (P|Q), its Cholesky factor and L^-1 on the second stream: independent
   // of everything until the final L^-1 df
+  // (the critical-path screening is enqueued first: the metric chain's ~100
+  // launches would otherwise delay its start by their host-side launch time)
   cudaStream_t s2 = ctx->stream2;
   PA_CUDA(cudaEventRecord(ctx->fork, s));
-  PA_CUDA(cudaStreamWaitEvent(s2, ctx->fork, 0));
-  PA_CUDA(cudaEventRecord(ctx->m0, s2));
-  stage_metric(aux, b, dt, o, s2, &ctx->la2, launches);
-  PA_CUDA(cudaEventRecord(ctx->m1, s2));
   PA_CUDA(cudaEventRecord(ctx->ev_scr0, s));
   PA_CUDA(cudaStreamWaitEvent(ctx->sscr, ctx->ev_scr0, 0));
   int st = run_screening(orb, aux, dt, o, b, ctx->sscr, launches);
   if (st != PA_OK) return st;
+  PA_CUDA(cudaStreamWaitEvent(s2, ctx->fork, 0));
+  PA_CUDA(cudaEventRecord(ctx->m0, s2));
+  stage_metric(aux, b, dt, o, s2, &ctx->la2, launches);
+  PA_CUDA(cudaEventRecord(ctx->m1, s2));
   PA_CUDA(cudaEventRecord(ctx->ev_scr1, ctx->sscr));
   PA_CUDA(cudaStreamWaitEvent(s, ctx->ev_scr1, 0));
   PA_CUDA(cudaEventRecord(ph[0], s));
