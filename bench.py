@@ -482,7 +482,7 @@ def main():
                 for w, arr in zip(ws, arrs):
                     R = dia.contract_coulomb_densities_4d(w.shells, w.shells_aux, arr)
                 return R
-        for _ in range(2):
+        for _ in range(max(3, args.warmup)):  # as many warm-up calls as the device loop
             R = call()
         torch.cuda.synchronize()
         barrier()
