@@ -210,7 +210,10 @@ __global__ void __launch_bounds__(256) k_schwarz_bra(DevBasis B, const int2* __r
 // Schwarz values of low-L pairs (Lab <= kSwLab), one warp per pair: the same
 // arithmetic as k_schwarz_bra with warp barriers instead of block barriers
 // (most pairs of a basis are low-L, and for them the block version mostly
-// waits at its barriers).
+// waits at its barriers). Launches per group of L_ab classes, each warp's
+// scratch sized for the group's largest class (sw_nr R entries, sw_nab x sw_nh
+// Y, sw_nab^2 out, stride sw_stride doubles), so low-L classes keep many more
+// warps resident.
 constexpr int kSwLab = 4;
 constexpr int kSwNR = ncum(2 * kSwLab);
 constexpr int kSwNH = ncum(kSwLab);
@@ -221,8 +224,8 @@ constexpr int kSwWarps = 4;
 __global__ void __launch_bounds__(32 * kSwWarps) k_schwarz_bra_warp(
     DevBasis B, const int2* __restrict__ pair_ab, const int* __restrict__ pair_unit0,
     const int* __restrict__ pair_list, UnitArrays U, int npairs, DeviceTables dt, int boys_mode,
-    double* __restrict__ Qab) {
-  extern __shared__ double sw_smem[];  // [kSwWarps][kSwScratch]
+    double* __restrict__ Qab, int sw_nr, int sw_nab, int sw_nh, int sw_stride) {
+  extern __shared__ double sw_smem[];  // [kSwWarps][sw_stride]
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i = blockIdx.x * kSwWarps + warp;
   if (i >= npairs) return;  // warp-uniform
@@ -233,11 +236,11 @@ __global__ void __launch_bounds__(32 * kSwWarps) k_schwarz_bra_warp(
   const int nab = (2 * la + 1) * (2 * lb + 1);
   const int NH = ncum(la + lb);
   const int L4 = 2 * (la + lb);
-  double* Rn = sw_smem + warp * kSwScratch;
+  double* Rn = sw_smem + warp * sw_stride;
   double* R0 = Rn + 32;
-  double* R1 = R0 + kSwNR;
-  double* Y = R1 + kSwNR;          // [nab][NH]
-  double* out = Y + kSwNab * kSwNH;  // [nab][nab]
+  double* R1 = R0 + sw_nr;
+  double* Y = R1 + sw_nr;            // [nab][NH]
+  double* out = Y + sw_nab * sw_nh;  // [nab][nab]
   const IndexTables* it = dt.idx;
   for (int k = lane; k < nab * nab; k += 32) out[k] = 0.0;
   const int u0 = pair_unit0[pair];
@@ -494,11 +497,26 @@ int launch_schwarz_bra(const DevBasis& B, const int2* pair_ab, const int* pair_u
   const int split = std::min(kSwLab, P.lab_max) + 1;  // classes [0, split) by warps
   const int nlow = P.pair_class_off[split];
   if (nlow > 0) {
-    const size_t wsm = sizeof(double) * kSwWarps * kSwScratch;
-    cudaFuncSetAttribute(k_schwarz_bra_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(wsm));
-    k_schwarz_bra_warp<<<(nlow + kSwWarps - 1) / kSwWarps, 32 * kSwWarps, wsm, s>>>(
-        B, pair_ab, pair_unit0, class_pair, U, nlow, dt, boys_mode, Qab);
-    ++launches;
+    cudaFuncSetAttribute(k_schwarz_bra_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(sizeof(double) * kSwWarps * kSwScratch));
+    // classes L_ab 0..2 together (their scratch is small either way), then
+    // 3 and 4 on their own
+    for (int g = 0; g < split;) {
+      const int lab = g < 2 ? std::min(2, split - 1) : g;  // largest class of the group
+      const int off = P.pair_class_off[g], n = P.pair_class_off[lab + 1] - off;
+      g = lab + 1;
+      if (n <= 0) continue;
+      int nab = 1;  // largest (2la+1)(2lb+1) with la + lb <= lab
+      for (int l = 0; l <= lab; ++l)
+        for (int la = std::max(0, l - PA_LMAX); la <= std::min(l, PA_LMAX); ++la)
+          nab = std::max(nab, (2 * la + 1) * (2 * (l - la) + 1));
+      const int nr = ncum(2 * lab), nh = ncum(lab);
+      const int stride = 32 + 2 * nr + nab * nh + nab * nab;
+      const size_t wsm = sizeof(double) * kSwWarps * stride;
+      k_schwarz_bra_warp<<<(n + kSwWarps - 1) / kSwWarps, 32 * kSwWarps, wsm, s>>>(
+          B, pair_ab, pair_unit0, class_pair + off, U, n, dt, boys_mode, Qab, nr, nab, nh, stride);
+      ++launches;
+    }
   }
   // one launch per higher class, each with its own shared-memory footprint
   cudaFuncSetAttribute(k_schwarz_bra, cudaFuncAttributeMaxDynamicSharedMemorySize,
