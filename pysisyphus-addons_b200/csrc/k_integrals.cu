@@ -105,10 +105,14 @@ __global__ void __launch_bounds__(128) k_unit_setup(DevBasis B, const int2* __re
 // ---------------------------------------------------------------------------
 // Schwarz values of high-L pairs, one block per pair. For every pair of bra
 // units (iu, ku) the block is
-//   (ab|ab)[r][s] = sum_(t,t') E_iu[r][t] (-1)^|t'| R[t + t'] E_ku[s][t'],
+//   M_ik[r][s] = sum_(t,t') E_iu[r][t] (-1)^|t'| R[t + t'] E_ku[s][t'],
 // two small GEMMs run on the FP64 tensor cores (DMMA m8n8k4):
 //   Y = E_iu * H with H[t][t'] = (-1)^|t'| R[t + t'] gathered through the
-//   multi-index sum table, then (ab|ab) += Y * E_ku^T.
+//   multi-index sum table, then M_ik = Y * E_ku^T.
+// Swapping the units negates P - Q, R_tau(-d) = (-1)^|tau| R_tau(d), so
+// M_ki = M_ik^T and (ab|ab) = sum_(i,k) M_ik = A + A^T with
+// A = sum_(i<k) M_ik + 1/2 sum_i M_ii: only the unordered unit pairs are
+// computed.
 __device__ __forceinline__ void sw_dmma(double& d0, double& d1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
                : "+d"(d0), "+d"(d1)
@@ -144,12 +148,13 @@ __global__ void __launch_bounds__(256) k_schwarz_bra(DevBasis B, const int2* __r
   const int u0 = pair_unit0[pair];
   const int nu = sa.y * sb.y;
   for (int iu = 0; iu < nu; ++iu)
-    for (int ku = 0; ku < nu; ++ku) {
+    for (int ku = iu; ku < nu; ++ku) {
       const double4 P = U.unit_pP[u0 + iu], Q = U.unit_pP[u0 + ku];
       const double p = P.x, q = Q.x, pq = p + q, alpha = p * q / pq;
       const double X = P.y - Q.y, Yd = P.z - Q.z, Z = P.w - Q.w;
       const double T = alpha * (X * X + Yd * Yd + Z * Z);
       const double pref = kTwoPi52 / (p * q * sqrt(pq));
+      const double w = ku == iu ? 0.5 : 1.0;
       __syncthreads();  // previous users of Rn / R buffers / Y are done
       if (tid <= L4) {
         double f = pref;
@@ -190,13 +195,17 @@ __global__ void __launch_bounds__(256) k_schwarz_bra(DevBasis B, const int2* __r
           sw_dmma(o0, o1, a, b);
         }
         const int cc = 8 * nt + 2 * t4;
-        if (r < nab && cc < nab) out[r * nab + cc] += o0;
-        if (r < nab && cc + 1 < nab) out[r * nab + cc + 1] += o1;
+        if (r < nab && cc < nab) out[r * nab + cc] = fma(w, o0, out[r * nab + cc]);
+        if (r < nab && cc + 1 < nab) out[r * nab + cc + 1] = fma(w, o1, out[r * nab + cc + 1]);
       }
     }
   __syncthreads();
   double s2 = 0.0;
-  for (int i = tid; i < nab * nab; i += blockDim.x) s2 += out[i] * out[i];
+  for (int i = tid; i < nab * nab; i += blockDim.x) {
+    const int r = i / nab, c = i - r * nab;
+    const double v = out[i] + out[c * nab + r];
+    s2 = fma(v, v, s2);
+  }
   for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
   if (lane == 0) red[warp] = s2;
   __syncthreads();
@@ -207,13 +216,17 @@ __global__ void __launch_bounds__(256) k_schwarz_bra(DevBasis B, const int2* __r
   }
 }
 
-// Schwarz values of low-L pairs (Lab <= kSwLab), one warp per pair: the same
-// arithmetic as k_schwarz_bra with warp barriers instead of block barriers
-// (most pairs of a basis are low-L, and for them the block version mostly
-// waits at its barriers). Launches per group of L_ab classes, each warp's
-// scratch sized for the group's largest class (sw_nr R entries, sw_nab x sw_nh
-// Y, sw_nab^2 out, stride sw_stride doubles), so low-L classes keep many more
-// warps resident.
+// Schwarz values of low-L pairs (Lab <= kSwLab), one warp per pair, with warp
+// barriers instead of block barriers (most pairs of a basis are low-L, and for
+// them the block version mostly waits at its barriers). Same unordered unit
+// pairs and A + A^T as k_schwarz_bra, with the products reassociated: R is
+// built for the displacement Q - P (R~ = (-1)^|tau| R), so that
+// H[t][t'] = (-1)^|t| R~[t + t'] carries the sign on the output row, and
+//   Z_i = sum_(k>=i) w_ik H_ik E_ku^T   (NH x nab, w_ii = 1/2)
+//   A  += E_iu Z_i                       (once per iu, not per unit pair).
+// Launches per group of L_ab classes, each warp's scratch sized for the
+// group's largest class (sw_nr R entries, sw_nh x sw_nab Z, sw_nab^2 A, stride
+// sw_stride doubles), so low-L classes keep many more warps resident.
 constexpr int kSwLab = 4;
 constexpr int kSwNR = ncum(2 * kSwLab);
 constexpr int kSwNH = ncum(kSwLab);
@@ -239,20 +252,24 @@ __global__ void __launch_bounds__(32 * kSwWarps) k_schwarz_bra_warp(
   double* Rn = sw_smem + warp * sw_stride;
   double* R0 = Rn + 32;
   double* R1 = R0 + sw_nr;
-  double* Y = R1 + sw_nr;            // [nab][NH]
-  double* out = Y + sw_nab * sw_nh;  // [nab][nab]
+  double* Zs = R1 + sw_nr;            // Z_i [NH][nab]
+  double* out = Zs + sw_nab * sw_nh;  // A [nab][nab]
   const IndexTables* it = dt.idx;
   for (int k = lane; k < nab * nab; k += 32) out[k] = 0.0;
   const int u0 = pair_unit0[pair];
   const int nu = sa.y * sb.y;
-  for (int iu = 0; iu < nu; ++iu)
-    for (int ku = 0; ku < nu; ++ku) {
-      const double4 P = U.unit_pP[u0 + iu], Q = U.unit_pP[u0 + ku];
+  for (int iu = 0; iu < nu; ++iu) {
+    const double4 P = U.unit_pP[u0 + iu];
+    __syncwarp();  // the previous A update has read Z
+    for (int k = lane; k < NH * nab; k += 32) Zs[k] = 0.0;
+    for (int ku = iu; ku < nu; ++ku) {
+      const double4 Q = U.unit_pP[u0 + ku];
       const double p = P.x, q = Q.x, pq = p + q, alpha = p * q / pq;
-      const double X = P.y - Q.y, Yd = P.z - Q.z, Z = P.w - Q.w;
+      const double X = Q.y - P.y, Yd = Q.z - P.z, Z = Q.w - P.w;
       const double T = alpha * (X * X + Yd * Yd + Z * Z);
       const double pref = kTwoPi52 / (p * q * sqrt(pq));
-      __syncwarp();  // previous users of Rn / R / Y are done
+      const double w = ku == iu ? 0.5 : 1.0;
+      __syncwarp();  // previous users of Rn / R are done
       if (lane <= L4) {
         double f = pref;
         for (int k = 0; k < lane; ++k) f *= -2.0 * alpha;
@@ -260,29 +277,34 @@ __global__ void __launch_bounds__(32 * kSwWarps) k_schwarz_bra_warp(
       }
       __syncwarp();
       hermite_R(dt.rdesc, L4, Rn, X, Yd, Z, R0, R1, lane, 32, WarpSync());
-      const double* Ei = U.esph + U.unit_esph[u0 + iu];
       const double* Ek = U.esph + U.unit_esph[u0 + ku];
-      for (int idx = lane; idx < nab * NH; idx += 32) {
-        const int rr = idx / NH, tp = idx - rr * NH;
-        const double* e = Ei + rr * NH;
-        const int16_t* sidx = dt.sum_idx + tp;
-        double y = 0.0;
-        for (int t = 0; t < NH; ++t) y = fma(e[t], R0[__ldg(sidx + t * kNSum)], y);
-        Y[idx] = (it->xyz[tp][3] & 1) ? -y : y;
-      }
-      __syncwarp();
-      for (int idx = lane; idx < nab * nab; idx += 32) {
-        const int rr = idx / nab, sc = idx - rr * nab;
+      // each lane updates its own entries of Z (the same ones it zeroed)
+      for (int idx = lane; idx < NH * nab; idx += 32) {
+        const int t = idx / nab, sc = idx - t * nab;
         const double* e = Ek + sc * NH;
-        const double* yr = Y + rr * NH;
-        double v = 0.0;
-        for (int tp = 0; tp < NH; ++tp) v = fma(yr[tp], e[tp], v);
-        out[idx] += v;
+        const int16_t* sidx = dt.sum_idx + t * kNSum;
+        double z = 0.0;
+        for (int tp = 0; tp < NH; ++tp) z = fma(R0[__ldg(sidx + tp)], e[tp], z);
+        Zs[idx] = fma((it->xyz[t][3] & 1) ? -w : w, z, Zs[idx]);
       }
     }
+    __syncwarp();
+    const double* Ei = U.esph + U.unit_esph[u0 + iu];
+    for (int idx = lane; idx < nab * nab; idx += 32) {
+      const int rr = idx / nab, sc = idx - rr * nab;
+      const double* e = Ei + rr * NH;
+      double v = 0.0;
+      for (int t = 0; t < NH; ++t) v = fma(e[t], Zs[t * nab + sc], v);
+      out[idx] += v;
+    }
+  }
   __syncwarp();
   double s2 = 0.0;
-  for (int k = lane; k < nab * nab; k += 32) s2 += out[k] * out[k];
+  for (int k = lane; k < nab * nab; k += 32) {
+    const int rr = k / nab, sc = k - rr * nab;
+    const double v = out[k] + out[sc * nab + rr];
+    s2 = fma(v, v, s2);
+  }
   for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
   if (lane == 0) Qab[pair] = sqrt(sqrt(s2));
 }
