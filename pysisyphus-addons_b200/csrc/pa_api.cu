@@ -9,7 +9,7 @@
 //   screened 3c2e contraction (k_df3c<LAB,LC>) -> ordered reduction
 //   B = L^-1 df (blocked forward substitution) [-> Coulomb tensor]
 #include <cub/device/device_reduce.cuh>
-#include <cub/device/device_segmented_radix_sort.cuh>
+#include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
 #include <limits>
@@ -458,9 +458,8 @@ __global__ void k_gather_unit_keys(int n, const int* __restrict__ class_unit,
                                    double* keys, int* vals) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const int u = class_unit[i];
-  keys[i] = Qab[unit_pair[u]];
-  vals[i] = u;
+  keys[i] = Qab[unit_pair[class_unit[i]]];
+  vals[i] = i;  // input position; class_sort_desc maps it back to the unit
 }
 
 // Sort keys of the auxiliary shells: Q_c, or with QVL screening (qvl != null)
@@ -482,7 +481,7 @@ __global__ void k_gather_aux_keys(int n, const int* __restrict__ shells, const d
     key = fmax(key, kPi * sqrt(2.0) * eb.y / (den_min * rl));
   }
   keys[i] = key;
-  vals[i] = s;
+  vals[i] = i;  // input position; class_sort_desc maps it back to the shell
 }
 
 // Per auxiliary slot: (Q_c, extent, beta, 0) of the sorted shell (QVL screening).
@@ -501,6 +500,29 @@ __global__ void k_boys_eval(DeviceTables dt, int mode, int nmax, int n, const do
   out[i] = boys_n(dt, mode, m, T[k]);
 }
 
+// Class of each entry of a globally sorted list, found from its input
+// position (inputs are ordered by class, class c at [off[c], off[c+1])).
+__global__ void k_class_of_sorted(int n, const int* __restrict__ pos, const int* __restrict__ off,
+                                  int nseg, unsigned char* cls, int* idx) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const int i = pos[j];
+  int c = 0;
+  while (c + 1 < nseg && i >= off[c + 1]) ++c;
+  cls[j] = static_cast<unsigned char>(c);
+  idx[j] = j;
+}
+
+__global__ void k_class_sort_finish(int n, const int* __restrict__ order, const double* __restrict__ keys,
+                                    const int* __restrict__ pos, const int* __restrict__ ids,
+                                    double* keys_out, int* ids_out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int j = order[k];
+  keys_out[k] = keys[j];
+  ids_out[k] = ids[pos[j]];
+}
+
 // Buffers of one density-fitting run.
 struct DfBuffers {
   double *Qab, *Qc, *qmax, *esph, *ukeys, *slot_Q, *akeys, *aux_Q, *G, *M, *partial, *lawork,
@@ -512,6 +534,10 @@ struct DfBuffers {
   double* slot_den;
   int *uvals, *sorted_unit, *avals, *sorted_aux, *info;
   int* counters = nullptr;  // one work counter per class run
+  // class_sort_desc scratch (max(nunits, naux shells) entries each)
+  double* sort_k;
+  int *sort_p, *sort_j, *sort_j2;
+  unsigned char *sort_c, *sort_c2;
   void* cub_tmp;
   size_t cub_bytes;
   std::vector<long long> g_off;      // per Lab class
@@ -524,18 +550,41 @@ struct DfBuffers {
 };
 
 size_t cub_temp_bytes(const pa_basis_s* orb, const pa_basis_s* aux) {
-  size_t b1 = 0, b2 = 0, b3 = 0;
-  const int nu = orb->pairs.nunits, nx = static_cast<int>(aux->host.shells.size());
-  cub::DeviceSegmentedRadixSort::SortPairsDescending(nullptr, b1, (const double*)nullptr, (double*)nullptr,
-                                                     (const int*)nullptr, (int*)nullptr, nu,
-                                                     orb->pairs.lab_max + 1, (const int*)nullptr,
-                                                     (const int*)nullptr);
-  cub::DeviceSegmentedRadixSort::SortPairsDescending(nullptr, b2, (const double*)nullptr, (double*)nullptr,
-                                                     (const int*)nullptr, (int*)nullptr, nx,
-                                                     aux->aux.lc_max + 1, (const int*)nullptr,
-                                                     (const int*)nullptr);
-  cub::DeviceReduce::Max(nullptr, b3, (const double*)nullptr, (double*)nullptr, nx);
-  return std::max(b1, std::max(b2, b3));
+  size_t need = 0;
+  for (const int n : {orb->pairs.nunits, static_cast<int>(aux->host.shells.size())}) {
+    size_t b1 = 0, b2 = 0, b3 = 0;
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, b1, (const double*)nullptr, (double*)nullptr,
+                                              (const int*)nullptr, (int*)nullptr, n, 0, 64);
+    cub::DeviceRadixSort::SortPairs(nullptr, b2, (const unsigned char*)nullptr, (unsigned char*)nullptr,
+                                    (const int*)nullptr, (int*)nullptr, n, 0, 8);
+    cub::DeviceReduce::Max(nullptr, b3, (const double*)nullptr, (double*)nullptr, n);
+    need = std::max(need, std::max(b1, std::max(b2, b3)));
+  }
+  return need;
+}
+
+// Stable descending sort of keys[0, n) inside each class segment
+// [off[c], off[c+1]), c < nseg, of a class-ordered input: one global stable
+// sort by key (position as value), then a stable sort by class. Within a class
+// this is key-descending with ties in input order, the order of a segmented
+// radix sort, but every pass runs on all SMs (a segmented sort gives each
+// segment one block, and there are only a handful of classes). Writes the
+// sorted keys and ids[position] of the entries.
+int class_sort_desc(DfBuffers& b, const double* keys, const int* positions, const int* ids,
+                    const int* d_off, int nseg, int n, double* keys_out, int* ids_out, cudaStream_t s) {
+  if (n <= 0) return 0;
+  size_t bytes = b.cub_bytes;
+  PA_CUDA(cub::DeviceRadixSort::SortPairsDescending(b.cub_tmp, bytes, keys, b.sort_k, positions, b.sort_p,
+                                                    n, 0, 64, s));
+  const int grid = (n + 255) / 256;
+  k_class_of_sorted<<<grid, 256, 0, s>>>(n, b.sort_p, d_off, nseg, b.sort_c, b.sort_j);
+  int bits = 1;
+  while ((1 << bits) < nseg) ++bits;
+  bytes = b.cub_bytes;
+  PA_CUDA(cub::DeviceRadixSort::SortPairs(b.cub_tmp, bytes, b.sort_c, b.sort_c2, b.sort_j, b.sort_j2, n, 0,
+                                          bits, s));
+  k_class_sort_finish<<<grid, 256, 0, s>>>(n, b.sort_j2, b.sort_k, b.sort_p, ids, keys_out, ids_out);
+  return 4;  // two kernels of this file + two CUB sort calls
 }
 
 // Lays out all buffers of a run (counting when c.base == nullptr).
@@ -573,6 +622,13 @@ void layout_df(Carver& c, const pa_basis_s* orb, const pa_basis_s* aux, int nd, 
   b->M = c.take<double>(naux * naux);
   b->lawork = c.take<double>(linalg_workspace_doubles(static_cast<int>(naux)));
   b->df_raw = c.take<double>(static_cast<size_t>(naux) * nd);
+  const int nsort = std::max(P.nunits, nx);
+  b->sort_k = c.take<double>(nsort);
+  b->sort_p = c.take<int>(nsort);
+  b->sort_j = c.take<int>(nsort);
+  b->sort_j2 = c.take<int>(nsort);
+  b->sort_c = c.take<unsigned char>(nsort);
+  b->sort_c2 = c.take<unsigned char>(nsort);
   b->cub_bytes = cub_temp_bytes(orb, aux);
   b->cub_tmp = c.take<char>(b->cub_bytes);
   // partial slabs; the work-item granularity grows with the system size (on
@@ -653,18 +709,12 @@ int run_screening(const pa_basis_s* orb, const pa_basis_s* aux, const DeviceTabl
     k_gather_unit_keys<<<(P.nunits + 255) / 256, 256, 0, s>>>(P.nunits, orb->d_class_unit,
                                                               orb->d_unit_pair, b.Qab, b.ukeys, b.uvals);
     ++*launches;
-    size_t bytes = b.cub_bytes;
-    PA_CUDA(cub::DeviceSegmentedRadixSort::SortPairsDescending(
-        b.cub_tmp, bytes, b.ukeys, b.slot_Q, b.uvals, b.sorted_unit, P.nunits, P.lab_max + 1,
-        orb->d_class_off, orb->d_class_off + 1, 0, 64, s));
-    *launches += 2;
+    *launches += class_sort_desc(b, b.ukeys, b.uvals, orb->d_class_unit, orb->d_class_off, P.lab_max + 1,
+                                 P.nunits, b.slot_Q, b.sorted_unit, s);
   }
   if (nx > 0) {
-    size_t bytes = b.cub_bytes;
-    PA_CUDA(cub::DeviceSegmentedRadixSort::SortPairsDescending(
-        b.cub_tmp, bytes, b.akeys, b.aux_Q, b.avals, b.sorted_aux, nx, aux->aux.lc_max + 1,
-        aux->d_aux_off, aux->d_aux_off + 1, 0, 64, s));
-    *launches += 2;
+    *launches += class_sort_desc(b, b.akeys, b.avals, aux->d_aux_shell, aux->d_aux_off, aux->aux.lc_max + 1,
+                                 nx, b.aux_Q, b.sorted_aux, s);
     if (qvl) {
       k_aux_slot_qvl<<<(nx + 255) / 256, 256, 0, s>>>(nx, b.sorted_aux, b.Qc, aux->d_aux_qvl, b.aux_slot_qvl);
       ++*launches;
