@@ -35,10 +35,13 @@ __device__ __forceinline__ int cidx_sum(const IndexTables* __restrict__ it, int 
 }
 
 // ---------------------------------------------------------------------------
+// One block per unit (higher L_ab classes; units: the class's slice of the
+// class-ordered unit list).
 __global__ void __launch_bounds__(128) k_unit_setup(DevBasis B, const int2* __restrict__ pair_ab,
-                                                    UnitArrays U, int nunits, DeviceTables dt) {
-  const int u = blockIdx.x;
-  if (u >= nunits) return;
+                                                    UnitArrays U, const int* __restrict__ units, int nunits,
+                                                    DeviceTables dt) {
+  if (static_cast<int>(blockIdx.x) >= nunits) return;
+  const int u = units[blockIdx.x];
   __shared__ double E[3][(PA_LMAX + 1) * (PA_LMAX + 1) * (2 * PA_LMAX + 1)];
   __shared__ double sh[8];
   const int pair = U.unit_pair[u];
@@ -96,6 +99,72 @@ __global__ void __launch_bounds__(128) k_unit_setup(DevBasis B, const int2* __re
         if (tt.x > ea.x + eb.x || tt.y > ea.y + eb.y || tt.z > ea.z + eb.z) continue;
         v += ca * dt.sph_val[kb] * E[0][(ea.x * nj + eb.x) * nt + tt.x] *
              E[1][(ea.y * nj + eb.y) * nt + tt.y] * E[2][(ea.z * nj + eb.z) * nt + tt.z];
+      }
+    }
+    out[idx] = pref * v;
+  }
+}
+
+// One warp per unit for the low classes (L_a + L_b <= kUsLab, at most 90
+// E_sph entries, where a block per unit mostly idles): every lane forms the
+// Gaussian-product data itself, lanes 0-2 the 1D Hermite coefficients.
+constexpr int kUsLab = 2;
+constexpr int kUsE = 12;  // largest (la+1)(lb+1)(la+lb+1) with la + lb <= kUsLab
+constexpr int kUsWarps = 8;
+
+__global__ void __launch_bounds__(32 * kUsWarps) k_unit_setup_warp(DevBasis B, const int2* __restrict__ pair_ab,
+                                                                 UnitArrays U, const int* __restrict__ units,
+                                                                 int nunits, DeviceTables dt) {
+  __shared__ double E[kUsWarps][3][kUsE];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = blockIdx.x * kUsWarps + warp;
+  if (i >= nunits) return;  // warp-uniform
+  const int u = units[i];
+  const int pair = U.unit_pair[u];
+  const int2 ab = pair_ab[pair];
+  const int4 sa = B.shell[ab.x], sb = B.shell[ab.y];
+  const int la = sa.x, lb = sb.x;
+  const int2 pr = U.unit_prims[u];
+  const double4 A = B.center[ab.x], Bc = B.center[ab.y];
+  const double2 pa_ = B.prim[pr.x], pb_ = B.prim[pr.y];
+  const double p = pa_.x + pb_.x;
+  const double Px = (pa_.x * A.x + pb_.x * Bc.x) / p;
+  const double Py = (pa_.x * A.y + pb_.x * Bc.y) / p;
+  const double Pz = (pa_.x * A.z + pb_.x * Bc.z) / p;
+  if (lane == 0) U.unit_pP[u] = make_double4(p, Px, Py, Pz);
+  if (lane < 3) {
+    const double Pd = lane == 0 ? Px : (lane == 1 ? Py : Pz);
+    const double Ad = lane == 0 ? A.x : (lane == 1 ? A.y : A.z);
+    const double Bd = lane == 0 ? Bc.x : (lane == 1 ? Bc.y : Bc.z);
+    hermite_E_1d(la, lb, Pd - Ad, Pd - Bd, 0.5 / p, E[warp][lane]);
+  }
+  const double ABx = A.x - Bc.x, ABy = A.y - Bc.y, ABz = A.z - Bc.z;
+  const double pref = pa_.y * pb_.y * exp(-pa_.x * pb_.x / p * (ABx * ABx + ABy * ABy + ABz * ABz));
+  __syncwarp();
+  const IndexTables* it = dt.idx;
+  const int nsb = 2 * lb + 1;
+  const int nab = (2 * la + 1) * nsb;
+  const int NH = ncum(la + lb);
+  const int nt = la + lb + 1, nj = lb + 1;
+  const int offa = ncum(la - 1 < 0 ? -1 : la - 1), offb = ncum(lb - 1 < 0 ? -1 : lb - 1);
+  const double* E0 = E[warp][0];
+  const double* E1 = E[warp][1];
+  const double* E2 = E[warp][2];
+  double* out = U.esph + U.unit_esph[u];
+  for (int idx = lane; idx < nab * NH; idx += 32) {
+    const int r = idx / NH, t = idx - r * NH;
+    const int ma = r / nsb, mb = r - ma * nsb;
+    const uchar4 tt = *reinterpret_cast<const uchar4*>(it->xyz[t]);
+    const int rowa = sph_row(la, ma), rowb = sph_row(lb, mb);
+    double v = 0.0;
+    for (int ka = dt.sph_start[rowa]; ka < dt.sph_start[rowa + 1]; ++ka) {
+      const uchar4 ea = *reinterpret_cast<const uchar4*>(it->xyz[offa + dt.sph_col[ka]]);
+      const double ca = dt.sph_val[ka];
+      for (int kb = dt.sph_start[rowb]; kb < dt.sph_start[rowb + 1]; ++kb) {
+        const uchar4 eb = *reinterpret_cast<const uchar4*>(it->xyz[offb + dt.sph_col[kb]]);
+        if (tt.x > ea.x + eb.x || tt.y > ea.y + eb.y || tt.z > ea.z + eb.z) continue;
+        v += ca * dt.sph_val[kb] * E0[(ea.x * nj + eb.x) * nt + tt.x] * E1[(ea.y * nj + eb.y) * nt + tt.y] *
+             E2[(ea.z * nj + eb.z) * nt + tt.z];
       }
     }
     out[idx] = pref * v;
@@ -490,11 +559,23 @@ __global__ void __launch_bounds__(256) k_bra_prep(DevBasis B, const int2* __rest
 // ---------------------------------------------------------------------------
 // Launchers.
 
-int launch_unit_setup(const DevBasis& B, const int2* pair_ab, UnitArrays U, int nunits,
-                      const DeviceTables& dt, cudaStream_t s) {
-  if (nunits == 0) return 0;
-  k_unit_setup<<<nunits, 128, 0, s>>>(B, pair_ab, U, nunits, dt);
-  return 1;
+int launch_unit_setup(const DevBasis& B, const int2* pair_ab, const int* class_unit, const PairLists& P,
+                      UnitArrays U, const DeviceTables& dt, cudaStream_t s) {
+  if (P.nunits == 0) return 0;
+  int launches = 0;
+  const int split = std::min(kUsLab, P.lab_max) + 1;  // classes [0, split) by warps
+  const int nlow = P.class_off[split];
+  if (nlow > 0) {
+    k_unit_setup_warp<<<(nlow + kUsWarps - 1) / kUsWarps, 32 * kUsWarps, 0, s>>>(B, pair_ab, U, class_unit, nlow,
+                                                                                 dt);
+    ++launches;
+  }
+  const int nhigh = P.nunits - nlow;
+  if (nhigh > 0) {
+    k_unit_setup<<<nhigh, 128, 0, s>>>(B, pair_ab, U, class_unit + nlow, nhigh, dt);
+    ++launches;
+  }
+  return launches;
 }
 
 // Shared memory of k_schwarz_bra for the pairs of class Lab = lab.

@@ -691,7 +691,7 @@ int run_screening(const pa_basis_s* orb, const pa_basis_s* aux, const DeviceTabl
   const PairLists& P = orb->pairs;
   const int nx = static_cast<int>(aux->host.shells.size());
   UnitArrays U = unit_arrays(orb, b);
-  *launches += launch_unit_setup(orb->dev, orb->d_pair_ab, U, P.nunits, dt, s);
+  *launches += launch_unit_setup(orb->dev, orb->d_pair_ab, orb->d_class_unit, P, U, dt, s);
   *launches += launch_schwarz_bra(orb->dev, orb->d_pair_ab, orb->d_pair_unit0, orb->d_class_pair, P, U, dt,
                                   o.boys_mode, b.Qab, s);
   *launches += launch_schwarz_aux(aux->dev, dt, o.boys_mode, b.Qc, s);
@@ -1523,7 +1523,7 @@ int std_device(pa_basis orb, pa_basis aux, int kind, int nmos, const double* d_m
   U.unit_esph = orb->d_unit_esph;
   U.unit_pP = b.pP;
   U.esph = b.esph;
-  launches += launch_unit_setup(orb->dev, orb->d_pair_ab, U, P.nunits, dt, s);
+  launches += launch_unit_setup(orb->dev, orb->d_pair_ab, orb->d_class_unit, P, U, dt, s);
   launches += launch_schwarz_bra(orb->dev, orb->d_pair_ab, orb->d_pair_unit0, orb->d_class_pair, P, U, dt,
                                  o.boys_mode, b.Qab, s);
   launches += launch_schwarz_aux(aux->dev, dt, o.boys_mode, b.Qc, s);
@@ -1920,7 +1920,7 @@ static int schwarz_impl(pa_basis orb, pa_basis aux, double* q_bra, double* q_aux
     U.unit_esph = orb->d_unit_esph;
     U.unit_pP = pP;
     U.esph = esph;
-    launches += launch_unit_setup(orb->dev, orb->d_pair_ab, U, P.nunits, dt, s);
+    launches += launch_unit_setup(orb->dev, orb->d_pair_ab, orb->d_class_unit, P, U, dt, s);
     launches += launch_schwarz_bra(orb->dev, orb->d_pair_ab, orb->d_pair_unit0, orb->d_class_pair, P, U, dt,
                                    o.boys_mode, Qab, s);
     if (P.npairs) PA_CUDA(cudaMemcpyAsync(q_bra, Qab, sizeof(double) * P.npairs, cudaMemcpyDeviceToHost, s));

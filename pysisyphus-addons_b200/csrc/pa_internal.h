@@ -131,8 +131,10 @@ struct UnitArrays {
   double* esph;       // E_sph blocks
 };
 
-int launch_unit_setup(const DevBasis& B, const int2* pair_ab, UnitArrays U, int nunits,
-                      const DeviceTables& dt, cudaStream_t s);
+// Unit data of all bra units: classes L_ab <= 2 one warp per unit, the others
+// one block per unit (class_unit: device copy of P.class_unit).
+int launch_unit_setup(const DevBasis& B, const int2* pair_ab, const int* class_unit, const PairLists& P,
+                      UnitArrays U, const DeviceTables& dt, cudaStream_t s);
 // Schwarz values of all pairs: pairs with Lab <= 4 one warp each, the others
 // one block each (class_pair: device copy of P.class_pair).
 int launch_schwarz_bra(const DevBasis& B, const int2* pair_ab, const int* pair_unit0,
