@@ -378,6 +378,174 @@ __global__ void __launch_bounds__(32 * kSwWarps) k_schwarz_bra_warp(
   if (lane == 0) Qab[pair] = sqrt(sqrt(s2));
 }
 
+// Schwarz values of the classes L_ab = LAB (3 and 4), one warp per pair, with
+// both products of k_schwarz_bra_warp on the FP64 tensor cores (DMMA
+// m8n8k4): Z_i (NH x nab, in registers across the unit pairs k >= i) gets
+// the tiles H_ik E_ku^T with H gathered from R~ through the multi-index sum
+// table, and A (nab x nab, in registers across the whole pair) gets E_iu Z_i.
+// Fragments: lane (g = lane / 4, t4 = lane % 4) holds A-row g / k-column t4,
+// B-column g / k-row t4, and accumulator row g, columns 2 t4 and 2 t4 + 1.
+constexpr int sw_nab_max(int lab) {
+  int m = 1;
+  for (int la = 0; la <= PA_LMAX; ++la) {
+    const int lb = lab - la;
+    if (lb < 0 || lb > PA_LMAX) continue;
+    const int v = (2 * la + 1) * (2 * lb + 1);
+    m = v > m ? v : m;
+  }
+  return m;
+}
+
+template <int LAB>
+struct SwDmma {
+  static constexpr int NH = ncum(LAB);
+  static constexpr int NR = ncum(2 * LAB);
+  static constexpr int NABM = sw_nab_max(LAB);
+  static constexpr int MT = (NH + 7) / 8;    // row tiles of Z
+  static constexpr int KT = (NH + 3) / 4;    // k steps of both products
+  static constexpr int NT = (NABM + 7) / 8;  // column tiles of Z, row and column tiles of A
+  static constexpr int STRIDE = 32 + 2 * NR + NH * NABM + NABM * NABM;  // doubles per warp
+};
+
+template <int LAB>
+__global__ void __launch_bounds__(32 * kSwWarps) k_schwarz_bra_dmma(
+    DevBasis B, const int2* __restrict__ pair_ab, const int* __restrict__ pair_unit0,
+    const int* __restrict__ pair_list, UnitArrays U, int npairs, DeviceTables dt, int boys_mode,
+    double* __restrict__ Qab) {
+  using C = SwDmma<LAB>;
+  constexpr int NH = C::NH, MT = C::MT, KT = C::KT, NT = C::NT;
+  extern __shared__ double sw_smem[];  // [kSwWarps][STRIDE]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t4 = lane & 3;
+  const int i = blockIdx.x * kSwWarps + warp;
+  if (i >= npairs) return;  // warp-uniform
+  const int pair = pair_list[i];
+  const int2 ab = pair_ab[pair];
+  const int4 sa = B.shell[ab.x], sb = B.shell[ab.y];
+  const int nab = (2 * sa.x + 1) * (2 * sb.x + 1);
+  const int ntr = (nab + 7) / 8;  // column tiles in use (warp-uniform)
+  double* Rn = sw_smem + warp * C::STRIDE;
+  double* R0 = Rn + 32;
+  double* R1 = R0 + C::NR;
+  double* Zs = R1 + C::NR;            // Z_i [NH][nab]
+  double* out = Zs + NH * C::NABM;    // A [nab][nab]
+  const IndexTables* it = dt.idx;
+  const int u0 = pair_unit0[pair];
+  const int nu = sa.y * sb.y;
+  double aacc[NT][NT][2];
+#pragma unroll
+  for (int mt = 0; mt < NT; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) aacc[mt][nt][0] = aacc[mt][nt][1] = 0.0;
+  for (int iu = 0; iu < nu; ++iu) {
+    const double4 P = U.unit_pP[u0 + iu];
+    double zacc[MT][NT][2];
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt) zacc[mt][nt][0] = zacc[mt][nt][1] = 0.0;
+    for (int ku = iu; ku < nu; ++ku) {
+      const double4 Q = U.unit_pP[u0 + ku];
+      const double p = P.x, q = Q.x, pq = p + q, alpha = p * q / pq;
+      const double X = Q.y - P.y, Yd = Q.z - P.z, Z = Q.w - P.w;
+      const double T = alpha * (X * X + Yd * Yd + Z * Z);
+      const double pref = kTwoPi52 / (p * q * sqrt(pq));
+      __syncwarp();  // previous readers of Rn / R are done
+      if (lane <= 2 * LAB) {
+        double f = pref;
+        for (int k = 0; k < lane; ++k) f *= -2.0 * alpha;
+        Rn[lane] = f * boys_n(dt, boys_mode, lane, T);
+      }
+      __syncwarp();
+      hermite_R(dt.rdesc, 2 * LAB, Rn, X, Yd, Z, R0, R1, lane, 32, WarpSync());
+      const double* Ek = U.esph + U.unit_esph[u0 + ku];
+#pragma unroll
+      for (int k4 = 0; k4 < KT; ++k4) {
+        const int tp = 4 * k4 + t4;
+        double af[MT], bf[NT];
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) {
+          const int t = 8 * mt + g;
+          af[mt] = (t < NH && tp < NH) ? R0[__ldg(dt.sum_idx + t * kNSum + tp)] : 0.0;
+        }
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt) {
+          const int c = 8 * nt + g;
+          bf[nt] = (nt < ntr && tp < NH && c < nab) ? Ek[c * NH + tp] : 0.0;
+        }
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+          for (int nt = 0; nt < NT; ++nt)
+            if (nt < ntr) sw_dmma(zacc[mt][nt][0], zacc[mt][nt][1], af[mt], bf[nt]);
+      }
+      if (ku == iu) {  // weight 1/2 of the diagonal unit pair (exact scaling)
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+          for (int nt = 0; nt < NT; ++nt) {
+            zacc[mt][nt][0] *= 0.5;
+            zacc[mt][nt][1] *= 0.5;
+          }
+      }
+    }
+    __syncwarp();  // the previous A step has read Zs
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) {
+      const int t = 8 * mt + g;
+      if (t >= NH) continue;
+      const double sg = (it->xyz[t][3] & 1) ? -1.0 : 1.0;  // (-1)^|t| of H = (-1)^|t| R~
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt) {
+        const int c = 8 * nt + 2 * t4;
+        if (c < nab) Zs[t * nab + c] = sg * zacc[mt][nt][0];
+        if (c + 1 < nab) Zs[t * nab + c + 1] = sg * zacc[mt][nt][1];
+      }
+    }
+    __syncwarp();
+    const double* Ei = U.esph + U.unit_esph[u0 + iu];
+#pragma unroll
+    for (int k4 = 0; k4 < KT; ++k4) {
+      const int t = 4 * k4 + t4;
+      double af[NT], bf[NT];
+#pragma unroll
+      for (int mt = 0; mt < NT; ++mt) {
+        const int r = 8 * mt + g;
+        af[mt] = (mt < ntr && r < nab && t < NH) ? Ei[r * NH + t] : 0.0;
+      }
+#pragma unroll
+      for (int nt = 0; nt < NT; ++nt) {
+        const int c = 8 * nt + g;
+        bf[nt] = (nt < ntr && t < NH && c < nab) ? Zs[t * nab + c] : 0.0;
+      }
+#pragma unroll
+      for (int mt = 0; mt < NT; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt)
+          if (mt < ntr && nt < ntr) sw_dmma(aacc[mt][nt][0], aacc[mt][nt][1], af[mt], bf[nt]);
+    }
+  }
+#pragma unroll
+  for (int mt = 0; mt < NT; ++mt) {
+    const int r = 8 * mt + g;
+    if (r >= nab) continue;
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+      const int c = 8 * nt + 2 * t4;
+      if (c < nab) out[r * nab + c] = aacc[mt][nt][0];
+      if (c + 1 < nab) out[r * nab + c + 1] = aacc[mt][nt][1];
+    }
+  }
+  __syncwarp();
+  double s2 = 0.0;
+  for (int k = lane; k < nab * nab; k += 32) {
+    const int rr = k / nab, sc = k - rr * nab;
+    const double v = out[k] + out[sc * nab + rr];
+    s2 = fma(v, v, s2);
+  }
+  for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+  if (lane == 0) Qab[pair] = sqrt(sqrt(s2));
+}
+
 // ---------------------------------------------------------------------------
 // Two-center block (P|Q)[mP][mQ] of two auxiliary shells, computed by one warp.
 // Scratch (per warp): Rn[16], R0/R1[ncum(lP+lQ)], Y[nsP * ncart(lQ)], out[nsP * nsQ].
@@ -592,6 +760,17 @@ size_t schwarz_bra_smem(int lab) {
   return sizeof(double) * best;
 }
 
+template <int LAB>
+int launch_schwarz_dmma(const DevBasis& B, const int2* pair_ab, const int* pair_unit0, const int* pairs,
+                        UnitArrays U, int n, const DeviceTables& dt, int boys_mode, double* Qab, cudaStream_t s) {
+  const size_t smem = sizeof(double) * kSwWarps * SwDmma<LAB>::STRIDE;
+  cudaFuncSetAttribute(k_schwarz_bra_dmma<LAB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(smem));
+  k_schwarz_bra_dmma<LAB><<<(n + kSwWarps - 1) / kSwWarps, 32 * kSwWarps, smem, s>>>(
+      B, pair_ab, pair_unit0, pairs, U, n, dt, boys_mode, Qab);
+  return 1;
+}
+
 int launch_schwarz_bra(const DevBasis& B, const int2* pair_ab, const int* pair_unit0,
                        const int* class_pair, const PairLists& P, UnitArrays U, const DeviceTables& dt,
                        int boys_mode, double* Qab, cudaStream_t s) {
@@ -602,13 +781,20 @@ int launch_schwarz_bra(const DevBasis& B, const int2* pair_ab, const int* pair_u
   if (nlow > 0) {
     cudaFuncSetAttribute(k_schwarz_bra_warp, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          static_cast<int>(sizeof(double) * kSwWarps * kSwScratch));
-    // classes L_ab 0..2 together (their scratch is small either way), then
-    // 3 and 4 on their own
+    // classes L_ab 0..2 together (their scratch is small either way); 3 and 4
+    // on their own, with both products on the tensor cores
     for (int g = 0; g < split;) {
       const int lab = g < 2 ? std::min(2, split - 1) : g;  // largest class of the group
       const int off = P.pair_class_off[g], n = P.pair_class_off[lab + 1] - off;
       g = lab + 1;
       if (n <= 0) continue;
+      if (lab == 3 || lab == 4) {
+        launches += lab == 3 ? launch_schwarz_dmma<3>(B, pair_ab, pair_unit0, class_pair + off, U, n, dt,
+                                                      boys_mode, Qab, s)
+                             : launch_schwarz_dmma<4>(B, pair_ab, pair_unit0, class_pair + off, U, n, dt,
+                                                      boys_mode, Qab, s);
+        continue;
+      }
       int nab = 1;  // largest (2la+1)(2lb+1) with la + lb <= lab
       for (int l = 0; l <= lab; ++l)
         for (int la = std::max(0, l - PA_LMAX); la <= std::min(l, PA_LMAX); ++la)
