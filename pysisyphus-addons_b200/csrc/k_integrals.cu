@@ -172,128 +172,30 @@ __global__ void __launch_bounds__(32 * kUsWarps) k_unit_setup_warp(DevBasis B, c
 }
 
 // ---------------------------------------------------------------------------
-// Schwarz values of high-L pairs, one block per pair. For every pair of bra
-// units (iu, ku) the block is
-//   M_ik[r][s] = sum_(t,t') E_iu[r][t] (-1)^|t'| R[t + t'] E_ku[s][t'],
-// two small GEMMs run on the FP64 tensor cores (DMMA m8n8k4):
-//   Y = E_iu * H with H[t][t'] = (-1)^|t'| R[t + t'] gathered through the
-//   multi-index sum table, then M_ik = Y * E_ku^T.
+// Schwarz values sqrt(||(ab|ab)||_F) of the bra pairs. For every pair of bra
+// units (iu, ku) the block of the pair is
+//   M_ik[r][s] = sum_(t,t') E_iu[r][t] (-1)^|t'| R[t + t'] E_ku[s][t'].
 // Swapping the units negates P - Q, R_tau(-d) = (-1)^|tau| R_tau(d), so
 // M_ki = M_ik^T and (ab|ab) = sum_(i,k) M_ik = A + A^T with
 // A = sum_(i<k) M_ik + 1/2 sum_i M_ii: only the unordered unit pairs are
-// computed.
+// computed. R is built for the displacement Q - P (R~ = (-1)^|tau| R), so that
+// H[t][t'] = (-1)^|t| R~[t + t'] carries the sign on the output row, and the
+// products are reassociated:
+//   Z_i = sum_(k>=i) w_ik H_ik E_ku^T   (NH x nab, w_ii = 1/2)
+//   A  += E_iu Z_i                       (once per iu, not per unit pair).
+// Three kernels: k_schwarz_bra_warp (L_ab <= 2, one warp per pair, FP64 FMA),
+// k_schwarz_bra_dmma<LAB> (L_ab 3, 4, one warp per pair) and
+// k_schwarz_bra<LAB> (L_ab >= 5, one block per pair), the last two on the
+// FP64 tensor cores (DMMA m8n8k4).
 __device__ __forceinline__ void sw_dmma(double& d0, double& d1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
                : "+d"(d0), "+d"(d1)
                : "d"(a), "d"(b));
 }
 
-__global__ void __launch_bounds__(256) k_schwarz_bra(DevBasis B, const int2* __restrict__ pair_ab,
-                                                     const int* __restrict__ pair_unit0,
-                                                     const int* __restrict__ pair_list, UnitArrays U,
-                                                     int npairs, DeviceTables dt, int boys_mode,
-                                                     double* __restrict__ Qab) {
-  extern __shared__ double smem[];
-  if (static_cast<int>(blockIdx.x) >= npairs) return;
-  const int pair = pair_list[blockIdx.x];
-  const int2 ab = pair_ab[pair];
-  const int4 sa = B.shell[ab.x], sb = B.shell[ab.y];
-  const int la = sa.x, lb = sb.x;
-  const int nsb = 2 * lb + 1, nab = (2 * la + 1) * nsb;
-  const int NH = ncum(la + lb);
-  const int L4 = 2 * (la + lb);
-  const int NR = ncum(L4);
-  const int MT = (nab + 7) / 8, NT = (NH + 7) / 8, KT = (NH + 3) / 4;
-  const int YS = NT * 8 + 1;          // row stride of Y
-  double* Rn = smem;                  // 32
-  double* R0 = Rn + 32;               // NR
-  double* R1 = R0 + NR;               // NR
-  double* Y = R1 + NR;                // [MT * 8][YS]
-  double* out = Y + MT * 8 * YS;      // [nab][nab]
-  __shared__ double red[8];
-  const IndexTables* it = dt.idx;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
-  for (int i = tid; i < nab * nab; i += blockDim.x) out[i] = 0.0;
-  const int u0 = pair_unit0[pair];
-  const int nu = sa.y * sb.y;
-  for (int iu = 0; iu < nu; ++iu)
-    for (int ku = iu; ku < nu; ++ku) {
-      const double4 P = U.unit_pP[u0 + iu], Q = U.unit_pP[u0 + ku];
-      const double p = P.x, q = Q.x, pq = p + q, alpha = p * q / pq;
-      const double X = P.y - Q.y, Yd = P.z - Q.z, Z = P.w - Q.w;
-      const double T = alpha * (X * X + Yd * Yd + Z * Z);
-      const double pref = kTwoPi52 / (p * q * sqrt(pq));
-      const double w = ku == iu ? 0.5 : 1.0;
-      __syncthreads();  // previous users of Rn / R buffers / Y are done
-      if (tid <= L4) {
-        double f = pref;
-        for (int k = 0; k < tid; ++k) f *= -2.0 * alpha;
-        Rn[tid] = f * boys_n(dt, boys_mode, tid, T);
-      }
-      __syncthreads();
-      hermite_R(dt.rdesc, L4, Rn, X, Yd, Z, R0, R1, tid, blockDim.x, BlockSync());
-      const double* Ei = U.esph + U.unit_esph[u0 + iu];
-      const double* Ek = U.esph + U.unit_esph[u0 + ku];
-      // Y = Ei * H, one 8 x 8 tile per warp at a time
-      for (int tile = warp; tile < MT * NT; tile += 8) {
-        const int mt = tile / NT, nt = tile - mt * NT;
-        const int r = 8 * mt + g, c = 8 * nt + g;
-        double y0 = 0.0, y1 = 0.0;
-        for (int k4 = 0; k4 < KT; ++k4) {
-          const int k = 4 * k4 + t4;
-          const double a = (r < nab && k < NH) ? Ei[r * NH + k] : 0.0;
-          const double b = (k < NH && c < NH) ? R0[__ldg(dt.sum_idx + k * kNSum + c)] : 0.0;
-          sw_dmma(y0, y1, a, b);
-        }
-        const int cc = 8 * nt + 2 * t4;
-        double* yrow = Y + (8 * mt + g) * YS;
-        if (cc < NH) yrow[cc] = (it->xyz[cc][3] & 1) ? -y0 : y0;
-        if (cc + 1 < NH) yrow[cc + 1] = (it->xyz[cc + 1][3] & 1) ? -y1 : y1;
-      }
-      __syncthreads();
-      // out += Y * Ek^T
-      const int MT2 = MT, NT2 = (nab + 7) / 8;
-      for (int tile = warp; tile < MT2 * NT2; tile += 8) {
-        const int mt = tile / NT2, nt = tile - mt * NT2;
-        const int r = 8 * mt + g, c = 8 * nt + g;
-        double o0 = 0.0, o1 = 0.0;
-        for (int k4 = 0; k4 < KT; ++k4) {
-          const int k = 4 * k4 + t4;
-          const double a = (k < NH) ? Y[r * YS + k] : 0.0;  // rows >= nab of Y are never read below
-          const double b = (k < NH && c < nab) ? Ek[c * NH + k] : 0.0;
-          sw_dmma(o0, o1, a, b);
-        }
-        const int cc = 8 * nt + 2 * t4;
-        if (r < nab && cc < nab) out[r * nab + cc] = fma(w, o0, out[r * nab + cc]);
-        if (r < nab && cc + 1 < nab) out[r * nab + cc + 1] = fma(w, o1, out[r * nab + cc + 1]);
-      }
-    }
-  __syncthreads();
-  double s2 = 0.0;
-  for (int i = tid; i < nab * nab; i += blockDim.x) {
-    const int r = i / nab, c = i - r * nab;
-    const double v = out[i] + out[c * nab + r];
-    s2 = fma(v, v, s2);
-  }
-  for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-  if (lane == 0) red[warp] = s2;
-  __syncthreads();
-  if (tid == 0) {
-    double tot = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
-    Qab[pair] = sqrt(sqrt(tot));
-  }
-}
-
-// Schwarz values of low-L pairs (Lab <= kSwLab), one warp per pair, with warp
-// barriers instead of block barriers (most pairs of a basis are low-L, and for
-// them the block version mostly waits at its barriers). Same unordered unit
-// pairs and A + A^T as k_schwarz_bra, with the products reassociated: R is
-// built for the displacement Q - P (R~ = (-1)^|tau| R), so that
-// H[t][t'] = (-1)^|t| R~[t + t'] carries the sign on the output row, and
-//   Z_i = sum_(k>=i) w_ik H_ik E_ku^T   (NH x nab, w_ii = 1/2)
-//   A  += E_iu Z_i                       (once per iu, not per unit pair).
-// Launches per group of L_ab classes, each warp's scratch sized for the
+// Low-L pairs, one warp per pair, with warp barriers instead of block
+// barriers (most pairs of a basis are low-L, and for them a block mostly waits
+// at its barriers). Launches per group of L_ab classes, each warp's scratch sized for the
 // group's largest class (sw_nr R entries, sw_nh x sw_nab Z, sw_nab^2 A, stride
 // sw_stride doubles), so low-L classes keep many more warps resident.
 constexpr int kSwLab = 4;
@@ -546,6 +448,120 @@ __global__ void __launch_bounds__(32 * kSwWarps) k_schwarz_bra_dmma(
   if (lane == 0) Qab[pair] = sqrt(sqrt(s2));
 }
 
+// High-L pairs (L_ab = LAB >= 5), one block of kSbWarps warps per pair. Each
+// warp takes whole 8 x 8 tiles (the K reduction in two registers, so many
+// blocks stay resident): the tiles of H_ik E_ku^T are added into Z_i in shared
+// memory after every unit pair, the tiles of E_iu Z_i into A once per bra unit.
+constexpr int kSbWarps = 8;
+
+template <int LAB>
+struct SwBlk {
+  static constexpr int NH = ncum(LAB);
+  static constexpr int NR = ncum(2 * LAB);
+  static constexpr int NABM = sw_nab_max(LAB);
+  static constexpr int MT = (NH + 7) / 8;
+  static constexpr int KT = (NH + 3) / 4;
+  // Rn, R0, R1, Z_i [NH][nab], A [nab][nab]
+  static constexpr int SMEM = 32 + 2 * NR + NH * NABM + NABM * NABM;
+};
+
+template <int LAB>
+__global__ void __launch_bounds__(32 * kSbWarps) k_schwarz_bra(DevBasis B, const int2* __restrict__ pair_ab,
+                                                            const int* __restrict__ pair_unit0,
+                                                            const int* __restrict__ pair_list, UnitArrays U,
+                                                            int npairs, DeviceTables dt, int boys_mode,
+                                                            double* __restrict__ Qab) {
+  using C = SwBlk<LAB>;
+  constexpr int NH = C::NH, KT = C::KT, MT = C::MT;
+  extern __shared__ double smem[];
+  __shared__ double red[kSbWarps];
+  if (static_cast<int>(blockIdx.x) >= npairs) return;
+  const int pair = pair_list[blockIdx.x];
+  const int2 ab = pair_ab[pair];
+  const int4 sa = B.shell[ab.x], sb = B.shell[ab.y];
+  const int nab = (2 * sa.x + 1) * (2 * sb.x + 1);
+  const int ntr = (nab + 7) / 8;  // column tiles in use
+  double* Rn = smem;
+  double* R0 = Rn + 32;
+  double* R1 = R0 + C::NR;
+  double* Zs = R1 + C::NR;        // Z_i [NH][nab]
+  double* out = Zs + NH * C::NABM;  // A [nab][nab]
+  const IndexTables* it = dt.idx;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
+  for (int i = tid; i < nab * nab; i += blockDim.x) out[i] = 0.0;
+  const int u0 = pair_unit0[pair];
+  const int nu = sa.y * sb.y;
+  for (int iu = 0; iu < nu; ++iu) {
+    const double4 P = U.unit_pP[u0 + iu];
+    for (int ku = iu; ku < nu; ++ku) {
+      const double4 Q = U.unit_pP[u0 + ku];
+      const double p = P.x, q = Q.x, pq = p + q, alpha = p * q / pq;
+      const double X = Q.y - P.y, Yd = Q.z - P.z, Z = Q.w - P.w;
+      const double T = alpha * (X * X + Yd * Yd + Z * Z);
+      const double pref = kTwoPi52 / (p * q * sqrt(pq));
+      const double w = ku == iu ? 0.5 : 1.0;
+      __syncthreads();  // previous readers of Rn / R / Zs are done
+      if (tid <= 2 * LAB) {
+        double f = pref;
+        for (int k = 0; k < tid; ++k) f *= -2.0 * alpha;
+        Rn[tid] = f * boys_n(dt, boys_mode, tid, T);
+      }
+      __syncthreads();
+      hermite_R(dt.rdesc, 2 * LAB, Rn, X, Yd, Z, R0, R1, tid, blockDim.x, BlockSync());
+      const double* Ek = U.esph + U.unit_esph[u0 + ku];
+      for (int tile = warp; tile < MT * ntr; tile += kSbWarps) {
+        const int mt = tile / ntr, nt = tile - mt * ntr;
+        const int t = 8 * mt + g, c = 8 * nt + g;
+        double z0 = 0.0, z1 = 0.0;
+        for (int k4 = 0; k4 < KT; ++k4) {
+          const int tp = 4 * k4 + t4;
+          const double a = (t < NH && tp < NH) ? R0[__ldg(dt.sum_idx + t * kNSum + tp)] : 0.0;
+          const double b = (tp < NH && c < nab) ? Ek[c * NH + tp] : 0.0;
+          sw_dmma(z0, z1, a, b);
+        }
+        const int tr = 8 * mt + g, cc = 8 * nt + 2 * t4;
+        if (tr < NH) {
+          const double ws = (it->xyz[tr][3] & 1) ? -w : w;  // (-1)^|t| of H = (-1)^|t| R~
+          double* zr = Zs + tr * nab;
+          if (cc < nab) zr[cc] = ku == iu ? ws * z0 : fma(ws, z0, zr[cc]);
+          if (cc + 1 < nab) zr[cc + 1] = ku == iu ? ws * z1 : fma(ws, z1, zr[cc + 1]);
+        }
+      }
+    }
+    __syncthreads();  // Z_i complete
+    const double* Ei = U.esph + U.unit_esph[u0 + iu];
+    for (int tile = warp; tile < ntr * ntr; tile += kSbWarps) {
+      const int mt = tile / ntr, nt = tile - mt * ntr;
+      const int r = 8 * mt + g, c = 8 * nt + g;
+      double o0 = 0.0, o1 = 0.0;
+      for (int k4 = 0; k4 < KT; ++k4) {
+        const int t = 4 * k4 + t4;
+        const double a = (r < nab && t < NH) ? Ei[r * NH + t] : 0.0;
+        const double b = (t < NH && c < nab) ? Zs[t * nab + c] : 0.0;
+        sw_dmma(o0, o1, a, b);
+      }
+      const int cc = 8 * nt + 2 * t4;
+      if (r < nab && cc < nab) out[r * nab + cc] += o0;
+      if (r < nab && cc + 1 < nab) out[r * nab + cc + 1] += o1;
+    }
+  }
+  __syncthreads();
+  double s2 = 0.0;
+  for (int i = tid; i < nab * nab; i += blockDim.x) {
+    const int r = i / nab, c = i - r * nab;
+    const double v = out[i] + out[c * nab + r];
+    s2 = fma(v, v, s2);
+  }
+  for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+  if (lane == 0) red[warp] = s2;
+  __syncthreads();
+  if (tid == 0) {
+    double tot = 0.0;
+    for (int w = 0; w < kSbWarps; ++w) tot += red[w];
+    Qab[pair] = sqrt(sqrt(tot));
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Two-center block (P|Q)[mP][mQ] of two auxiliary shells, computed by one warp.
 // Scratch (per warp): Rn[16], R0/R1[ncum(lP+lQ)], Y[nsP * ncart(lQ)], out[nsP * nsQ].
@@ -746,18 +762,13 @@ int launch_unit_setup(const DevBasis& B, const int2* pair_ab, const int* class_u
   return launches;
 }
 
-// Shared memory of k_schwarz_bra for the pairs of class Lab = lab.
-size_t schwarz_bra_smem(int lab) {
-  size_t best = 0;
-  for (int la = 0; la <= PA_LMAX; ++la)
-    for (int lb = 0; lb <= la; ++lb) {
-      if (la + lb != lab) continue;
-      const int nab = (2 * la + 1) * (2 * lb + 1), NH = ncum(la + lb), NR = ncum(2 * (la + lb));
-      const int MT = (nab + 7) / 8, NT = (NH + 7) / 8;
-      const size_t d = 32 + 2 * NR + static_cast<size_t>(MT) * 8 * (NT * 8 + 1) + nab * nab;
-      best = best > d ? best : d;
-    }
-  return sizeof(double) * best;
+template <int LAB>
+int launch_schwarz_blk(const DevBasis& B, const int2* pair_ab, const int* pair_unit0, const int* pairs,
+                       UnitArrays U, int n, const DeviceTables& dt, int boys_mode, double* Qab, cudaStream_t s) {
+  const size_t smem = sizeof(double) * SwBlk<LAB>::SMEM;
+  cudaFuncSetAttribute(k_schwarz_bra<LAB>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  k_schwarz_bra<LAB><<<n, 32 * kSbWarps, smem, s>>>(B, pair_ab, pair_unit0, pairs, U, n, dt, boys_mode, Qab);
+  return 1;
 }
 
 template <int LAB>
@@ -807,15 +818,18 @@ int launch_schwarz_bra(const DevBasis& B, const int2* pair_ab, const int* pair_u
       ++launches;
     }
   }
-  // one launch per higher class, each with its own shared-memory footprint
-  cudaFuncSetAttribute(k_schwarz_bra, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       static_cast<int>(schwarz_bra_smem(2 * PA_LMAX)));
+  // one block per pair for the higher classes, one launch per class
   for (int lab = split; lab <= P.lab_max; ++lab) {
     const int off = P.pair_class_off[lab], n = P.pair_class_off[lab + 1] - off;
     if (n <= 0) continue;
-    k_schwarz_bra<<<n, 256, schwarz_bra_smem(lab), s>>>(B, pair_ab, pair_unit0, class_pair + off, U, n, dt,
-                                                        boys_mode, Qab);
-    ++launches;
+    const int* pl = class_pair + off;
+    switch (lab) {
+      case 5: launches += launch_schwarz_blk<5>(B, pair_ab, pair_unit0, pl, U, n, dt, boys_mode, Qab, s); break;
+      case 6: launches += launch_schwarz_blk<6>(B, pair_ab, pair_unit0, pl, U, n, dt, boys_mode, Qab, s); break;
+      case 7: launches += launch_schwarz_blk<7>(B, pair_ab, pair_unit0, pl, U, n, dt, boys_mode, Qab, s); break;
+      case 8: launches += launch_schwarz_blk<8>(B, pair_ab, pair_unit0, pl, U, n, dt, boys_mode, Qab, s); break;
+      default: break;
+    }
   }
   return launches;
 }
