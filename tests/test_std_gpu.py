@@ -19,7 +19,7 @@ import pytest
 import oracle
 from pysisyphus_addons import _native as nat
 from pysisyphus_addons.common.shells import Shell, Shells
-from pysisyphus_addons.common.synthetic import config_workload
+from pysisyphus_addons.common.synthetic import config_workload, make_workload
 from pysisyphus_addons.std import intor as std
 
 pytestmark = pytest.mark.gpu
@@ -103,6 +103,37 @@ def test_df2c_mo_reconstructs_df1c_pairs(w1, raw):
         row = X[k * (k + 1) // 2 + k]
         big = np.abs(T[mu]) > 1e-8
         np.testing.assert_allclose(row[big], T[mu][big], rtol=1e-12)
+
+
+@pytest.fixture(scope="module")
+def w4():
+    """Orbital g and auxiliary h shells: 3 atoms, lmax 4 / 5 (metric condition
+    number ~3.6e9)."""
+    return make_workload(natoms=3, lmax=4, lauxmax=5, nstates=3, seed=1)
+
+
+# df2c_mo raw differences measured on a B200 (of the largest element): up to
+# 4.2e-12 with the reference's Boys interpolation, 1.3e-13 with exact Boys;
+# the bounds are about 7x those.
+DF2C_LMAX4 = {"reference": 3e-11, "exact": 1e-12}
+
+
+def test_std_raw_lmax4(w4, mode, raw):
+    """df1c and eri2c agreed to 1.6e-15 of their maximum on a B200."""
+    close(std.int_df1c(w4.shells, w4.shells_aux), oracle.int_df1c(w4.shells, w4.shells_aux), 1e-13)
+    close(std.int_eri2c(w4.shells, w4.shells_aux), oracle.int_eri2c(w4.shells, w4.shells_aux), 1e-13)
+    for ncol in (12, 90):  # 90: all MOs, two chunks of the half-transformation kernel
+        C = w4.mo_coeffs[:, :ncol]
+        X = std.int_df2c_mo(w4.shells, w4.shells_aux, C)
+        close(X, oracle.int_df2c_mo(w4.shells, w4.shells_aux, C), DF2C_LMAX4[mode])
+
+
+def test_std_full_lmax4(w4, mode):
+    """With L^-T: conditioning-bound, 4.2e-9 (df1c) and 2.8e-9 (df2c_mo) of the
+    largest element measured on a B200."""
+    close(std.int_df1c(w4.shells, w4.shells_aux), oracle.int_df1c(w4.shells, w4.shells_aux), 3e-8)
+    C = w4.mo_coeffs[:, :12]
+    close(std.int_df2c_mo(w4.shells, w4.shells_aux, C), oracle.int_df2c_mo(w4.shells, w4.shells_aux, C), 3e-8)
 
 
 def test_std_errors():
