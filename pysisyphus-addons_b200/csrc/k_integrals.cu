@@ -1,8 +1,10 @@
 // Integral kernels of the density-fitting path (McMurchie-Davidson, FP64):
-//  * k_unit_setup   per primitive pair of an orbital shell pair ("bra unit"):
-//                   Gaussian-product data and the spherical Hermite expansion
-//                   E_sph[(ma,mb)][tuv] (contraction coefficients folded in);
-//  * k_schwarz_bra  sqrt(||(ab|ab)||_F) per shell pair
+//  * k_unit_setup_warp / k_unit_setup   per primitive pair of an orbital shell
+//                   pair ("bra unit"): Gaussian-product data and the spherical
+//                   Hermite expansion E_sph[(ma,mb)][tuv] (contraction
+//                   coefficients folded in);
+//  * k_schwarz_bra_warp / k_schwarz_bra_dmma<LAB> / k_schwarz_bra<LAB>
+//                   sqrt(||(ab|ab)||_F) per shell pair
 //                   (common/integrals/intor.f90:131-160);
 //  * k_schwarz_aux  sqrt(||(c|c)||_F) per auxiliary shell (intor.f90:97-129);
 //  * k_metric       the symmetric (P|Q) matrix (intor.f90:40-95);
