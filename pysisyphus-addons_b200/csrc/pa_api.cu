@@ -570,6 +570,7 @@ size_t cub_temp_bytes(const pa_basis_s* orb, const pa_basis_s* aux) {
 // radix sort, but every pass runs on all SMs (a segmented sort gives each
 // segment one block, and there are only a handful of classes). Writes the
 // sorted keys and ids[position] of the entries.
+static_assert(2 * PA_LMAX + 1 <= 256, "class ids of the sort are unsigned char");
 int class_sort_desc(DfBuffers& b, const double* keys, const int* positions, const int* ids,
                     const int* d_off, int nseg, int n, double* keys_out, int* ids_out, cudaStream_t s) {
   if (n <= 0) return 0;
