@@ -207,3 +207,27 @@ def test_oracle_qvl_screening_cfg1():
     assert st_q["nskipped"] != st_s["nskipped"]
     diff = np.abs(got - ref).max()
     assert 0.0 < diff < 1e-9 * np.abs(ref).max()
+
+
+def test_oracle_schwarz_f_g_shells_high_precision():
+    """Oracle Schwarz values of same-center pairs with f and g shells (f-d and
+    g-p, L_ab 5) against 30-digit McMurchie-Davidson values (tests/md_ref.py):
+    the reference's golden vectors stop at d functions. On pairs of a tight g
+    shell with a shell on another atom the oracle's horizontal recurrence loses
+    up to 7.4e-4 relative; the device is pinned there by test_lmax4_gpu.py."""
+    from md_ref import schwarz_pair_mp
+    from pysisyphus_addons.common.synthetic import make_workload
+
+    w = make_workload(natoms=3, lmax=4, lauxmax=5, nstates=3, seed=1)
+    oracle.set_boys_mode("exact")
+    try:
+        q = oracle.int_schwarz_bra(w.shells)
+    finally:
+        oracle.set_boys_mode("reference")
+    ia, ib = np.tril_indices(len(w.shells))
+    index = {(int(a), int(b)): k for k, (a, b) in enumerate(zip(ia, ib))}
+    for a, b, L in ((6, 5, (3, 2)), (7, 3, (4, 1)), (14, 13, (3, 2))):
+        sa, sb = w.shells[a], w.shells[b]
+        assert (sa.L, sb.L) == L and sa.center_ind == sb.center_ind
+        ref = float(schwarz_pair_mp(sa, sb, dps=30))
+        assert abs(q[index[(a, b)]] - ref) <= 1e-13 * ref, ((a, b), q[index[(a, b)]], ref)
