@@ -572,7 +572,46 @@ std::vector<double> schwarz_aux(const OBasis& B) {
 
 // intor_schwarz_bra (common/integrals/intor.f90:131-160): sqrt(||(ab|ab)||_F)
 // at packed index a(a-1)/2 + b (1-based), b <= a.
+// Fingerprint of a basis (every shell's L, center, exponents and
+// coefficients), the key of the bra Schwarz cache.
+std::vector<double> basis_key(const OBasis& B) {
+  std::vector<double> k;
+  for (const OShell& s : B.shells) {
+    k.push_back(s.L);
+    k.push_back(s.nprim);
+    k.insert(k.end(), s.A, s.A + 3);
+    k.insert(k.end(), s.exps.begin(), s.exps.end());
+    k.insert(k.end(), s.coefs.begin(), s.coefs.end());
+  }
+  return k;
+}
+
+// With g_reuse_screening, the bra Schwarz vector of the last orbital basis is
+// kept and reused while the basis stays the same (a timing aid: the CPU
+// baseline times the three-center work of a sample of auxiliary shells, and
+// the O(npairs) screening pass, once per tensor, would dominate a small
+// sample). Off by default.
+int g_reuse_screening = 0;
+std::mutex g_sbra_mu;
+std::vector<double> g_sbra_key, g_sbra_val;
+
+std::vector<double> schwarz_bra_compute(const OBasis& B);
+
 std::vector<double> schwarz_bra(const OBasis& B) {
+  if (!g_reuse_screening) return schwarz_bra_compute(B);
+  std::vector<double> key = basis_key(B);
+  {
+    std::lock_guard<std::mutex> lk(g_sbra_mu);
+    if (key == g_sbra_key) return g_sbra_val;
+  }
+  std::vector<double> v = schwarz_bra_compute(B);
+  std::lock_guard<std::mutex> lk(g_sbra_mu);
+  g_sbra_key = std::move(key);
+  g_sbra_val = v;
+  return v;
+}
+
+std::vector<double> schwarz_bra_compute(const OBasis& B) {
   const int n = static_cast<int>(B.shells.size());
   std::vector<double> out(static_cast<size_t>(n) * (n + 1) / 2);
 #pragma omp parallel
@@ -1039,6 +1078,7 @@ int oracle_get_boys_mode(void) { return g_boys_mode; }
 void oracle_set_skip_metric(int skip) { g_skip_metric = skip ? 1 : 0; }
 void oracle_set_metric_shift(double shift) { g_metric_shift = shift; }
 void oracle_set_screening(int mode) { g_screening = mode ? 1 : 0; }
+void oracle_set_reuse_screening(int reuse) { g_reuse_screening = reuse ? 1 : 0; }
 void oracle_set_threads(int nthreads) {
   if (nthreads > 0) omp_set_num_threads(nthreads);
 }
@@ -1192,5 +1232,86 @@ void oracle_intor_df2c_mo(int nshells, int, const int* bc, const int* bs, const 
 }
 
 void oracle_last_stats(OracleStats* out) { *out = g_stats; }
+
+// Extended-precision factor and solve (x87 long double: 64-bit significand,
+// unit roundoff 5.4e-20, against 1.1e-16 in double). Not part of the
+// reference: a checker for FP64 factorizations of ill-conditioned metrics.
+// M is n x n column-major (lower triangle read), B is n x nrhs column-major.
+// L = chol(M) and Y = L^-1 B are formed in long double; Y (and, when L_out is
+// given, L, rounded, upper triangle zero) are returned in double.
+// Returns 0, or the 1-based column of the first non-positive pivot.
+int oracle_chol_solve_ld(int n, const double* M, int nrhs, const double* B, double* Y,
+                         double* L_out) {
+  typedef long double ld;
+  std::vector<ld> L(static_cast<size_t>(n) * n, 0.0L);  // row-major: L[i * n + k]
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k <= i; ++k) L[static_cast<size_t>(i) * n + k] = M[i + static_cast<size_t>(k) * n];
+  int info = 0;
+  for (int j = 0; j < n && info == 0; ++j) {
+    ld* Lj = L.data() + static_cast<size_t>(j) * n;
+    ld d = Lj[j];
+    for (int k = 0; k < j; ++k) d -= Lj[k] * Lj[k];
+    if (!(d > 0.0L)) {
+      info = j + 1;
+      break;
+    }
+    d = std::sqrt(d);
+    Lj[j] = d;
+#pragma omp parallel for schedule(static)
+    for (int i = j + 1; i < n; ++i) {
+      ld* Li = L.data() + static_cast<size_t>(i) * n;
+      ld s = Li[j];
+      for (int k = 0; k < j; ++k) s -= Li[k] * Lj[k];
+      Li[j] = s / d;
+    }
+  }
+  if (info) return info;
+#pragma omp parallel
+  {
+    std::vector<ld> y(n);
+#pragma omp for schedule(static)
+    for (int r = 0; r < nrhs; ++r) {
+      for (int i = 0; i < n; ++i) {
+        const ld* Li = L.data() + static_cast<size_t>(i) * n;
+        ld s = B[i + static_cast<size_t>(n) * r];
+        for (int k = 0; k < i; ++k) s -= Li[k] * y[k];
+        y[i] = s / Li[i];
+      }
+      for (int i = 0; i < n; ++i) Y[i + static_cast<size_t>(n) * r] = static_cast<double>(y[i]);
+    }
+  }
+  if (L_out)
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i)
+        L_out[i + static_cast<size_t>(n) * j] =
+            i >= j ? static_cast<double>(L[static_cast<size_t>(i) * n + j]) : 0.0;
+  return 0;
+}
+
+// ||L L^T - M||_F / ||M||_F in long double, for L the lower triangle of the
+// column-major n x n array Lc (its upper triangle is ignored): the backward
+// error of a Cholesky factor.
+double oracle_chol_backward_error_ld(int n, const double* M, const double* Lc) {
+  typedef long double ld;
+  std::vector<ld> L(static_cast<size_t>(n) * n, 0.0L);  // row-major lower
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k <= i; ++k) L[static_cast<size_t>(i) * n + k] = Lc[i + static_cast<size_t>(k) * n];
+  ld num = 0.0L, den = 0.0L;
+#pragma omp parallel for schedule(dynamic) reduction(+ : num, den)
+  for (int i = 0; i < n; ++i) {
+    const ld* Li = L.data() + static_cast<size_t>(i) * n;
+    for (int j = 0; j <= i; ++j) {
+      const ld* Lj = L.data() + static_cast<size_t>(j) * n;
+      ld s = 0.0L;
+      for (int k = 0; k <= j; ++k) s += Li[k] * Lj[k];
+      const ld m = M[i + static_cast<size_t>(j) * n];
+      const ld w = i == j ? 1.0L : 2.0L;  // symmetric: count the mirrored entry
+      num += w * (s - m) * (s - m);
+      den += w * m * m;
+    }
+  }
+  return static_cast<double>(std::sqrt(num / den));
+}
+
 
 }  // extern "C"

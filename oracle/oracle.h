@@ -36,6 +36,9 @@ void oracle_set_skip_metric(int skip);
 void oracle_set_metric_shift(double shift);
 // 0: schwarz_estimate (default), 1: qvl_estimate in the Coulomb contraction.
 void oracle_set_screening(int mode);
+/* 1: keep the bra Schwarz vector of the last orbital basis and reuse it while
+ * the basis is unchanged (timing aid for sampled CPU baselines; default 0). */
+void oracle_set_reuse_screening(int reuse);
 int oracle_get_threads(void);
 /* Optional BLAS/LAPACK (Fortran calling convention) used by inv_chol / dtrmm /
  * dgemm, exactly as the reference calls them; naive loops when unset. */
@@ -96,6 +99,14 @@ typedef struct {
   double t_screener, t_metric, t_chol, t_3c, t_trmm, t_total;
 } OracleStats;
 void oracle_last_stats(OracleStats* out);
+
+/* Extended-precision (long double) Cholesky factor of M and Y = L^-1 B, for
+ * checking FP64 solves of ill-conditioned metrics. Returns 0 or the 1-based
+ * column of the first non-positive pivot; L_out may be NULL. */
+int oracle_chol_solve_ld(int n, const double* M, int nrhs, const double* B, double* Y,
+                         double* L_out);
+/* ||L L^T - M||_F / ||M||_F in long double (L: lower triangle of Lc). */
+double oracle_chol_backward_error_ld(int n, const double* M, const double* Lc);
 
 #ifdef __cplusplus
 }

@@ -86,9 +86,14 @@ def lib():
     L.oracle_set_skip_metric.argtypes = [_i]
     L.oracle_set_metric_shift.argtypes = [_d]
     L.oracle_set_screening.argtypes = [_i]
+    L.oracle_set_reuse_screening.argtypes = [_i]
     L.oracle_get_threads.restype = _i
     L.oracle_register_lapack.argtypes = [ctypes.c_void_p] * 4
     L.oracle_last_stats.argtypes = [ctypes.POINTER(OracleStats)]
+    L.oracle_chol_solve_ld.argtypes = [_i, _pd, _i, _pd, _pd, _pd]
+    L.oracle_chol_solve_ld.restype = _i
+    L.oracle_chol_backward_error_ld.argtypes = [_i, _pd, _pd]
+    L.oracle_chol_backward_error_ld.restype = _d
     if os.environ.get("PA_ORACLE_NO_LAPACK", "0") != "1":
         try:
             from scipy.linalg import cython_blas, cython_lapack
@@ -139,6 +144,12 @@ def set_screening(mode):
     """'schwarz' (default) or 'qvl': the triplet estimate of the Coulomb
     contraction (diabatization/intor.f90:137-138)."""
     lib().oracle_set_screening({"schwarz": 0, "qvl": 1}[mode])
+
+
+def set_reuse_screening(reuse):
+    """Keep the bra Schwarz vector of the last orbital basis for later calls
+    with the same basis (timing aid for sampled baselines)."""
+    lib().oracle_set_reuse_screening(int(bool(reuse)))
 
 
 def set_threads(n):
@@ -279,3 +290,43 @@ def int_df2c_mo(shells, shells_aux, mo_tensor):
     lib().oracle_intor_df2c_mo(*b1, *b2, nbf, nmos, _p(C, ctypes.c_double), naux,
                                _p(out, ctypes.c_double))
     return out
+
+
+def chol_solve_ld(M, B, want_L=False):
+    """Y = L^-1 B with L = chol(M), factor and solve in long double (64-bit
+    significand), rounded to double. Checker for FP64 solves of
+    ill-conditioned metrics; returns Y (and L with want_L)."""
+    M = np.asfortranarray(M, dtype=np.float64)
+    n = M.shape[0]
+    B2 = np.asfortranarray(np.asarray(B, dtype=np.float64).reshape(n, -1))
+    Y = np.zeros_like(B2, order="F")
+    L = np.zeros((n, n), order="F") if want_L else None
+    rc = lib().oracle_chol_solve_ld(n, _p(M, ctypes.c_double), B2.shape[1], _p(B2, ctypes.c_double),
+                                    _p(Y, ctypes.c_double), _p(L, ctypes.c_double) if want_L else None)
+    if rc:
+        raise np.linalg.LinAlgError(f"long-double Cholesky: non-positive pivot in column {rc}")
+    Y = Y.reshape(np.shape(B))
+    return (Y, L) if want_L else Y
+
+
+def chol_backward_error_ld(M, L):
+    """||L L^T - M||_F / ||M||_F in long double (lower triangle of L)."""
+    M = np.asfortranarray(M, dtype=np.float64)
+    L = np.asfortranarray(L, dtype=np.float64)
+    return lib().oracle_chol_backward_error_ld(M.shape[0], _p(M, ctypes.c_double), _p(L, ctypes.c_double))
+
+
+def coulomb_from_df(df, nstates):
+    """The Coulomb tensor R[i,j,k,l] = sum_m B[m,(ij)] B[m,(kl)] of a df matrix
+    (naux x ndens, pairs i >= j in the order of diabatization/intor.f90:241-269)."""
+    df = np.asarray(df)
+    G = df.T @ df
+    R = np.zeros((nstates,) * 4)
+    pairs = [(i, j) for i in range(nstates) for j in range(i + 1)]
+    for p, (i, j) in enumerate(pairs):
+        for q, (k, l) in enumerate(pairs):
+            v = G[p, q]
+            for a, b in ((i, j), (j, i)):
+                for c, d in ((k, l), (l, k)):
+                    R[a, b, c, d] = v
+    return R

@@ -231,3 +231,59 @@ def test_oracle_schwarz_f_g_shells_high_precision():
         assert (sa.L, sb.L) == L and sa.center_ind == sb.center_ind
         ref = float(schwarz_pair_mp(sa, sb, dps=30))
         assert abs(q[index[(a, b)]] - ref) <= 1e-13 * ref, ((a, b), q[index[(a, b)]], ref)
+
+
+def test_long_double_solve_against_mpmath():
+    """The extended-precision factor + solve used to check FP64 solves of
+    ill-conditioned metrics: a Hilbert matrix (condition number ~1e13 at n 10)
+    against 50-digit arithmetic. The long-double solve's error is ~1e4x below
+    the FP64 LAPACK solve's (the ratio of the unit roundoffs is 4.9e-4)."""
+    import mpmath
+    import scipy.linalg as sl
+
+    n = 10
+    H = np.array([[1.0 / (i + j + 1) for j in range(n)] for i in range(n)])
+    b = np.arange(1.0, n + 1.0)
+    Y, L = oracle.chol_solve_ld(H, b[:, None], want_L=True)
+    mpmath.mp.dps = 50
+    Lm = mpmath.cholesky(mpmath.matrix(H.tolist()))
+    ym = mpmath.lu_solve(Lm, mpmath.matrix(b.tolist()))
+    y_ref = np.array([float(v) for v in ym])
+    err_ld = np.abs(Y[:, 0] - y_ref).max()
+    err_lp = np.abs(sl.solve_triangular(np.linalg.cholesky(H), b, lower=True) - y_ref).max()
+    assert err_ld <= 2e-3 * err_lp, (err_ld, err_lp)
+    assert oracle.chol_backward_error_ld(H, L) < 1e-16
+    assert oracle.chol_backward_error_ld(H, np.linalg.cholesky(H)) < 1e-15
+    with pytest.raises(np.linalg.LinAlgError):
+        oracle.chol_solve_ld(np.diag([1.0, -1.0]), np.ones((2, 1)))
+
+
+def test_coulomb_from_df_matches_driver():
+    from pysisyphus_addons.common.synthetic import config_workload
+
+    w = config_workload("cfg1")
+    oracle.set_boys_mode("reference")
+    df = oracle.contract_coulomb_densities_2d(w.shells, w.shells_aux, w.densities)
+    R = oracle.contract_coulomb_densities_4d(w.shells, w.shells_aux, w.densities)
+    np.testing.assert_allclose(oracle.coulomb_from_df(df, w.nstates), R, rtol=0, atol=1e-12 * np.abs(R).max())
+
+
+def test_reused_screening_gives_the_same_result():
+    from pysisyphus_addons.common.shells import Shells
+    from pysisyphus_addons.common.synthetic import config_workload
+
+    w = config_workload("cfg1")
+    oracle.set_boys_mode("reference")
+    a = oracle.contract_coulomb_densities_2d(w.shells, w.shells_aux, w.densities)
+    oracle.set_reuse_screening(1)
+    try:
+        b = oracle.contract_coulomb_densities_2d(w.shells, w.shells_aux, w.densities)
+        c = oracle.contract_coulomb_densities_2d(w.shells, w.shells_aux, w.densities)  # from the cache
+        sub = Shells(w.shells[:-1])  # another basis: recomputed, not taken from the cache
+        d = oracle.contract_coulomb_densities_2d(sub, w.shells_aux, w.densities[:, :sub.sph_size, :sub.sph_size])
+    finally:
+        oracle.set_reuse_screening(0)
+    e = oracle.contract_coulomb_densities_2d(sub, w.shells_aux, w.densities[:, :sub.sph_size, :sub.sph_size])
+    np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(a, c)
+    np.testing.assert_array_equal(d, e)
