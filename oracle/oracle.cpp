@@ -1066,6 +1066,193 @@ double rational(double x, double base0, const double* P, const double* Q, int n)
   return x * num / den;
 }
 
+// ---------------------------------------------------------------------------
+// Grid densities (grid/grid.f90) and GDMA primitive densities
+// (gdma/prim_dens.f90). Cartesian functions in pysisyphus order (x^L, x^(L-1) y,
+// x^(L-1) z, ..., z^L), each scaled by 1/sqrt((2i-1)!! (2j-1)!! (2k-1)!!) --
+// the NORM2 / NORM3 / NORM4 / NORM22 constants of grid.f90:9-13.
+
+constexpr double GRID_CUTOFF = -36.0;  // grid.f90:9, prim_dens.f90:13
+
+double cart_norm(int i, int j, int k) {
+  auto df = [](int n) {  // (2n - 1)!!
+    double r = 1.0;
+    for (int m = 2 * n - 1; m > 1; m -= 2) r *= m;
+    return r;
+  };
+  return 1.0 / std::sqrt(df(i) * df(j) * df(k));
+}
+
+// Powers (i, j, k) of Cartesian component c of degree L in pysisyphus order.
+void cart_powers(int L, int c, int* i, int* j, int* k) {
+  int idx = 0;
+  for (int a = L; a >= 0; --a)
+    for (int b = L - a; b >= 0; --b) {
+      if (idx == c) {
+        *i = a;
+        *j = b;
+        *k = L - a - b;
+        return;
+      }
+      ++idx;
+    }
+}
+
+double ipow(double x, int n) {
+  double r = 1.0;
+  for (int m = 0; m < n; ++m) r *= x;
+  return r;
+}
+
+// cart_gto3d_rel (grid.f90:17-108): the Cartesian functions of one shell at
+// offset RA from its center; exp arguments below -36 are skipped.
+void cart_gto3d(const OShell& s, const double* RA, double* out) {
+  const int nc = (s.L + 1) * (s.L + 2) / 2;
+  for (int c = 0; c < nc; ++c) out[c] = 0.0;
+  const double dist = RA[0] * RA[0] + RA[1] * RA[1] + RA[2] * RA[2];
+  for (int p = 0; p < s.nprim; ++p) {
+    const double arg = -s.exps[p] * dist;
+    if (arg < GRID_CUTOFF) continue;
+    const double e = s.coefs[p] * std::exp(arg);
+    for (int c = 0; c < nc; ++c) {
+      int i = 0, j = 0, k = 0;
+      cart_powers(s.L, c, &i, &j, &k);
+      out[c] += cart_norm(i, j, k) * ipow(RA[0], i) * ipow(RA[1], j) * ipow(RA[2], k) * e;
+    }
+  }
+}
+
+// eval_densities (grid.f90:110-286): blocks of blk_size points; per block the
+// Cartesian functions, their mean |values| over the block, then every pair
+// nu <= mu whose estimate factor * D(j, mu, nu) * mean(nu) * mean(mu) reaches
+// thresh adds factor * D(j, mu, nu) chi(:, mu) chi(:, nu).
+void eval_densities(const OBasis& B, int npoints, const double* grid3d, int ndens, int nbfs,
+                    const double* D, double* rho, int blk_size, double thresh) {
+  std::vector<int> cart_off(B.shells.size() + 1, 0);
+  for (size_t a = 0; a < B.shells.size(); ++a)
+    cart_off[a + 1] = cart_off[a] + (B.shells[a].L + 1) * (B.shells[a].L + 2) / 2;
+  const int ncart = cart_off.back();
+  std::fill(rho, rho + static_cast<size_t>(ndens) * npoints, 0.0);
+  if (blk_size <= 0 || ncart != nbfs) return;
+  const int nblks = (npoints + blk_size - 1) / blk_size;
+#pragma omp parallel
+  {
+    std::vector<double> chis(static_cast<size_t>(blk_size) * ncart), mean(ncart);
+    std::vector<double> scratch(static_cast<size_t>(ndens) * blk_size * ncart);
+    std::vector<char> contributed(static_cast<size_t>(ndens) * ncart);
+#pragma omp for schedule(dynamic)
+    for (int blk = 0; blk < nblks; ++blk) {
+      const int start = blk * blk_size;
+      const int n = std::min(blk_size, npoints - start);
+      for (int i = 0; i < n; ++i) {
+        const double* R = grid3d + 3 * static_cast<size_t>(start + i);
+        for (size_t a = 0; a < B.shells.size(); ++a) {
+          const OShell& sh = B.shells[a];
+          const double RA[3] = {R[0] - sh.A[0], R[1] - sh.A[1], R[2] - sh.A[2]};
+          double v[15];
+          cart_gto3d(sh, RA, v);
+          for (int c = 0; c < cart_off[a + 1] - cart_off[a]; ++c)
+            chis[i + static_cast<size_t>(blk_size) * (cart_off[a] + c)] = v[c];
+        }
+      }
+      for (int nu = 0; nu < ncart; ++nu) {
+        double m = 0.0;
+        for (int i = 0; i < n; ++i) m += std::fabs(chis[i + static_cast<size_t>(blk_size) * nu]);
+        mean[nu] = m / n;
+      }
+      std::fill(scratch.begin(), scratch.end(), 0.0);
+      std::fill(contributed.begin(), contributed.end(), 0);
+      for (int nu = 0; nu < ncart; ++nu)
+        for (int mu = nu; mu < ncart; ++mu) {
+          const double f = nu == mu ? 1.0 : 2.0;
+          for (int j = 0; j < ndens; ++j) {
+            const double dnm = D[j + static_cast<size_t>(ndens) * (mu + static_cast<size_t>(nbfs) * nu)];
+            const double contrib = f * dnm * mean[nu] * mean[mu];
+            if (std::fabs(contrib) >= thresh) {
+              double* sc = &scratch[static_cast<size_t>(j) + static_cast<size_t>(ndens) * blk_size * nu];
+              const double* cm = &chis[static_cast<size_t>(blk_size) * mu];
+              for (int i = 0; i < n; ++i) sc[static_cast<size_t>(ndens) * i] += f * dnm * cm[i];
+              contributed[j + static_cast<size_t>(ndens) * nu] = 1;
+            }
+          }
+        }
+      for (int nu = 0; nu < ncart; ++nu)
+        for (int j = 0; j < ndens; ++j) {
+          if (!contributed[j + static_cast<size_t>(ndens) * nu]) continue;
+          for (int i = 0; i < n; ++i)
+            rho[j + static_cast<size_t>(ndens) * (start + i)] +=
+                scratch[j + static_cast<size_t>(ndens) * (i + static_cast<size_t>(blk_size) * nu)] *
+                chis[i + static_cast<size_t>(blk_size) * nu];
+        }
+    }
+  }
+}
+
+// f_eval_prim_density (gdma/prim_dens.f90:100-259). ls_inds(2, nprims) = (L,
+// 0-based Cartesian start index); primdata(5, nprims) = (coefficient,
+// exponent, x, y, z); P(nbfs, nbfs) column-major. Pairs ai <= bi with
+// ax + bx < switch; a pair is skipped when -mu * (sum_d (A_d - B_d))^2 <= -36
+// -- the reference squares the sum of the differences there
+// (prim_dens.f90:212), not the sum of their squares; its prefactor K uses the
+// squared distance. Cartesian prefactors as prefacts (:17-92) for L <= 3; for
+// L = 4 the 15 components of grid.f90's order (prefacts fills 14 of them and
+// leaves the 15th unset).
+void eval_prim_density(int nprims, int npoints, int nbfs, const int* ls_inds, const double* primdata,
+                       const double* coords3d, const double* P, double sw, double* rho) {
+  std::fill(rho, rho + npoints, 0.0);
+#pragma omp parallel
+  {
+    std::vector<double> loc(npoints, 0.0);
+    double pa[15], pb[15];
+#pragma omp for schedule(dynamic)
+    for (int ai = 0; ai < nprims; ++ai) {
+      const double da = primdata[5 * ai], ax = primdata[5 * ai + 1];
+      const double* A = primdata + 5 * ai + 2;
+      const int La = ls_inds[2 * ai], ia = ls_inds[2 * ai + 1];
+      const int na = (La + 1) * (La + 2) / 2;
+      for (int bi = ai; bi < nprims; ++bi) {
+        const double db = primdata[5 * bi], bx = primdata[5 * bi + 1];
+        if (ax + bx >= sw) continue;
+        const double* Bc = primdata + 5 * bi + 2;
+        const int Lb = ls_inds[2 * bi], ib = ls_inds[2 * bi + 1];
+        const int nb = (Lb + 1) * (Lb + 2) / 2;
+        const double px = ax + bx, mux = ax * bx / px;
+        const double dsum = (A[0] - Bc[0]) + (A[1] - Bc[1]) + (A[2] - Bc[2]);
+        if (-mux * dsum * dsum <= GRID_CUTOFF) continue;
+        const double AB2 = (A[0] - Bc[0]) * (A[0] - Bc[0]) + (A[1] - Bc[1]) * (A[1] - Bc[1]) +
+                           (A[2] - Bc[2]) * (A[2] - Bc[2]);
+        const double K = da * db * (ai == bi ? 1.0 : 2.0) * std::exp(-mux * AB2);
+        const double Pc[3] = {(ax * A[0] + bx * Bc[0]) / px, (ax * A[1] + bx * Bc[1]) / px,
+                              (ax * A[2] + bx * Bc[2]) / px};
+        for (int i = 0; i < npoints; ++i) {
+          const double* R = coords3d + 3 * static_cast<size_t>(i);
+          const double r2 = (R[0] - Pc[0]) * (R[0] - Pc[0]) + (R[1] - Pc[1]) * (R[1] - Pc[1]) +
+                            (R[2] - Pc[2]) * (R[2] - Pc[2]);
+          if (-px * r2 <= GRID_CUTOFF) continue;
+          const double Pexp = std::exp(-px * r2);
+          for (int c = 0; c < na; ++c) {
+            int x = 0, y = 0, z = 0;
+            cart_powers(La, c, &x, &y, &z);
+            pa[c] = cart_norm(x, y, z) * ipow(R[0] - A[0], x) * ipow(R[1] - A[1], y) * ipow(R[2] - A[2], z);
+          }
+          for (int c = 0; c < nb; ++c) {
+            int x = 0, y = 0, z = 0;
+            cart_powers(Lb, c, &x, &y, &z);
+            pb[c] = cart_norm(x, y, z) * ipow(R[0] - Bc[0], x) * ipow(R[1] - Bc[1], y) * ipow(R[2] - Bc[2], z);
+          }
+          double acc = 0.0;
+          for (int nu = 0; nu < na; ++nu)
+            for (int mu = 0; mu < nb; ++mu)
+              acc += K * Pexp * P[(ia + nu) + static_cast<size_t>(nbfs) * (ib + mu)] * pa[nu] * pb[mu];
+          loc[i] += acc;
+        }
+      }
+    }
+#pragma omp critical
+    for (int i = 0; i < npoints; ++i) rho[i] += loc[i];
+  }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -1232,6 +1419,18 @@ void oracle_intor_df2c_mo(int nshells, int, const int* bc, const int* bs, const 
 }
 
 void oracle_last_stats(OracleStats* out) { *out = g_stats; }
+
+void oracle_eval_densities(int nshells, int, const int* bc, const int* bs, const double* bd, int npoints,
+                           const double* grid3d, int ndens, int nbfs, const double* densities,
+                           double* grid_densities, int blk_size, double thresh) {
+  const OBasis B = make_basis(nshells, bc, bs, bd);
+  eval_densities(B, npoints, grid3d, ndens, nbfs, densities, grid_densities, blk_size, thresh);
+}
+
+void oracle_eval_prim_density(int nprims, int npoints, int nbfs, const int* ls_inds, const double* primdata,
+                              const double* coords3d, const double* P, double sw, double* rho) {
+  eval_prim_density(nprims, npoints, nbfs, ls_inds, primdata, coords3d, P, sw, rho);
+}
 
 // Extended-precision factor and solve (x87 long double: 64-bit significand,
 // unit roundoff 5.4e-20, against 1.1e-16 in double). Not part of the

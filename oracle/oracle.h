@@ -108,6 +108,16 @@ int oracle_chol_solve_ld(int n, const double* M, int nrhs, const double* B, doub
 /* ||L L^T - M||_F / ||M||_F in long double (L: lower triangle of Lc). */
 double oracle_chol_backward_error_ld(int n, const double* M, const double* Lc);
 
+/* Mirror of f_eval_densities (grid/grid_wrapper.f90:12-38): densities on grid
+ * points from Cartesian AO density matrices (ndens, nbfs, nbfs), column-major
+ * grid3d(3, npoints), output grid_densities(ndens, npoints). */
+void oracle_eval_densities(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
+                           const double* bas_data, int npoints, const double* grid3d, int ndens, int nbfs,
+                           const double* densities, double* grid_densities, int blk_size, double thresh);
+/* Mirror of f_eval_prim_density (gdma/prim_dens.f90:100-259). */
+void oracle_eval_prim_density(int nprims, int npoints, int nbfs, const int* ls_inds, const double* primdata,
+                              const double* coords3d, const double* P, double sw, double* rho);
+
 #ifdef __cplusplus
 }
 #endif

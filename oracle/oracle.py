@@ -94,6 +94,8 @@ def lib():
     L.oracle_chol_solve_ld.restype = _i
     L.oracle_chol_backward_error_ld.argtypes = [_i, _pd, _pd]
     L.oracle_chol_backward_error_ld.restype = _d
+    L.oracle_eval_densities.argtypes = basis + [_i, _pd, _i, _i, _pd, _pd, _i, _d]
+    L.oracle_eval_prim_density.argtypes = [_i, _i, _i, _pi, _pd, _pd, _pd, _d, _pd]
     if os.environ.get("PA_ORACLE_NO_LAPACK", "0") != "1":
         try:
             from scipy.linalg import cython_blas, cython_lapack
@@ -330,3 +332,34 @@ def coulomb_from_df(df, nstates):
                 for c, d in ((k, l), (l, k)):
                     R[a, b, c, d] = v
     return R
+
+
+def eval_densities(shells, grid3d, densities, blk_size=100, thresh=1e-8):
+    """Densities on grid points, (ndens, npoints) F-ordered, like
+    pysisyphus_addons.grid.grid.eval_densities (grid/_grid.pyx:35-75):
+    grid3d (npoints, 3), Cartesian AO densities (ndens, nbfs, nbfs)."""
+    k1, b1 = _basis_args(shells)
+    G = np.asfortranarray(np.asarray(grid3d, dtype=np.float64).T)
+    D = np.asfortranarray(densities, dtype=np.float64)
+    ndens, nbfs = D.shape[0], D.shape[1]
+    npoints = G.shape[1]
+    out = np.zeros((ndens, npoints), order="F")
+    lib().oracle_eval_densities(*b1, npoints, _p(G, ctypes.c_double), ndens, nbfs, _p(D, ctypes.c_double),
+                                _p(out, ctypes.c_double), int(blk_size), float(thresh))
+    return out
+
+
+def eval_prim_density(Ls_inds, prim_data, coords3d, P_tot_cart, switch, rho_pseudo):
+    """In-place like pysisyphus_addons.gdma.prim_dens.eval_prim_density
+    (gdma/prim_dens.pyx:26-50): Ls_inds (nprims, 2), prim_data (nprims, 5),
+    coords3d (npoints, 3), P_tot_cart (nbfs, nbfs)."""
+    Li = np.asfortranarray(np.asarray(Ls_inds, dtype=np.int32).T)
+    Pd = np.asfortranarray(np.asarray(prim_data, dtype=np.float64).T)
+    C = np.asfortranarray(np.asarray(coords3d, dtype=np.float64).T)
+    P = np.asfortranarray(P_tot_cart, dtype=np.float64)
+    rho = np.zeros(C.shape[1])
+    lib().oracle_eval_prim_density(Li.shape[1], C.shape[1], P.shape[0], _p(Li, ctypes.c_int), _p(Pd, ctypes.c_double),
+                                   _p(C, ctypes.c_double), _p(P, ctypes.c_double), float(switch),
+                                   _p(rho, ctypes.c_double))
+    rho_pseudo[:] = rho
+    return rho_pseudo
