@@ -5,6 +5,7 @@ implementations with different summation orders agree to a few ulp of the
 largest element, so tensors are compared at atol 1e-12 + 1e-13 * max|ref|
 (about 1e-11 on the ~345 golden diagonal)."""
 
+import ctypes
 import json
 
 import numpy as np
@@ -264,3 +265,44 @@ def test_metric_shift_matches_oracle():
     assert np.abs(plain - df).max() > 1e-9  # the shift is actually applied
     with pytest.raises(nat.PaError):
         nat.set_metric_shift(-1.0)
+
+
+def _reference_call(name, shells, shells_aux, densities, out_shape, last_int):
+    """Calls an f_* entry point the way the reference's Cython module does
+    (diabatization/_intor.pyx:55-113): F-ordered copies of the basis arrays
+    and the densities, len() of the centers and data arrays, a zeroed
+    F-ordered output."""
+    lib = nat.load()
+    bc, bs, bd = (np.asfortranarray(a) for a in shells.as_arrays(fortran=True))
+    bca, bsa, bda = (np.asfortranarray(a) for a in shells_aux.as_arrays(fortran=True))
+    bc, bs, bca, bsa = (np.asfortranarray(a, dtype=np.int32) for a in (bc, bs, bca, bsa))
+    D = np.asfortranarray(densities, dtype=np.float64)
+    ndens, nbfs = D.shape[0], D.shape[1]
+    out = np.zeros(out_shape, dtype=np.float64, order="F")
+    ip = lambda a: nat.ptr(a, ctypes.c_int)  # noqa: E731
+    rc = getattr(lib, name)(len(bc), len(bd), ip(bc), ip(bs), nat.ptr(bd),
+                            len(bca), len(bda), ip(bca), ip(bsa), nat.ptr(bda),
+                            ndens, nbfs, nat.ptr(D), last_int, nat.ptr(out))
+    nat.check(rc)
+    return out
+
+
+def test_reference_abi_entry_points_vs_oracle():
+    """f_contract_coulomb_densities_2d / _4d, the symbols a Cython caller of
+    the reference binds, with host arrays in the reference's argument order:
+    against the oracle (8-atom workload) and against the Python front end."""
+    w = config_workload("cfg1")
+    nat.set_boys_mode("reference")
+    oracle.set_boys_mode("reference")
+    naux, nd, ns = w.shells_aux.sph_size, len(w.densities), w.nstates
+    df = _reference_call("f_contract_coulomb_densities_2d", w.shells, w.shells_aux, w.densities, (naux, nd), naux)
+    R = _reference_call("f_contract_coulomb_densities_4d", w.shells, w.shells_aux, w.densities, (ns,) * 4, ns)
+    assert_tensor_close(df, oracle.contract_coulomb_densities_2d(w.shells, w.shells_aux, w.densities), atol=3e-11)
+    assert_tensor_close(R, oracle.contract_coulomb_densities_4d(w.shells, w.shells_aux, w.densities))
+    np.testing.assert_array_equal(df, dia.contract_coulomb_densities_2d(w.shells, w.shells_aux, w.densities))
+    np.testing.assert_array_equal(R, dia.contract_coulomb_densities_4d(w.shells, w.shells_aux, w.densities))
+    # a naux that does not match the auxiliary basis is rejected, not written past
+    with pytest.raises(nat.PaError) as e:
+        _reference_call("f_contract_coulomb_densities_2d", w.shells, w.shells_aux, w.densities, (naux, nd),
+                        naux - 1)
+    assert e.value.code == nat.PA_ERR_ARG
