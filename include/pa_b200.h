@@ -260,17 +260,22 @@ int pa_cholesky_solve(int n, double* A, int nrhs, double* B);
  *
  * d_A (n x n, column-major, device): its lower triangle is replaced by L with
  * A = L L^T (entries above the diagonal are left as they were). d_B (n x nrhs,
- * device) is read only; d_X (n x nrhs, device) receives L^-1 B. stream is a
- * cudaStream_t (0 = default stream); the call returns after the work on it has
- * finished. Limit: 4096 * ceil(n / 64) + n * nrhs + 32 <= PA_NOALLOC_SCRATCH_DOUBLES
- * (e.g. n = 2240 with nrhs up to 404), else PA_ERR_SCRATCH before any device
- * work. PA_ERR_NOT_SPD as for pa_cholesky_solve.
+ * device) is read only; d_X (n x nrhs, device) receives L^-1 B. d_X may be d_B
+ * (B is copied to the scratch array first) but must not overlap d_A
+ * (PA_ERR_ARG). stream is a cudaStream_t (0 = default stream). The call is
+ * synchronous: it reads a status word back to the host and waits for `stream`
+ * before it returns. Limit: 4096 * ceil(n / 64) + n * nrhs + 32 <=
+ * PA_NOALLOC_SCRATCH_DOUBLES (e.g. n = 2240 with nrhs up to 404), else
+ * PA_ERR_SCRATCH before any device work. PA_ERR_NOT_SPD as for
+ * pa_cholesky_solve. A CUDA error already pending from the caller's earlier
+ * work is reported (PA_ERR_CUDA) and left pending.
  *
- * The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture. All calls in the process share the one array per
- * device: calls that overlap on the GPU (concurrent streams or host threads)
- * race on it and must be serialized by the caller. */
+ * Every call looks up the array's device address in the current context
+ * (cudaGetSymbolAddress, with the device current); the first call on a device
+ * also loads the library's device code there, so make that first call before
+ * any stream capture. All calls in the process share the one array per device:
+ * calls that overlap on the GPU (concurrent streams or host threads) race on
+ * it and must be serialized by the caller. */
 #define PA_NOALLOC_SCRATCH_DOUBLES (1 << 20)
 int pa_cholesky_solve_noalloc(int n, double* d_A, int nrhs, const double* d_B, double* d_X,
                               void* stream);

@@ -18,7 +18,7 @@
 //                                     every call before the factorization
 #include <cuda_runtime.h>
 
-#include <mutex>
+#include <cstdint>
 #include <string>
 
 #include "k_linalg.cuh"
@@ -32,33 +32,27 @@ int set_error(int code, const std::string& msg);
 namespace {
 
 constexpr size_t kScratchDoubles = PA_NOALLOC_SCRATCH_DOUBLES;
-constexpr int kMaxDevices = 64;
 
 // Every GPU that loads this library holds this array until the process exits.
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
-std::mutex g_mu;
-double* g_scratch_addr[kMaxDevices] = {};
-
-// Device address of g_noalloc_scratch on the current device, looked up once
-// per device (the host-side name is only a stand-in for the symbol).
+// Device address of g_noalloc_scratch in the current context. The host-side
+// name is only a stand-in for the symbol; the address belongs to a context
+// (it changes after cudaDeviceReset, and differs on a non-primary context of
+// the same device), so it is looked up on every call -- a host-side table
+// lookup once the module is loaded on the device.
 int scratch_address(double** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess)
-    return pa::set_error(PA_ERR_NO_DEVICE, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-  if (dev < 0 || dev >= kMaxDevices) return pa::set_error(PA_ERR_ARG, "device index out of range");
-  std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p)
-      return pa::set_error(PA_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") +
-                                            cudaGetErrorString(e));
-    g_scratch_addr[dev] = static_cast<double*>(p);
-  }
-  *out = g_scratch_addr[dev];
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p)
+    return pa::set_error(PA_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+  *out = static_cast<double*>(p);
   return PA_OK;
+}
+
+bool overlaps(const void* a, size_t abytes, const void* b, size_t bbytes) {
+  const auto x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
+  return abytes && bbytes && x < y + bbytes && y < x + abytes;
 }
 
 }  // namespace
@@ -77,6 +71,16 @@ extern "C" int pa_cholesky_solve_noalloc(int n, double* d_A, int nrhs, const dou
                              " scratch doubles; the fixed maximum is " + std::to_string(kScratchDoubles) +
                              " (64 * ceil(n / 64) * 64 + n * nrhs + 32 <= " +
                              std::to_string(kScratchDoubles) + ")");
+  const size_t nb = static_cast<size_t>(n) * nrhs;
+  // X is written while L is still being read: it must not overlap A (X == B is fine,
+  // B is copied to the scratch array before anything is written)
+  if (nb && overlaps(d_X, sizeof(double) * nb, d_A, sizeof(double) * n * static_cast<size_t>(n)))
+    return pa::set_error(PA_ERR_ARG, "pa_cholesky_solve_noalloc: d_X overlaps d_A");
+  // an error left by earlier, unrelated work is reported as such and not cleared
+  cudaError_t e = cudaPeekAtLastError();
+  if (e != cudaSuccess)
+    return pa::set_error(PA_ERR_CUDA, std::string("a CUDA error from earlier work is pending: ") +
+                                          cudaGetErrorString(e));
   double* scratch = nullptr;
   int st = scratch_address(&scratch);
   if (st != PA_OK) return st;
@@ -85,16 +89,15 @@ extern "C" int pa_cholesky_solve_noalloc(int n, double* d_A, int nrhs, const dou
   double* work = scratch;
   double* Bw = scratch + dinv;
   int* info = reinterpret_cast<int*>(scratch + dinv + static_cast<size_t>(n) * nrhs);
-  const size_t nb = static_cast<size_t>(n) * nrhs;
   if (nb) {
-    const cudaError_t e = cudaMemcpyAsync(Bw, d_B, sizeof(double) * nb, cudaMemcpyDeviceToDevice, s);
+    e = cudaMemcpyAsync(Bw, d_B, sizeof(double) * nb, cudaMemcpyDeviceToDevice, s);
     if (e != cudaSuccess)
       return pa::set_error(PA_ERR_CUDA, std::string("copy of B: ") + cudaGetErrorString(e));
   }
   pa::cholesky_lower(d_A, n, info, work, s);  // clears *info first
   if (nb) pa::trsm_lower_left(d_A, n, work, Bw, n, nrhs, d_X, n, s);
   int h_info = 0;
-  cudaError_t e = cudaGetLastError();
+  e = cudaGetLastError();  // nothing was pending on entry: this is this call's own launch error
   if (e == cudaSuccess) e = cudaMemcpyAsync(&h_info, info, sizeof(int), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return pa::set_error(PA_ERR_CUDA, std::string("Cholesky solve: ") + cudaGetErrorString(e));

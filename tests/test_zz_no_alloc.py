@@ -107,3 +107,40 @@ def test_lookahead_factor_is_bitwise_the_plain_order():
     Lref, Yref = nat.cholesky_solve(A, B)
     np.testing.assert_array_equal(np.tril(L), np.tril(Lref))
     np.testing.assert_array_equal(Y, Yref)
+
+
+def test_noalloc_cholesky_rejects_output_overlapping_the_matrix():
+    """L is read while X is written: an output inside A is refused before any
+    device work; X == B is allowed (B is copied to the scratch array first)."""
+    torch = pytest.importorskip("torch")
+    torch.cuda.set_device(0)
+    n, nrhs = 64, 2
+    A = _spd(np.random.default_rng(3), n)
+    dA = torch.from_numpy(np.asfortranarray(A).ravel(order="F").copy()).cuda()
+    dB = torch.ones(n * nrhs, dtype=torch.float64, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    lib = nat.load()
+    rc = lib.pa_cholesky_solve_noalloc(n, dA.data_ptr(), nrhs, dB.data_ptr(), dA.data_ptr() + 8 * 100, s)
+    assert rc == nat.PA_ERR_ARG and "overlaps" in lib.pa_last_error().decode()
+    np.testing.assert_array_equal(dA.cpu().numpy().reshape(n, n, order="F"), A)  # untouched
+    Lref, Yref = nat.cholesky_solve(A, np.ones((n, nrhs)))
+    nat.check(lib.pa_cholesky_solve_noalloc(n, dA.data_ptr(), nrhs, dB.data_ptr(), dB.data_ptr(), s))
+    np.testing.assert_allclose(dB.cpu().numpy().reshape(n, nrhs, order="F"), Yref,
+                               atol=1e-12 * np.abs(Yref).max(), rtol=0)
+
+
+def test_noalloc_cholesky_on_a_second_device():
+    """The scratch address is looked up in the current context: a call on
+    device 1 after one on device 0 uses device 1's copy of the array."""
+    torch = pytest.importorskip("torch")
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two visible GPUs")
+    rng = np.random.default_rng(13)
+    A = _spd(rng, 200)
+    B = rng.normal(size=(200, 5))
+    Lref, Yref = nat.cholesky_solve(A, B)
+    for dev in (0, 1, 0):
+        torch.cuda.set_device(dev)
+        L, Y = _noalloc(torch, A, B)
+        np.testing.assert_allclose(Y, Yref, atol=1e-12 * np.abs(Yref).max(), rtol=0)
+    torch.cuda.set_device(0)
