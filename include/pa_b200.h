@@ -245,6 +245,18 @@ int pa_metric(pa_basis aux, double* metric);
  * (n x nrhs) by L^-1 B. PA_ERR_NOT_SPD when A is not positive definite. */
 int pa_cholesky_solve(int n, double* A, int nrhs, double* B);
 
+/* The metric half of contract_coulomb_densities_2d / _4d on device buffers
+ * (common/linalg.f90:60-82 inv_chol, diabatization/intor.f90:198 dtrmm and
+ * :204-270 the tensor): (P|Q) of `aux` (+ the metric shift), its Cholesky
+ * factor, d_df = L^-1 d_raw (naux x ndens, column-major) and, with nstates > 0,
+ * the Coulomb tensor (nstates^4, column-major) into d_coulomb. d_raw is the
+ * screened three-center contraction, e.g. gathered from auxiliary-shell shards
+ * (pa_df_2d with the metric skipped, on a sub-basis of consecutive auxiliary
+ * shells per rank); it is read only. Synchronous on `stream`. No counterpart
+ * entry point in the reference, whose driver does these steps inline. */
+int pa_df_solve(pa_basis aux, int ndens, const double* d_raw, double* d_df, int nstates, double* d_coulomb,
+                void* stream);
+
 /* Allocation-free variant of pa_cholesky_solve on device buffers. This entry
  * point has no counterpart in the reference.
  *

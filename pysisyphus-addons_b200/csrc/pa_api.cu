@@ -2082,6 +2082,68 @@ int pa_metric(pa_basis aux, double* metric) {
   return PA_OK;
 }
 
+// The metric half of the path on device buffers: (P|Q) of the auxiliary basis
+// (+ the metric shift), its Cholesky factor, d_df = L^-1 d_raw and, with
+// nstates > 0, the Coulomb tensor. The same stages as the end of run_df
+// (stage_metric, stage_solve, coulomb_4d), for a raw contraction assembled
+// from auxiliary-shell shards computed elsewhere (other ranks).
+int pa_df_solve(pa_basis aux, int ndens, const double* d_raw, double* d_df, int nstates, double* d_coulomb,
+                void* stream) {
+  if (!aux) return fail(PA_ERR_ARG, "null basis handle");
+  if (ndens < 0 || (ndens > 0 && (!d_raw || !d_df))) return fail(PA_ERR_ARG, "null raw or df pointer");
+  if (nstates < 0 || (nstates > 0 && (nstates * (nstates + 1) / 2 != ndens || !d_coulomb)))
+    return fail(PA_ERR_ARG, "nstates must be 0, or satisfy ndens = nstates (nstates + 1) / 2 with an output");
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (aux->device != dev) return fail(PA_ERR_ARG, "basis handle belongs to another device");
+  Ctx* c = nullptr;
+  DeviceTables dt;
+  int st = current_ctx(&c, &dt);
+  if (st != PA_OK) return st;
+  std::lock_guard<std::mutex> lk(c->mu);
+  const Options o = options();
+  const int naux = aux->host.nsph;
+  const size_t nn = static_cast<size_t>(naux) * naux;
+  Carver cnt;
+  for (int pass = 0; pass < 2; ++pass) {
+    Carver cv;
+    if (pass == 1) {
+      PA_CUDA(c->arena.reserve(cnt.used));
+      cv.base = c->arena.base;
+    }
+    DfBuffers b;
+    b.M = cv.take<double>(nn);
+    b.lawork = cv.take<double>(linalg_workspace_doubles(naux));
+    b.info = cv.take<int>(4);
+    double* gram = cv.take<double>(static_cast<size_t>(ndens) * ndens);
+    double* raw_copy = cv.take<double>(static_cast<size_t>(naux) * ndens);  // the solve overwrites its input
+    if (pass == 0) {
+      cnt = cv;
+      continue;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    PA_CUDA(cudaEventRecord(c->ev0, s));
+    int launches = 0;
+    stage_metric(aux, b, dt, o, s, nullptr, &launches);
+    if (ndens > 0) {
+      PA_CUDA(cudaMemcpyAsync(raw_copy, d_raw, sizeof(double) * naux * ndens, cudaMemcpyDeviceToDevice, s));
+      b.df_raw = raw_copy;
+      st = stage_solve(aux, ndens, b, o, d_df, s, &launches);
+      if (st != PA_OK) return st;
+      if (nstates > 0) launches += coulomb_4d(d_df, naux, ndens, nstates, gram, d_coulomb, s);
+    }
+    PA_CUDA(cudaEventRecord(c->ph[0], s));
+    PA_CUDA(cudaEventRecord(c->ph[1], s));
+    PA_CUDA(cudaEventRecord(c->m0, s));
+    PA_CUDA(cudaEventRecord(c->m1, s));
+    PA_CUDA(cudaEventRecord(c->ph[2], s));
+    float ms = 0.f;
+    g_stats = pa_stats{};
+    return finish(c, b, s, launches, &ms);
+  }
+  return PA_OK;
+}
+
 int pa_cholesky_solve(int n, double* A, int nrhs, double* B) {
   if (n < 0 || nrhs < 0 || (n > 0 && !A) || (n > 0 && nrhs > 0 && !B))
     return fail(PA_ERR_ARG, "invalid Cholesky arguments");

@@ -115,6 +115,7 @@ SIGNATURES = {
     "pa_std_eri2c": [_vp, _vp, _vp, _vp],
     "pa_std_df2c_mo": [_vp, _vp, _i, _vp, _vp, _vp],
     "pa_cholesky_solve_noalloc": [_i, _vp, _i, _vp, _vp, _vp],
+    "pa_df_solve": [_vp, _i, _vp, _vp, _i, _vp, _vp],
 }
 
 _lib = None
