@@ -1,25 +1,34 @@
 """Benchmark of the density-fitting Coulomb-tensor path on B200.
 
-Default (the headline line): one step = one full Coulomb tensor of the 40-atom
-workload (lmax 3 / lauxmax 4, 8 states, 36 densities) on the device: Schwarz
-screening, class sorting, density folding, metric + Cholesky, screened 3c2e
-contraction, L^-1 df and the tensor assembly. Inputs (basis handles, densities)
-are resident in HBM when the timed region starts; the densities (133 MB)
-exceed the 126 MB L2.
+Default (the headline line): the 200-atom cluster (lmax 4 / lauxmax 5, 8
+states, 36 densities, 4950 basis / 13400 auxiliary functions). One step = one
+full Coulomb tensor on the device: Schwarz screening, class sorting, density
+folding, metric + Cholesky, screened 3c2e contraction, L^-1 df and the tensor
+assembly. Two forms run back to back on the same inputs:
+
+  - the plain FP64 form (pa_df_4d, precision fp64);
+  - the headline form, mixed precision + batched (pa_df_4d_batch over the
+    molecule, recorded once as a CUDA graph; FP32 recurrences for triplets
+    whose Schwarz bound is below 1e-6).
+
+`value` is the headline form's throughput; `forms` gives both forms' times,
+their ratio and the max-abs / relative error of the headline form's tensor
+against the FP64 form's. Inputs (basis handles, densities) are resident in
+HBM when the timed region starts; the densities (7 GB) exceed the 126 MB L2.
 
 metric: surviving spherical 3c2e integrals per second (the integrals the
 reference evaluates after Schwarz screening, diabatization/intor.f90:126-151).
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
-                  [--config cfg1|cfg2|cfg5|cfg4] [--precision fp64|mixed]
+                  [--config cfg5|cfg2|cfg1|cfg4] [--form headline|fp64|mixed]
 
---config cfg5 is the 200-atom cluster (lmax 4 / lauxmax 5), cfg4 the batch of 64
-molecules (5-60 atoms, 4-16 states) run through pa_df_4d_batch (one CUDA graph
-per step). Both use the exact Boys function and a 1e-7 diagonal shift of the
-metric: with the reference's Boys interpolation their auxiliary metrics are
-indefinite and the Cholesky fails (the reference ignores that failure).
---precision mixed runs the precision form (FP32 recurrences for triplets with
-Schwarz bound < 1e-6).
+--config cfg2 is the 40-atom workload (lmax 3 / lauxmax 4), cfg4 the batch of
+64 molecules (5-60 atoms, 4-16 states) run through pa_df_4d_batch (one CUDA
+graph per step; --sequential: one pa_df_4d call per molecule). cfg5 and cfg4
+use the exact Boys function and a 1e-7 diagonal shift of the metric: with the
+reference's Boys interpolation their auxiliary metrics are indefinite and the
+Cholesky fails (the reference ignores that failure). --form fp64 / mixed
+measure a single form through pa_df_4d.
 
 --impl reference times the reference's CPU algorithm (the C++ OpenMP
 restatement under oracle/, as the Fortran reference cannot be built here) on
@@ -44,16 +53,35 @@ sys.path.insert(0, str(ROOT / "pysisyphus-addons_b200"))
 sys.path.insert(0, str(ROOT / "oracle"))
 
 UNIT = "ints/s"
-CONFIG_KEY = "cfg2"
+CONFIG_KEY = "cfg5"
+# the metric as named by the headline measurement
+HEADLINE_METRIC = "3c2e ints/s and Coulomb-tensor time at \u22641e-9 err: mixed+batched vs FP64 GPU"
+FP32_THRESH = 1e-6
 # workloads whose auxiliary metric needs the exact Boys function and a shift
 SHIFTED = {"cfg5": 1e-7, "cfg4": 1e-7}
+# DRAM bytes (read + write) of the three-center family per step from ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum, -k regex:k_df3c): None until captured
+TRAFFIC_3C = {}
+
+
+def single_molecule(args):
+    return args.config in ("cfg1", "cfg2", "cfg5")
+
+
+def headline(args):
+    """The headline measurement: mixed + batched against the plain FP64 form."""
+    return single_molecule(args) and args.form == "headline"
 
 
 def metric_name(args):
-    form = "mixed precision" if args.precision == "mixed" else "FP64 plain"
-    path = "batched Coulomb tensors" if args.config == "cfg4" else "Coulomb tensor"
-    if args.config == "cfg4" and args.sequential:
-        path = "Coulomb tensors of the batch, one call per molecule"
+    if headline(args):
+        return HEADLINE_METRIC
+    if args.config == "cfg4":
+        form = "mixed precision" if args.precision == "mixed" else "FP64 plain"
+        path = "Coulomb tensors of the batch, one call per molecule" if args.sequential else "batched Coulomb tensors"
+    else:
+        form = "mixed precision" if args.form == "mixed" else "FP64 plain"
+        path = "Coulomb tensor"
     if args.screening == "qvl":
         form += ", QVL screening"
     return f"3c2e ints/s ({path}, {form} path)"
@@ -62,11 +90,15 @@ def metric_name(args):
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 5 for the 200-atom workload and the batch, 10 otherwise)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default=CONFIG_KEY, choices=["cfg1", "cfg2", "cfg5", "cfg4"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--form", default="headline", choices=["headline", "fp64", "mixed"],
+                    help="single-molecule workloads: headline = FP64 plain and mixed + batched back to back "
+                         "(value = mixed + batched); fp64 / mixed = one form through pa_df_4d")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"], help="cfg4: precision of the batch")
     ap.add_argument("--boys", default=None, choices=["reference", "exact"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -84,6 +116,10 @@ def parse():
     a = ap.parse_args()
     if a.boys is None:
         a.boys = "exact" if a.config in SHIFTED else "reference"
+    if a.steps is None:
+        a.steps = 5 if a.config in ("cfg5", "cfg4") else 10
+    if not a.profile:
+        a.warmup = max(3, a.warmup)  # at least three untimed warm-up steps
     return a
 
 
@@ -96,11 +132,19 @@ def workloads(args, rank=0):
 
 
 def workload_config(args, ws):
+    """The `config` object; both arms (ours and --impl reference) print the same one."""
     from pysisyphus_addons.common.synthetic import CONFIGS
 
     shift = SHIFTED.get(args.config, 0.0)
-    base = {"boys_mode": args.boys, "precision": args.precision, "screen_thresh": "float32(1e-10)",
-            "screening": args.screening, "metric_shift": shift}
+    base = {"boys_mode": args.boys, "screen_thresh": "float32(1e-10)", "screening": args.screening,
+            "metric_shift": shift}
+    if headline(args):
+        base["forms"] = (f"fp64 plain (pa_df_4d) and mixed precision (FP32 recurrences below Schwarz bound "
+                         f"{FP32_THRESH:g}) + batched (pa_df_4d_batch, CUDA graph); value = mixed + batched")
+    elif args.config == "cfg4":
+        base["precision"] = args.precision
+    else:
+        base["precision"] = args.form
     if shift:
         base["metric_shift_reason"] = ("auxiliary metric numerically singular for this workload "
                                        "(smallest eigenvalues ~ -1e-13 with exact Boys)")
@@ -121,6 +165,7 @@ def workload_config(args, ws):
                 natoms=c["natoms"], lmax=c["lmax"], lauxmax=c["lauxmax"], nstates=c["nstates"],
                 ndens=len(w.densities), nbf=w.shells.sph_size, naux=w.shells_aux.sph_size,
                 nshells=len(w.shells), nshells_aux=len(w.shells_aux))
+
 
 
 class Clocks:
@@ -222,9 +267,14 @@ def aggregate_over_ranks(dist, torch, elapsed_s, nints, device):
 
 def oracle_sample(args, ws, budget_s=20.0):
     """Time the oracle (C++ OpenMP restatement of the reference driver) on a
-    bounded sample of the workload: whole tensors while they fit the budget,
-    else the leading auxiliary shells of the molecule (every (ab|c) of those c,
-    their metric and solve). Returns (ints/s, cores, description)."""
+    bounded sample of the workload. 8- and 40-atom workloads: one whole tensor.
+    The batch: whole tensors of its first molecules while they fit the budget.
+    200 atoms: every 200th auxiliary shell (17 shells of every angular momentum,
+    on atoms across the cluster) against the full orbital basis -- all their
+    surviving (ab|c), the metric and the solve; the bra Schwarz vector (an
+    O(npairs) pass done once per tensor, ~0.1 % of a full CPU tensor) is
+    computed on the first call and reused. Returns (ints/s, cores,
+    description)."""
     import oracle
 
     from pysisyphus_addons.common.shells import Shells
@@ -252,17 +302,17 @@ def oracle_sample(args, ws, budget_s=20.0):
                 break
         return ints / t_tot, threads, f"the first {done} molecules of the batch, whole tensors ({t_tot:.1f} s)"
     w = ws[0]
-    k = 8
-    while True:
-        sub = Shells(w.shells_aux.shells[:k])
-        t0 = time.perf_counter()
+    sub = Shells(w.shells_aux.shells[::200])
+    oracle.set_reuse_screening(1)
+    try:
         oracle.contract_coulomb_densities_2d(w.shells, sub, w.densities)
-        dt = time.perf_counter() - t0
-        n = oracle.last_stats()["nints"]
-        if dt > budget_s / 4 or k >= len(w.shells_aux):
-            return n / dt, threads, (f"the first {k} of {len(w.shells_aux)} auxiliary shells of the workload: "
-                                     f"all their surviving (ab|c), metric and solve ({dt:.1f} s)")
-        k *= 2
+        st = oracle.last_stats()
+    finally:
+        oracle.set_reuse_screening(0)
+    dt = st["t_total"]
+    return st["nints"] / dt, threads, (
+        f"every 200th auxiliary shell ({len(sub)} of {len(w.shells_aux)}) against the full orbital basis: "
+        f"all their surviving (ab|c), metric and solve ({dt:.1f} s; bra Schwarz vector reused)")
 
 
 def run_reference(args):
@@ -272,7 +322,7 @@ def run_reference(args):
     ws = workloads(args)
     steps = []
     for i in range(args.warmup + args.steps):
-        v, threads, sample = oracle_sample(args, ws, budget_s=20.0 if args.config in SHIFTED else 1e9)
+        v, threads, sample = oracle_sample(args, ws)
         if i >= args.warmup:
             steps.append(v)
     value = statistics.mean(steps) if steps else v
@@ -287,6 +337,7 @@ def run_reference(args):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
 
 
 def precision_report(args):
@@ -381,7 +432,6 @@ def main():
 
     nat.set_boys_mode(args.boys)
     nat.set_metric_shift(SHIFTED.get(args.config, 0.0))
-    nat.set_precision(args.precision, 1e-6)
     nat.set_screening(args.screening)
     ws = workloads(args, rank)
     orbs = [nat.Basis(w.shells, "orbital") for w in ws]
@@ -399,81 +449,128 @@ def main():
             assert tm == t_c and im == n_i, (tm, t_c, im, n_i)
             flops_3c += f
 
-    # densities live in pinned host memory (one copy per molecule: the batch
-    # holds ~11 GB of them), and on the device
+    # densities live in pinned host memory (one copy per molecule) and on the device
     for w in ws:
         w.densities = torch.from_numpy(np.ascontiguousarray(w.densities)).pin_memory().numpy()
     dens = [torch.from_numpy(w.densities).cuda() for w in ws]
     ns = [w.nstates for w in ws]
-    outs = [torch.empty(k**4, dtype=torch.float64, device="cuda") for k in ns]
     stream = torch.cuda.current_stream()
     lib = nat.load()
-    batched = args.config == "cfg4" and not args.sequential
     step_stats = []  # statistics of every call of the last step
 
-    def step():
-        step_stats.clear()
-        if batched:
-            nat.df_4d_batch(orbs, auxs, dens, ns, outs, use_graph=True, stream=stream.cuda_stream)
-            step_stats.append(nat.get_stats())
-            return
-        for o, a, d, k, out in zip(orbs, auxs, dens, ns, outs):
-            nat.check(lib.pa_df_4d(o.handle, a.handle, d.shape[0], d.shape[1], d.data_ptr(),
-                                   nat.PA_LAYOUT_C, k, out.data_ptr(), stream.cuda_stream))
-            step_stats.append(nat.get_stats())
+    def set_form(form):
+        if form in ("mixed", "mixed_batched") or (form == "batched" and args.precision == "mixed"):
+            nat.set_precision("mixed", FP32_THRESH)
+        else:
+            nat.set_precision("fp64")
+
+    def make_step(kind, outs):
+        """kind: "plain" (one pa_df_4d per molecule) or "batched" (pa_df_4d_batch)."""
+        def step():
+            step_stats.clear()
+            if kind == "batched":
+                nat.df_4d_batch(orbs, auxs, dens, ns, outs, use_graph=True, stream=stream.cuda_stream)
+                step_stats.append(nat.get_stats())
+                return
+            for o, a, d, k, out in zip(orbs, auxs, dens, ns, outs):
+                nat.check(lib.pa_df_4d(o.handle, a.handle, d.shape[0], d.shape[1], d.data_ptr(),
+                                       nat.PA_LAYOUT_C, k, out.data_ptr(), stream.cuda_stream))
+                step_stats.append(nat.get_stats())
+        return step
+
+    # the measured forms, in order; the last one gives `value`
+    if headline(args):
+        forms = [("fp64", "plain"), ("mixed_batched", "batched")]
+    elif args.config == "cfg4":
+        forms = [("mixed" if args.precision == "mixed" else "fp64", "plain" if args.sequential else "batched")]
+    else:
+        forms = [(args.form, "plain")]
+    outs = {name: [torch.empty(k**4, dtype=torch.float64, device="cuda") for k in ns] for name, _ in forms}
 
     if args.profile:
-        for _ in range(args.warmup + args.steps):
+        for name, kind in forms:
+            set_form(name)
+            step = make_step(kind, outs[name])
+            for _ in range(args.warmup + args.steps):
+                step()
+        torch.cuda.synchronize()
+        nat.set_precision("fp64")
+        return
+
+    clocks = Clocks(local)
+    results = {}
+    launches = 0
+    total_ints = float(nints)
+    for name, kind in forms:
+        set_form(name)
+        step = make_step(kind, outs[name])
+        for _ in range(args.warmup):
             step()
         torch.cuda.synchronize()
-        return
-    for _ in range(max(3, args.warmup)):
-        step()
-    torch.cuda.synchronize()
-    clocks = Clocks(local)
-    ms3c, launches, launches3c, phases = [], 0, 0, []
-    barrier()
-    torch.cuda.synchronize()
-    clocks.start()
-    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    t_start.record(stream)
-    for _ in range(args.steps):
-        step()
-        # the class kernels start while the density folding of later L_ab
-        # classes still runs, so the span timed for them is folding + 3c
-        ms3c.append(sum(st["ms_bra"] + st["ms_3c"] for st in step_stats))
-        phases.append({k: sum(st[k] for st in step_stats)
-                       for k in ("ms_screen", "ms_bra", "ms_metric", "ms_3c", "ms_solve")})
-        launches += sum(st["kernel_launches"] for st in step_stats)
-        launches3c += sum(st["launches_3c"] for st in step_stats)
-    t_end.record(stream)
-    torch.cuda.synchronize()
-    barrier()
+        ms3c, phases, lc, lc3 = [], [], 0, 0
+        barrier()
+        torch.cuda.synchronize()
+        if clocks.thread is None and clocks.error is None:
+            clocks.start()
+        t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t_start.record(stream)
+        for _ in range(args.steps):
+            step()
+            # the class kernels start while the density folding of later L_ab
+            # classes still runs, so the span timed for them is folding + 3c
+            ms3c.append(sum(st["ms_bra"] + st["ms_3c"] for st in step_stats))
+            phases.append({k: sum(st[k] for st in step_stats)
+                           for k in ("ms_screen", "ms_bra", "ms_metric", "ms_3c", "ms_solve")})
+            lc += sum(st["kernel_launches"] for st in step_stats)
+            lc3 += sum(st["launches_3c"] for st in step_stats)
+        t_end.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        elapsed = t_start.elapsed_time(t_end) / 1e3
+        if world > 1:
+            elapsed, total_ints = aggregate_over_ranks(dist, torch, elapsed, nints, "cuda")
+        launches += lc
+        results[name] = {"kind": kind, "step_s": elapsed / args.steps, "value": total_ints / (elapsed / args.steps),
+                         "ms3c": ms3c, "phases": phases, "launches": lc, "launches_3c": lc3}
     clk = clocks.stop()
-    elapsed = t_start.elapsed_time(t_end) / 1e3
-    if world > 1:
-        elapsed, total_ints = aggregate_over_ranks(dist, torch, elapsed, nints, "cuda")
-    else:
-        total_ints = float(nints)
-    step_s = elapsed / args.steps
-    value = total_ints / step_s
+    nat.set_precision("fp64")
+    head = results[forms[-1][0]]
+    step_s, value = head["step_s"], head["value"]
 
-    # end to end through the public Python API: pinned host densities copied in
-    # and the tensors copied out in every call
+    # errors of the headline form's tensor against the FP64 form's
+    form_report = None
+    if headline(args):
+        Rf = outs["fp64"][0].cpu().numpy()
+        Rm = outs["mixed_batched"][0].cpu().numpy()
+        dmax = float(np.abs(Rm - Rf).max())
+        form_report = {
+            "fp64_plain": {"ms_per_step": results["fp64"]["step_s"] * 1e3, "value": results["fp64"]["value"]},
+            "mixed_batched": {"ms_per_step": step_s * 1e3, "value": value},
+            "speedup_mixed_batched_vs_fp64": results["fp64"]["step_s"] / step_s,
+            "tensor_err_vs_fp64": {"max_abs": dmax, "rel_of_max": dmax / float(np.abs(Rf).max())},
+            "fp32_thresh": FP32_THRESH,
+        }
+
+    # end to end through the reference-facing Python API: pinned host densities
+    # copied in and the tensors copied out in every call
     e2e = None
     if not args.no_e2e:
         pinned = [torch.from_numpy(w.densities) for w in ws]  # already pinned
-        if batched:
+        e2e_form = forms[-1][0]
+        set_form(e2e_form)
+        batched_e2e = args.config == "cfg4" and not args.sequential
+        if batched_e2e:
             host_out = [torch.empty(k**4, dtype=torch.float64).pin_memory() for k in ns]
 
             def call():
                 for dd, hp in zip(dens, pinned):
                     dd.copy_(hp, non_blocking=True)
-                nat.df_4d_batch(orbs, auxs, dens, ns, outs, use_graph=True, stream=stream.cuda_stream)
-                for ho, o in zip(host_out, outs):
+                nat.df_4d_batch(orbs, auxs, dens, ns, outs[e2e_form], use_graph=True, stream=stream.cuda_stream)
+                for ho, o in zip(host_out, outs[e2e_form]):
                     ho.copy_(o, non_blocking=True)
                 torch.cuda.synchronize()
                 return host_out[0].numpy()
+            api = "pysisyphus_addons._native.df_4d_batch (device buffers filled from pinned host memory)"
         else:
             arrs = [p.numpy() for p in pinned]
 
@@ -482,28 +579,28 @@ def main():
                 for w, arr in zip(ws, arrs):
                     R = dia.contract_coulomb_densities_4d(w.shells, w.shells_aux, arr)
                 return R
-        for _ in range(max(3, args.warmup)):  # as many warm-up calls as the device loop
-            R = call()
+            api = ("pysisyphus_addons.diabatization.intor.contract_coulomb_densities_4d (the reference's "
+                   "function, host arrays; precision " + ("fp64" if e2e_form == "fp64" else "mixed") + ")")
+        for _ in range(args.warmup):  # as many warm-up calls as the device loop
+            call()
         torch.cuda.synchronize()
         barrier()
         iters = []
         t0 = time.perf_counter()
         for _ in range(args.steps):
             ti = time.perf_counter()
-            R = call()
+            call()
             iters.append((time.perf_counter() - ti) * 1e3)
         torch.cuda.synchronize()
         e2e_s = (time.perf_counter() - t0) / args.steps
+        nat.set_precision("fp64")
         if world > 1:
             e2e_s, _ = aggregate_over_ranks(dist, torch, e2e_s, 0, "cuda")
         keep = [a for w in ws for a in (w.shells.as_arrays(fortran=True) + w.shells_aux.as_arrays(fortran=True))]
-        h2d = int(sum(p.numpy().nbytes for p in pinned) + (0 if batched else sum(a.nbytes for a in keep)))
+        h2d = int(sum(p.numpy().nbytes for p in pinned) + (0 if batched_e2e else sum(a.nbytes for a in keep)))
         d2h = int(sum(k**4 * 8 for k in ns))
-        e2e = {"value": total_ints / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3,
-               "api": "pysisyphus_addons._native.df_4d_batch (device buffers filled from pinned host memory)"
-               if batched else "pysisyphus_addons.diabatization.intor.contract_coulomb_densities_4d",
-               "ms_per_call": [round(x, 3) for x in iters]}
+        e2e = {"value": total_ints / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": e2e_s * 1e3, "api": api, "ms_per_call": [round(x, 3) for x in iters]}
 
     if rank != 0:
         if world > 1:
@@ -511,29 +608,36 @@ def main():
         return
     line = {
         "metric": metric_name(args), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": max(3, args.warmup), "ms_per_step": step_s * 1e3, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-        "config": dict(workload_config(args, ws),
-                       parallelism=f"independent molecules x{world}" if world > 1 else "single GPU"),
+        "config": workload_config(args, ws),
         "screening": {"triplets": ntrip_all, "computed": ntrip, "ints": nints},
         "gpu_launches": launches,
         "clocks": clk,
     }
-    if len(ws) == 1 and args.screening == "schwarz":
+    if world > 1:
+        line["ranks"] = f"independent molecules x{world} (seed = rank)"
+    if form_report:
+        line["forms"] = form_report
+    # roofline of the three-center family, timed in the plain form (its phase
+    # events bracket the density folding + three-center span)
+    plain = [n for n, k in forms if k == "plain" and len(ws) == 1]
+    if plain and args.screening == "schwarz":
+        r = results[plain[0]]
         peak = fp64_peak_tflops(torch)
-        ms3 = statistics.mean(ms3c)
+        ms3 = statistics.mean(r["ms3c"])
         achieved = flops_3c / (ms3 / 1e3) / 1e12
         line["roofline"] = {
             "bound": "tensor", "pipe": "FP64 (DMMA m8n8k4 tensor cores + FP64 FMA)",
-            "kernel": "k_df3c<LAB,LC> (all classes) + ordered reduction, timed over the folding + "
-                      "three-center span (k_bra_prep overlaps the first class launches)",
+            "kernel": f"k_df3c<LAB,LC> (all classes) + ordered reduction in the {plain[0]} form, timed over the "
+                      "folding + three-center span (k_bra_prep overlaps the first class launches)",
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
             "peak_source": "of measured: FP64 GEMM (torch.matmul float64 8192^3) in this run; "
                            "MEASURED_PEAKS.json has no FP64 figure",
-            "flops_per_step_3c": flops_3c, "ms_bra_plus_3c": ms3, "traffic": None}
-    if len(ws) == 1:
-        line["phases_ms"] = {k: statistics.mean(p[k] for p in phases) for k in phases[0]}
-        line["gpu_launches_3c"] = launches3c
+            "flops_per_step_3c": flops_3c, "ms_bra_plus_3c": ms3,
+            "traffic": TRAFFIC_3C.get(args.config)}
+        line["phases_ms"] = {k: statistics.mean(p[k] for p in r["phases"]) for k in r["phases"][0]}
+        line["gpu_launches_3c"] = r["launches_3c"]
     if e2e:
         line["e2e"] = e2e
     if world == 1 and not args.no_cpu_baseline:
