@@ -245,6 +245,26 @@ int pa_metric(pa_basis aux, double* metric);
  * (n x nrhs) by L^-1 B. PA_ERR_NOT_SPD when A is not positive definite. */
 int pa_cholesky_solve(int n, double* A, int nrhs, double* B);
 
+/* Densities on grid points (replaces grid/grid_wrapper.f90:12-38,
+ * f_eval_densities, same arguments): grid3d(3, npoints) column-major,
+ * densities(ndens, nbfs, nbfs) Cartesian AO density matrices in pysisyphus
+ * order (nbfs = the basis' Cartesian size), grid_densities(ndens, npoints)
+ * written. Points in consecutive blocks of blk_size (1..4096); a function pair
+ * contributes to a block when |f D mean_nu mean_mu| >= thresh
+ * (grid/grid.f90:236-258). Shells up to g (PA_ERR_LMAX above, where the
+ * reference writes NaN). Host buffers; synchronous. */
+int f_eval_densities(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
+                     const double* bas_data, int npoints, const double* grid3d, int ndens, int nbfs,
+                     const double* densities, double* grid_densities, int blk_size, double thresh);
+/* Density of the primitive pairs with exponent sum below `sw` on grid points
+ * (replaces gdma/prim_dens.f90:100-259, f_eval_prim_density, same arguments):
+ * ls_inds(2, nprims) = (L, 0-based Cartesian start), primdata(5, nprims) =
+ * (coefficient, exponent, x, y, z), coords3d(3, npoints), P(nbfs, nbfs),
+ * rho(npoints) written. L up to 4 (the reference's g prefactors fill 14 of
+ * the 15 components; these are all 15). Host buffers; synchronous. */
+int f_eval_prim_density(int nprims, int npoints, int nbfs, const int* ls_inds, const double* primdata,
+                        const double* coords3d, const double* P, double sw, double* rho);
+
 /* The metric half of contract_coulomb_densities_2d / _4d on device buffers
  * (common/linalg.f90:60-82 inv_chol, diabatization/intor.f90:198 dtrmm and
  * :204-270 the tensor): (P|Q) of `aux` (+ the metric shift), its Cholesky

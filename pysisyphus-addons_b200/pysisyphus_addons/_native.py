@@ -116,6 +116,8 @@ SIGNATURES = {
     "pa_std_df2c_mo": [_vp, _vp, _i, _vp, _vp, _vp],
     "pa_cholesky_solve_noalloc": [_i, _vp, _i, _vp, _vp, _vp],
     "pa_df_solve": [_vp, _i, _vp, _vp, _i, _vp, _vp],
+    "f_eval_densities": _BASIS + [_i, _pd, _i, _i, _pd, _pd, _i, _d],
+    "f_eval_prim_density": [_i, _i, _i, _pi, _pd, _pd, _pd, _d, _pd],
 }
 
 _lib = None
