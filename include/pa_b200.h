@@ -177,6 +177,13 @@ typedef struct {
   int launches_3c;           /* of which three-center contraction kernels      */
 } pa_stats;
 int pa_get_stats(pa_stats* out);
+/* Profiling aid (no counterpart in the reference): with on = 1 the
+ * three-center class launches of the single-molecule path run one after
+ * another on one stream, each bracketed by CUDA events; pa_get_class_times
+ * then gives (L_ab, L_c, ms) of every class run of the last call (up to cap
+ * entries) and returns their number. */
+int pa_set_class_timing(int on);
+int pa_get_class_times(int cap, int* lab, int* lc, double* ms);
 
 /* Device-resident path. A pa_basis holds an unpacked, normalized basis on the
  * host and its copy in device memory of the current device. */

@@ -374,7 +374,17 @@ struct Ctx {
   CholLookahead la2;
   CholLookahead la_met[kNs3c];
   struct BatchPlan* plan = nullptr;  // the last batch, kept for replay
+  // class timing (Options::class_timing): an event pair per class run
+  std::vector<cudaEvent_t> ct_ev;
 };
+
+// Per-class device times of the last single-molecule run in class-timing mode.
+struct ClassTime {
+  int lab, lc;
+  double ms;
+};
+std::mutex g_ct_mu;
+std::vector<ClassTime> g_class_times;
 
 std::mutex g_ctx_mu;
 std::vector<Ctx*> g_ctx;
@@ -895,12 +905,22 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
     // waits for the class streams and reduces that group while the next
     // groups run
     const int nr = static_cast<int>(b.runs.size());
+    if (o.class_timing)
+      while (static_cast<int>(ctx->ct_ev.size()) < 2 * nr) {
+        cudaEvent_t e;
+        PA_CUDA(cudaEventCreate(&e));
+        ctx->ct_ev.push_back(e);
+      }
     for (int ri = 0; ri < nr; ++ri) {
       const auto& r = b.runs[ri];
       Df3cArgs a = class_args(orb, aux, nd, b, dt, o, r);
       a.counter = b.counters + ri;
-      PA_CUDA(cudaStreamWaitEvent(ctx->s3c[ri % Ctx::kNs3c], ctx->ev_bra[r.lab], 0));
-      *launches += launch_df3c_class(r.lab, r.lc, a, r.ny, ctx->s3c[ri % Ctx::kNs3c]);
+      // class timing: every class on the first class stream, one after another
+      cudaStream_t cs = ctx->s3c[o.class_timing ? 0 : ri % Ctx::kNs3c];
+      PA_CUDA(cudaStreamWaitEvent(cs, ctx->ev_bra[r.lab], 0));
+      if (o.class_timing) PA_CUDA(cudaEventRecord(ctx->ct_ev[2 * ri], cs));
+      *launches += launch_df3c_class(r.lab, r.lc, a, r.ny, cs);
+      if (o.class_timing) PA_CUDA(cudaEventRecord(ctx->ct_ev[2 * ri + 1], cs));
       if (ri + 1 == nr || b.runs[ri + 1].lc != r.lc) {
         for (int i = 0; i < Ctx::kNs3c; ++i) {
           PA_CUDA(cudaEventRecord(ctx->j3c[i], ctx->s3c[i]));
@@ -935,6 +955,16 @@ int finish(Ctx* c, const DfBuffers& b, cudaStream_t s, int launches, float* ms) 
   g_stats.ms_solve = t[4];
   g_stats.kernel_launches = launches;
   g_stats.ms_total = *ms;
+  if (options().class_timing && !b.runs.empty() && c->ct_ev.size() >= 2 * b.runs.size()) {
+    std::vector<ClassTime> ct;
+    for (size_t ri = 0; ri < b.runs.size(); ++ri) {
+      float t = 0.f;
+      PA_CUDA(cudaEventElapsedTime(&t, c->ct_ev[2 * ri], c->ct_ev[2 * ri + 1]));
+      ct.push_back({b.runs[ri].lab, b.runs[ri].lc, static_cast<double>(t)});
+    }
+    std::lock_guard<std::mutex> lk(g_ct_mu);
+    g_class_times = std::move(ct);
+  }
   if (*c->h_info != 0)
     return fail(PA_ERR_NOT_SPD, "metric (P|Q) is not positive definite (Cholesky pivot " +
                                     std::to_string(*c->h_info) + ")");
@@ -1696,6 +1726,23 @@ int pa_set_items_per_sm(int items) {
   std::lock_guard<std::mutex> lk(g_opt_mu);
   g_opts.items_per_sm = items;
   return PA_OK;
+}
+
+int pa_set_class_timing(int on) {
+  std::lock_guard<std::mutex> lk(g_opt_mu);
+  g_opts.class_timing = on ? 1 : 0;
+  return PA_OK;
+}
+
+int pa_get_class_times(int cap, int* lab, int* lc, double* ms) {
+  std::lock_guard<std::mutex> lk(g_ct_mu);
+  const int n = static_cast<int>(g_class_times.size());
+  for (int i = 0; i < std::min(n, cap); ++i) {
+    if (lab) lab[i] = g_class_times[i].lab;
+    if (lc) lc[i] = g_class_times[i].lc;
+    if (ms) ms[i] = g_class_times[i].ms;
+  }
+  return n;
 }
 
 int pa_set_metric_shift(double shift) {

@@ -90,6 +90,7 @@ struct Options {
   double fp32_thresh = 1e-6;  // Schwarz bound below which the mixed form uses FP32
   int items_per_sm = 0;       // work items per SM and class of the three-center kernel (0 = by size)
   int screening = 0;          // triplet estimate: 0 = Schwarz (reference), 1 = QVL
+  int class_timing = 0;       // 1: class launches serialized on one stream, each timed with events
 };
 
 struct Stats {

@@ -116,6 +116,8 @@ SIGNATURES = {
     "pa_std_df2c_mo": [_vp, _vp, _i, _vp, _vp, _vp],
     "pa_cholesky_solve_noalloc": [_i, _vp, _i, _vp, _vp, _vp],
     "pa_df_solve": [_vp, _i, _vp, _vp, _i, _vp, _vp],
+    "pa_set_class_timing": [_i],
+    "pa_get_class_times": [_i, _pi, _pi, _pd],
     "f_eval_densities": _BASIS + [_i, _pd, _i, _i, _pd, _pd, _i, _d],
     "f_eval_prim_density": [_i, _i, _i, _pi, _pd, _pd, _pd, _d, _pd],
 }
@@ -214,6 +216,21 @@ def set_metric_shift(shift):
 
 def set_skip_metric(skip):
     check(load().pa_set_skip_metric(int(bool(skip))))
+
+
+def set_class_timing(on):
+    """Serialize and time the three-center class launches (profiling aid)."""
+    check(load().pa_set_class_timing(int(bool(on))))
+
+
+def get_class_times():
+    """[(L_ab, L_c, ms)] of the class runs of the last single-molecule call in
+    class-timing mode."""
+    lib = load()
+    n = lib.pa_get_class_times(0, None, None, None)
+    lab, lc, ms = (ctypes.c_int * max(n, 1))(), (ctypes.c_int * max(n, 1))(), (ctypes.c_double * max(n, 1))()
+    lib.pa_get_class_times(n, lab, lc, ms)
+    return [(lab[i], lc[i], ms[i]) for i in range(n)]
 
 
 def get_stats():
