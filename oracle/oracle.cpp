@@ -95,10 +95,10 @@ void boys_exact(int nmax, double x, double* F) {
 }
 
 // Reference-compatible mode (common/integrals/boys.f90:22-97): table on
-// x_i = i * 0.01 (i = 0 .. 2710, boys.f90:213-221), 5-point Neville
-// interpolation through points i0 .. i0+4 with i0 = int(100 x) (:252-253), and
+// x_i = i * 0.01 (i = 0 .. 2710, boys.f90:22-30), 5-point Neville
+// interpolation through points i0 .. i0+4 with i0 = int(100 x) (:53-85), and
 // for x >= 27 the asymptotic formula (2n-1)!! / 2^(n+1) * sqrt(pi / x^(2n+1))
-// (:235-240, :279-288). The table is regenerated here (exact mode) instead of
+// (:44-49, switch at :88-97). The table is regenerated here (exact mode) instead of
 // being copied; the reference stores n <= 14 only, this table extends to
 // BOYS_NMAX so that high-L Schwarz integrals stay defined.
 constexpr int REF_NPTS = 2711;

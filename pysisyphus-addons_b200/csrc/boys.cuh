@@ -74,7 +74,7 @@ __device__ __forceinline__ double boys_exact_n(const double* __restrict__ tab, i
 __device__ __forceinline__ int boys_ref_weights(double T, double w[5]) {
   const int i0 = static_cast<int>(T * 100.0);
   double xs[5], d[5];
-  // The grid points are the rounded doubles i * 0.01 (boys.f90:221); __dmul_rn
+  // The grid points are the rounded doubles i * 0.01 (boys.f90:30); __dmul_rn
   // keeps the compiler from fusing the product into the later T - x subtraction.
 #pragma unroll
   for (int k = 0; k < 5; ++k) {
