@@ -202,19 +202,26 @@ __device__ __forceinline__ Real sph_row(const Real* R, int tx, int ty, int tz,
   return (static_cast<Real>(-0.0) + ... + sph_term<LC, M, Cs, Real>(R, tx, ty, tz));
 }
 
-// xr[m] += N_lc,m * sum_tau S_lc,m[tau] R[t + tau] (accumulated in FP64)
-template <int LC, class Real, int... Ms>
+// xr[m] (+)= N_lc,m * sum_tau S_lc,m[tau] R[t + tau] (in FP64). The first
+// auxiliary primitive stores (ACC = false), later ones accumulate: the X tile
+// needs no zeroing pass (fma(a, b, 0) and a * b round alike).
+template <int LC, class Real, bool ACC, int... Ms>
 __device__ __forceinline__ void sph_rows(const Real* R, int tx, int ty, int tz, double* xr,
                                          std::integer_sequence<int, Ms...>) {
-  ((xr[Ms] = fma(c_sph_rownorm[LC * LC + Ms],
-                 static_cast<double>(sph_row<LC, Ms, Real>(R, tx, ty, tz,
-                                                           std::make_integer_sequence<int, ncart(LC)>{})),
-                 xr[Ms])),
-   ...);
+  if constexpr (ACC)
+    ((xr[Ms] = fma(c_sph_rownorm[LC * LC + Ms],
+                   static_cast<double>(sph_row<LC, Ms, Real>(R, tx, ty, tz,
+                                                             std::make_integer_sequence<int, ncart(LC)>{})),
+                   xr[Ms])),
+     ...);
+  else
+    ((xr[Ms] = c_sph_rownorm[LC * LC + Ms] *
+               static_cast<double>(sph_row<LC, Ms, Real>(R, tx, ty, tz, std::make_integer_sequence<int, ncart(LC)>{}))),
+     ...);
 }
 
 // X rows of one triplet, per thread: rows t with t % TPT == part.
-template <int LAB, int LC, int TPT, class Real>
+template <int LAB, int LC, int TPT, class Real, bool ACC>
 __device__ __forceinline__ void x_rows_thread(const Real* R, double* xrow0, int mpad, int part) {
 #pragma unroll
   for (int tl = 0; tl <= LAB; ++tl)
@@ -225,8 +232,17 @@ __device__ __forceinline__ void x_rows_thread(const Real* R, double* xrow0, int 
         const int tz = tl - tx - ty;
         const int th = cidx(tx, ty, tz);
         if (th % TPT != part) continue;
-        sph_rows<LC, Real>(R, tx, ty, tz, xrow0 + th * mpad, std::make_integer_sequence<int, 2 * LC + 1>{});
+        sph_rows<LC, Real, ACC>(R, tx, ty, tz, xrow0 + th * mpad, std::make_integer_sequence<int, 2 * LC + 1>{});
       }
+}
+
+// Zeros the X rows of a screened triplet (per thread: rows t % TPT == part).
+template <int LAB, int LC, int TPT>
+__device__ __forceinline__ void x_rows_zero(double* xrow0, int mpad, int part) {
+#pragma unroll
+  for (int th = part; th < ncum(LAB); th += TPT)
+#pragma unroll
+    for (int m = 0; m < 2 * LC + 1; ++m) xrow0[th * mpad + m] = 0.0;
 }
 
 // X of one triplet by one thread (L <= 5): Boys, R in registers, solid harmonics.
@@ -252,7 +268,10 @@ __device__ __forceinline__ void x_triplet_thread(const Df3cArgs& a, double p, do
     }
     Real R[NR];
     hermite_R_thread<L, Real>(Rn, static_cast<Real>(X), static_cast<Real>(Y), static_cast<Real>(Z), R);
-    x_rows_thread<LAB, LC, TPT, Real>(R, xrow0, MPAD, part);
+    if (kp == 0)
+      x_rows_thread<LAB, LC, TPT, Real, false>(R, xrow0, MPAD, part);
+    else
+      x_rows_thread<LAB, LC, TPT, Real, true>(R, xrow0, MPAD, part);
   }
 }
 
@@ -289,37 +308,50 @@ __device__ __forceinline__ void x_triplet_team(const Df3cArgs& a, const uchar4* 
       }
     }
     __syncwarp();
-    // Hermite R, level by level
+    // Hermite R, level by level. The loops have compile-time trip counts and
+    // are unrolled: the components of one level are independent, so their
+    // descriptor and operand loads are issued back to back instead of one
+    // dependent load chain per component.
     {
       Real* top = (L & 1) ? b1 : b0;
       if (has && tl == 0) top[0] = Rn[L];
       __syncwarp();
+#pragma unroll
       for (int n = L - 1; n >= 0; --n) {
         Real* dst = (n & 1) ? b1 : b0;
         const Real* src = (n & 1) ? b0 : b1;
-        const int cnt = has ? ncum(L - n) : 0;
-        for (int idx = tl; idx < cnt; idx += TS) {
-          Real v;
-          if (idx == 0) {
-            v = Rn[n];
-          } else {
-            const int dsc = rdesc[idx];
-            const int d = rdesc_d(dsc), c = rdesc_c(dsc);
-            const Real xd = d == 0 ? Xr : (d == 1 ? Yr : Zr);
-            v = xd * src[rdesc_s1(dsc)];
-            if (c) v = fma(static_cast<Real>(c), src[rdesc_s2(dsc)], v);
+        const int cnt = ncum(L - n);
+#pragma unroll
+        for (int it = 0; it < (cnt + TS - 1) / TS; ++it) {
+          const int idx = tl + it * TS;
+          if (has && idx < cnt) {
+            Real v;
+            if (idx == 0) {
+              v = Rn[n];
+            } else {
+              const int dsc = rdesc[idx];
+              const int d = rdesc_d(dsc), c = rdesc_c(dsc);
+              const Real xd = d == 0 ? Xr : (d == 1 ? Yr : Zr);
+              v = xd * src[rdesc_s1(dsc)];
+              if (c) v = fma(static_cast<Real>(c), src[rdesc_s2(dsc)], v);
+            }
+            dst[idx] = v;
           }
-          dst[idx] = v;
         }
         __syncwarp();
       }
     }
     // X rows: lanes over the Hermite components t of the bra, compile-time
-    // solid-harmonic terms of the auxiliary shell
-    if (has) {
-      for (int t = tl; t < NH; t += TS) {
+    // solid-harmonic terms of the auxiliary shell (the first primitive stores)
+#pragma unroll
+    for (int it = 0; it < (NH + TS - 1) / TS; ++it) {
+      const int t = tl + it * TS;
+      if (has && t < NH) {
         const uchar4 e = txyz[t];
-        sph_rows<LC, Real>(b0, e.x, e.y, e.z, xrow + t * mpad, std::make_integer_sequence<int, 2 * LC + 1>{});
+        if (kp == 0)
+          sph_rows<LC, Real, false>(b0, e.x, e.y, e.z, xrow + t * mpad, std::make_integer_sequence<int, 2 * LC + 1>{});
+        else
+          sph_rows<LC, Real, true>(b0, e.x, e.y, e.z, xrow + t * mpad, std::make_integer_sequence<int, 2 * LC + 1>{});
       }
     }
     __syncwarp();
@@ -405,8 +437,10 @@ __device__ __forceinline__ void df3c_item(const Df3cArgs& a, int bx, int by, int
     npP = a.slot_pP[a.unit_slot0 + ub + tid];
   }
   for (int u0 = ub; u0 < ue && tile_n > 0; u0 += C::UB) {
-    __syncthreads();  // previous step's GEMM is done with Xs / Gs / unit data
-    // units of this step that can meet the tile: a prefix, units are sorted
+    // units of this step that can meet the tile: a prefix, units are sorted.
+    // The unit data written here were last read by the previous step's X
+    // build (before its closing barrier); the barrier of the count below
+    // orders the previous step's product before this step's writes to Xs / Gs.
     bool valid = false;
     if (tid < C::UB) {
       valid = u0 + tid < ue && nq * qc_max >= thr;
@@ -441,8 +475,10 @@ __device__ __forceinline__ void df3c_item(const Df3cArgs& a, int bx, int by, int
         Gs[r * kGStride + c] = 0.0;
       }
     }
-    // zero X
-    for (int i = tid; i < C::KP * C::MPAD; i += kThreads) Xs[i] = 0.0;
+    // (no zeroing pass over X: every triplet of a valid unit and auxiliary
+    // shell writes its rows below -- values, or zeros when screened; rows of
+    // invalid units meet zero G rows, and columns of shells past the tile end
+    // feed accumulator rows that are not written out)
     __syncthreads();
 
     // 2. X
@@ -453,12 +489,15 @@ __device__ __forceinline__ void df3c_item(const Df3cArgs& a, int bx, int by, int
         if (ci >= tile_n || ui >= nvalid) continue;
         const double4 cc = c_C[ci];
         const double est = triplet_estimate<LC>(a, u0 + ui, c0 + ci, u_Q[ui], cc);
-        if (est < thr) continue;
+        double* xrow0 = Xs + (ui * C::NH) * C::MPAD + ci * C::NC;
+        if (est < thr) {
+          x_rows_zero<LAB, LC, C::TPT>(xrow0, C::MPAD, part);
+          continue;
+        }
         const double4 up = u_pP[ui];
         const double p = up.x;
         const double X = up.y - cc.x, Y = up.z - cc.y, Z = up.w - cc.z;
         const int np = c_info[2 * ci], po = c_info[2 * ci + 1];
-        double* xrow0 = Xs + (ui * C::NH) * C::MPAD + ci * C::NC;
         if (est < a.thr32)
           x_triplet_thread<LAB, LC, C::NR, C::MPAD, C::TPT, float>(a, p, X, Y, Z, np, po, xrow0, part);
         else
@@ -487,6 +526,10 @@ __device__ __forceinline__ void df3c_item(const Df3cArgs& a, int bx, int by, int
       const double X = up.y - cc.x, Y = up.z - cc.y, Z = up.w - cc.z;
       const int np = active ? c_info[2 * ci] : 0, po = c_info[2 * ci + 1];
       double* xrow = Xs + (ui * C::NH) * C::MPAD + ci * C::NC;
+      if (valid && !active)  // screened: its X rows are zero
+        for (int t = tl; t < C::NH; t += C::TS)
+#pragma unroll
+          for (int m = 0; m < C::NC; ++m) xrow[t * C::MPAD + m] = 0.0;
       // FP32 recurrences only when every active team of the warp has a weak triplet
       const bool weak = !active || est < a.thr32;
       const bool f32 = __all_sync(0xffffffffu, weak) && __any_sync(0xffffffffu, active);
@@ -542,10 +585,19 @@ __device__ __forceinline__ void df3c_item(const Df3cArgs& a, int bx, int by, int
 // first (items are numbered with the bra-unit chunk slowest; units and aux
 // shells are sorted by Schwarz value, so early chunks and tiles carry the most
 // surviving triplets).
+// The X tile starts zeroed: entries that no step writes (padding rows and
+// columns) must be finite.
+template <int LAB, int LC>
+__device__ __forceinline__ void zero_x_tile(double* smem) {
+  using C = Cfg<LAB, LC>;
+  for (int i = threadIdx.x; i < C::KP * C::MPAD; i += blockDim.x) smem[i] = 0.0;
+}
+
 template <int LAB, int LC>
 __global__ void __launch_bounds__(kThreads, 2) k_df3c(Df3cArgs a) {
   extern __shared__ __align__(16) double smem[];
   __shared__ int s_item;
+  zero_x_tile<LAB, LC>(smem);
   for (;;) {
     __syncthreads();  // the previous item is done with shared memory and s_item
     if (threadIdx.x == 0) s_item = atomicAdd(a.counter, 1);
@@ -571,6 +623,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_df3c_batch(const Df3cArgs* __re
   __shared__ __align__(16) unsigned char s_raw[sizeof(Df3cArgs)];
   const Df3cArgs& sa = *reinterpret_cast<const Df3cArgs*>(s_raw);
   const int total = item_off[nm];
+  zero_x_tile<LAB, LC>(smem);
   for (;;) {
     __syncthreads();  // the previous item is done with shared memory and the descriptor
     if (threadIdx.x == 0) {
