@@ -252,6 +252,22 @@ int pa_metric(pa_basis aux, double* metric);
  * (n x nrhs) by L^-1 B. PA_ERR_NOT_SPD when A is not positive definite. */
 int pa_cholesky_solve(int n, double* A, int nrhs, double* B);
 
+/* The estimator study (replaces intor/benchmark_wrapper.f90:13-37,
+ * f_benchmark_int3c2e, same arguments): prints the basis sizes, the time and
+ * the number of shell triplets the QVL estimate skips, and writes
+ * int_estimates.bin (4 doubles per record) in the working directory.
+ * pa_int3c2e_estimates gives the records themselves: (schwarz_estimate,
+ * qvl_estimate, ||(ab|c)||_2, distance of the pair's contracted center to the
+ * auxiliary center) for every shell pair a >= b that is not concentric and
+ * whose Schwarz value exceeds 1e-10, and every auxiliary shell c, in the
+ * reference's loop order (intor/benchmark.f90:82-118); records == NULL
+ * returns only *nrecords and *nskipped (records with qvl_estimate < 1e-10). */
+int f_benchmark_int3c2e(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
+                        const double* bas_data, int nshells_aux, int ndata_aux, const int* bas_centers_aux,
+                        const int* bas_spec_aux, const double* bas_data_aux);
+int pa_int3c2e_estimates(pa_basis orbital, pa_basis aux, long long cap, double* records, long long* nrecords,
+                         long long* nskipped);
+
 /* Densities on grid points (replaces grid/grid_wrapper.f90:12-38,
  * f_eval_densities, same arguments): grid3d(3, npoints) column-major,
  * densities(ndens, nbfs, nbfs) Cartesian AO density matrices in pysisyphus

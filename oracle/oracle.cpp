@@ -1253,6 +1253,61 @@ void eval_prim_density(int nprims, int npoints, int nbfs, const int* ls_inds, co
   }
 }
 
+// benchmark_int3c2e (intor/benchmark.f90:15-132): for every shell pair a >= b
+// that is not concentric (|A - B| > 1e-6) and whose bra Schwarz value exceeds
+// 1e-10, and every auxiliary shell c, the record (schwarz_estimate,
+// qvl_estimate, ||(ab|c)||_2 over the block, |contracted center - C|) in the
+// reference's loop order; *nskipped counts records with qvl_estimate < 1e-10
+// (REAL(4) literal, promoted). Returns the number of records; writes at most
+// cap records.
+long long int3c2e_estimates(const OBasis& B, const OBasis& X, long long cap, double* rec, long long* nskipped) {
+  const int nsh = static_cast<int>(B.shells.size()), nsx = static_cast<int>(X.shells.size());
+  const std::vector<double> sbra = schwarz_bra(B);
+  const std::vector<double> saux = schwarz_aux(X);
+  const QvlScreener q = qvl_screener(B, X);
+  std::vector<std::pair<int, int>> pairs;
+  for (int a = 0; a < nsh; ++a)
+    for (int b = 0; b <= a; ++b) {
+      const OShell& sa = B.shells[a];
+      const OShell& sb = B.shells[b];
+      double d2 = 0.0;
+      for (int d = 0; d < 3; ++d) d2 += (sa.A[d] - sb.A[d]) * (sa.A[d] - sb.A[d]);
+      const bool concentric = std::sqrt(d2) <= 1e-6;
+      const bool small = sbra[static_cast<size_t>(a) * (a + 1) / 2 + b] <= 1e-10;
+      if (!concentric && !small) pairs.push_back({a, b});
+    }
+  const long long n = static_cast<long long>(pairs.size()) * nsx;
+  long long skipped = 0;
+#pragma omp parallel reduction(+ : skipped)
+  {
+    Workspace ws;
+    std::vector<double> blk;
+#pragma omp for schedule(dynamic)
+    for (long long r = 0; r < n; ++r) {
+      const int a = pairs[r / nsx].first, b = pairs[r / nsx].second, c = static_cast<int>(r % nsx);
+      const size_t k = static_cast<size_t>(a) * (a + 1) / 2 + b;
+      const double sch = sbra[k] * saux[c];
+      const double qvl = qvl_estimate(q, X, sbra, saux, a, b, c);
+      if (qvl < SCREEN_THRESH) ++skipped;
+      if (r >= cap) continue;
+      const OShell& sa = B.shells[a];
+      const OShell& sb = B.shells[b];
+      const OShell& sc = X.shells[c];
+      blk.assign(static_cast<size_t>(2 * sa.L + 1) * (2 * sb.L + 1) * (2 * sc.L + 1), 0.0);
+      eri_sph(sa, sb, sc, null_shell(sc), blk.data(), ws);
+      double ss = 0.0;
+      for (double v : blk) ss += v * v;
+      const double dx = q.cx[k] - sc.A[0], dy = q.cy[k] - sc.A[1], dz = q.cz[k] - sc.A[2];
+      rec[4 * r + 0] = sch;
+      rec[4 * r + 1] = qvl;
+      rec[4 * r + 2] = std::sqrt(ss);
+      rec[4 * r + 3] = std::sqrt(dx * dx + dy * dy + dz * dz);
+    }
+  }
+  *nskipped = skipped;
+  return n;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -1419,6 +1474,14 @@ void oracle_intor_df2c_mo(int nshells, int, const int* bc, const int* bs, const 
 }
 
 void oracle_last_stats(OracleStats* out) { *out = g_stats; }
+
+long long oracle_int3c2e_estimates(int nshells, int, const int* bc, const int* bs, const double* bd,
+                                   int nshells_aux, int, const int* bca, const int* bsa, const double* bda,
+                                   long long cap, double* records, long long* nskipped) {
+  const OBasis B = make_basis(nshells, bc, bs, bd);
+  const OBasis X = make_basis(nshells_aux, bca, bsa, bda);
+  return int3c2e_estimates(B, X, cap, records, nskipped);
+}
 
 void oracle_eval_densities(int nshells, int, const int* bc, const int* bs, const double* bd, int npoints,
                            const double* grid3d, int ndens, int nbfs, const double* densities,

@@ -114,6 +114,15 @@ double oracle_chol_backward_error_ld(int n, const double* M, const double* Lc);
 void oracle_eval_densities(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
                            const double* bas_data, int npoints, const double* grid3d, int ndens, int nbfs,
                            const double* densities, double* grid_densities, int blk_size, double thresh);
+/* Records of the estimator study benchmark_int3c2e (intor/benchmark.f90:15-132):
+ * (schwarz_estimate, qvl_estimate, ||(ab|c)||_2, distance) per non-concentric,
+ * non-small pair and auxiliary shell, in the reference's loop order. Returns
+ * their number; writes at most cap. */
+long long oracle_int3c2e_estimates(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
+                                   const double* bas_data, int nshells_aux, int ndata_aux,
+                                   const int* bas_centers_aux, const int* bas_spec_aux,
+                                   const double* bas_data_aux, long long cap, double* records,
+                                   long long* nskipped);
 /* Mirror of f_eval_prim_density (gdma/prim_dens.f90:100-259). */
 void oracle_eval_prim_density(int nprims, int npoints, int nbfs, const int* ls_inds, const double* primdata,
                               const double* coords3d, const double* P, double sw, double* rho);

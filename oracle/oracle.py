@@ -94,6 +94,9 @@ def lib():
     L.oracle_chol_solve_ld.restype = _i
     L.oracle_chol_backward_error_ld.argtypes = [_i, _pd, _pd]
     L.oracle_chol_backward_error_ld.restype = _d
+    L.oracle_int3c2e_estimates.argtypes = basis + basis + [ctypes.c_longlong, _pd,
+                                                           ctypes.POINTER(ctypes.c_longlong)]
+    L.oracle_int3c2e_estimates.restype = ctypes.c_longlong
     L.oracle_eval_densities.argtypes = basis + [_i, _pd, _i, _i, _pd, _pd, _i, _d]
     L.oracle_eval_prim_density.argtypes = [_i, _i, _i, _pi, _pd, _pd, _pd, _d, _pd]
     if os.environ.get("PA_ORACLE_NO_LAPACK", "0") != "1":
@@ -363,3 +366,16 @@ def eval_prim_density(Ls_inds, prim_data, coords3d, P_tot_cart, switch, rho_pseu
                                    _p(rho, ctypes.c_double))
     rho_pseudo[:] = rho
     return rho_pseudo
+
+
+def int3c2e_estimates(shells, shells_aux):
+    """(records (n, 4), nskipped) of the estimator study
+    (intor/benchmark.f90:15-132): schwarz_estimate, qvl_estimate, ||(ab|c)||_2
+    and the pair-center distance per record."""
+    k1, b1 = _basis_args(shells)
+    k2, b2 = _basis_args(shells_aux)
+    sk = ctypes.c_longlong()
+    n = lib().oracle_int3c2e_estimates(*b1, *b2, 0, None, ctypes.byref(sk))
+    rec = np.zeros((max(n, 1), 4))
+    lib().oracle_int3c2e_estimates(*b1, *b2, n, _p(rec, ctypes.c_double), ctypes.byref(sk))
+    return rec[:n], sk.value

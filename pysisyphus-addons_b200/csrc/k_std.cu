@@ -141,6 +141,30 @@ __global__ void __launch_bounds__(kStdThreads) k_std_df1c(StdArgs a, double* __r
   }
 }
 
+// ||(ab|c)||_2 of the block of pair rec_pair[blockIdx.y] and auxiliary shell
+// blockIdx.x (the estimator study of intor/benchmark.f90:96-118).
+__global__ void __launch_bounds__(kStdThreads) k_std_block_norm(StdArgs a, const int* __restrict__ rec_pair,
+                                                                int nx, double* __restrict__ out) {
+  __shared__ double scratch[kBlk3cDoubles];
+  __shared__ double s_red[kStdThreads / 32];
+  const int c = blockIdx.x, kp = blockIdx.y;
+  const int pair = rec_pair[kp];
+  Blk3cScratch s = blk3c_scratch(scratch);
+  block_3c(a, pair, c, s);
+  const int2 ab = a.pair_ab[pair];
+  const int n = (2 * a.B.shell[ab.x].x + 1) * (2 * a.B.shell[ab.y].x + 1) * (2 * a.X.shell[c].x + 1);
+  double ss = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) ss = fma(s.I[i], s.I[i], ss);
+  for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
+  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = ss;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < kStdThreads / 32; ++w) t += s_red[w];
+    out[static_cast<long long>(kp) * nx + c] = sqrt(t);
+  }
+}
+
 // One block per (aux shell c, target shell b, chunk of MOs).
 __global__ void __launch_bounds__(kStdThreads) k_std_df2c_half(StdArgs a, int c0, int k0, int nmos,
                                                                const double* __restrict__ mo,
@@ -246,6 +270,18 @@ int launch_std_df2c_half(const StdArgs& a, int c0, int c1, int k0, int nmos, con
   dim3 grid(c1 - c0, a.B.nshells, (nmos + moc - 1) / moc);
   k_std_df2c_half<<<grid, kStdThreads, smem, s>>>(a, c0, k0, nmos, mo, W, moc);
   return 1;
+}
+
+int launch_std_block_norms(const StdArgs& a, const int* rec_pair, int npairs, double* out, cudaStream_t s) {
+  if (npairs <= 0 || a.X.nshells == 0) return 0;
+  int done = 0;
+  for (int p0 = 0; p0 < npairs; p0 += 65535) {  // grid y limit
+    dim3 grid(a.X.nshells, std::min(65535, npairs - p0));
+    k_std_block_norm<<<grid, kStdThreads, 0, s>>>(a, rec_pair + p0, a.X.nshells,
+                                                 out + static_cast<long long>(p0) * a.X.nshells);
+    ++done;
+  }
+  return done;
 }
 
 int launch_std_pack(const double* Res, int nk, int nmos, int k0, int naux, double* Raw, cudaStream_t s) {

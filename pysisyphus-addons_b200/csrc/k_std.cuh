@@ -35,6 +35,10 @@ int launch_std_df2c_half(const StdArgs& a, int c0, int c1, int k0, int nmos, con
 int launch_std_pack(const double* Res, int nk, int nmos, int k0, int naux, double* Raw,
                     cudaStream_t s);
 
+// out[kp * nshells_aux + c] = ||(ab|c)||_2 for pair rec_pair[kp] (kp < npairs)
+// and every auxiliary shell c.
+int launch_std_block_norms(const StdArgs& a, const int* rec_pair, int npairs, double* out, cudaStream_t s);
+
 // out[i + rows * j] = in[j + cols * i] (out: rows x cols, column-major).
 int launch_transpose(const double* in, int rows, int cols, double* out, cudaStream_t s);
 

@@ -14,7 +14,9 @@
 #include <algorithm>
 #include <limits>
 #include <atomic>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -2078,6 +2080,168 @@ int pa_count_triplets(pa_basis orbital, pa_basis aux, long long* ntriplets, long
   g_stats.ntriplets = static_cast<long long>(orbital->pairs.npairs) * qc.size();
   g_stats.nskipped = g_stats.ntriplets - ncomp;
   g_stats.nints = ni;
+  return PA_OK;
+}
+
+// The estimator study of intor/benchmark.f90:15-132 (benchmark_int3c2e):
+// records (schwarz_estimate, qvl_estimate, ||(ab|c)||_2, |contracted center -
+// C|) for every shell pair a >= b that is not concentric (|A - B| > 1e-6) and
+// whose Schwarz value exceeds 1e-10, and every auxiliary shell c, in the
+// reference's loop order. The block norms come from explicit (ab|c) blocks on
+// the device (k_std_block_norm); the estimates are the screener's formulas
+// on the host. With records == nullptr only the counts are returned.
+int pa_int3c2e_estimates(pa_basis orbital, pa_basis aux, long long cap, double* records, long long* nrecords,
+                         long long* nskipped) {
+  int st = check_pair(orbital, aux);
+  if (st != PA_OK) return st;
+  if (orbital->host.shells.size() > 65535 && records)
+    return fail(PA_ERR_ARG, "more than 65535 orbital shells");
+  st = ensure_qvl(orbital);
+  if (st != PA_OK) return st;
+  const PairLists& P = orbital->pairs;
+  const HostBasis& B = orbital->host;
+  const HostBasis& X = aux->host;
+  const int nx = static_cast<int>(X.shells.size());
+  std::vector<double> qb(P.npairs), qc(nx);
+  st = schwarz_impl(orbital, aux, qb.data(), qc.data());
+  if (st != PA_OK) return st;
+  std::vector<int> keep;
+  for (int p = 0; p < P.npairs; ++p) {
+    const int2 ab = P.pair_ab[p];
+    const double* A = B.shells[ab.x].A;
+    const double* Bc = B.shells[ab.y].A;
+    const double d = std::sqrt((A[0] - Bc[0]) * (A[0] - Bc[0]) + (A[1] - Bc[1]) * (A[1] - Bc[1]) +
+                               (A[2] - Bc[2]) * (A[2] - Bc[2]));
+    if (d <= 1e-6 || qb[p] <= 1e-10) continue;  // benchmark.f90:88-93
+    keep.push_back(p);
+  }
+  const long long n = static_cast<long long>(keep.size()) * nx;
+  const double thr = static_cast<double>(1e-10f);  // benchmark.f90:100, REAL(4) literal
+  long long skipped = 0;
+  std::vector<double> est;
+  if (records) {
+    if (cap < n) return fail(PA_ERR_ARG, "records buffer holds " + std::to_string(cap) + " of " + std::to_string(n));
+    est.resize(static_cast<size_t>(3) * n);
+  }
+  for (size_t k = 0; k < keep.size(); ++k) {
+    const int p = keep[k];
+    const double4 pq = orbital->pair_qvl[p];
+    for (int c = 0; c < nx; ++c) {
+      const HostShell& sc = X.shells[c];
+      const double dx = pq.x - sc.A[0], dy = pq.y - sc.A[1], dz = pq.z - sc.A[2];
+      const double R = std::sqrt(dx * dx + dy * dy + dz * dz);
+      const double sch = qb[p] * qc[c];
+      double qvl = sch;  // qvl_estimate (common/screening.f90:267-299)
+      if (R > pq.w + aux->aux_qvl[c].x) {
+        double RL = R;
+        for (int l = 0; l < sc.L; ++l) RL *= R;
+        qvl = qb[p] * kPi * 1.4142135623730951 * aux->aux_qvl[c].y / (orbital->pair_den[p] * RL);
+      }
+      if (qvl < thr) ++skipped;
+      if (records) {
+        const size_t r = k * nx + c;
+        est[3 * r] = sch;
+        est[3 * r + 1] = qvl;
+        est[3 * r + 2] = R;
+      }
+    }
+  }
+  if (nrecords) *nrecords = n;
+  if (nskipped) *nskipped = skipped;
+  if (!records || n == 0) return PA_OK;
+  // block norms on the device
+  Ctx* c = nullptr;
+  DeviceTables dt;
+  st = current_ctx(&c, &dt);
+  if (st != PA_OK) return st;
+  std::lock_guard<std::mutex> lk(c->mu);
+  const Options o = options();
+  cudaStream_t s = c->stream;
+  Carver cnt;
+  double *Qab = nullptr, *esph = nullptr, *norms = nullptr;
+  double4* pP = nullptr;
+  int* d_keep = nullptr;
+  for (int pass = 0; pass < 2; ++pass) {
+    Carver cv;
+    if (pass == 1) {
+      PA_CUDA(c->arena.reserve(cnt.used));
+      cv.base = c->arena.base;
+    }
+    Qab = cv.take<double>(P.npairs);
+    pP = cv.take<double4>(P.nunits);
+    esph = cv.take<double>(P.esph_total);
+    d_keep = cv.take<int>(keep.size());
+    norms = cv.take<double>(n);
+    if (pass == 0) cnt = cv;
+  }
+  UnitArrays U;
+  U.unit_pair = orbital->d_unit_pair;
+  U.unit_prims = orbital->d_unit_prims;
+  U.unit_esph = orbital->d_unit_esph;
+  U.unit_pP = pP;
+  U.esph = esph;
+  int launches = launch_unit_setup(orbital->dev, orbital->d_pair_ab, orbital->d_class_unit, P, U, dt, s);
+  PA_CUDA(cudaMemcpyAsync(d_keep, keep.data(), sizeof(int) * keep.size(), cudaMemcpyHostToDevice, s));
+  StdArgs a;
+  a.B = orbital->dev;
+  a.X = aux->dev;
+  a.dt = dt;
+  a.boys_mode = o.boys_mode;
+  a.thresh = o.screen_thresh;
+  a.pair_ab = orbital->d_pair_ab;
+  a.pair_unit0 = orbital->d_pair_unit0;
+  a.unit_pP = pP;
+  a.esph = esph;
+  a.unit_esph = orbital->d_unit_esph;
+  a.Qab = Qab;
+  launches += launch_std_block_norms(a, d_keep, static_cast<int>(keep.size()), norms, s);
+  PA_CUDA(cudaGetLastError());
+  std::vector<double> h_norms(n);
+  PA_CUDA(cudaMemcpyAsync(h_norms.data(), norms, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  PA_CUDA(cudaStreamSynchronize(s));
+  for (long long r = 0; r < n; ++r) {
+    records[4 * r] = est[3 * r];
+    records[4 * r + 1] = est[3 * r + 1];
+    records[4 * r + 2] = h_norms[r];
+    records[4 * r + 3] = est[3 * r + 2];
+  }
+  g_stats = pa_stats{};
+  g_stats.kernel_launches = launches;
+  return PA_OK;
+}
+
+// f_benchmark_int3c2e (intor/benchmark_wrapper.f90:13-37): prints the basis
+// sizes, the time of the study and the number of triplets the QVL estimate
+// skips, and writes the records to int_estimates.bin in the working
+// directory (a stream of 4 doubles per record, benchmark.f90:117).
+int f_benchmark_int3c2e(int nshells, int ndata, const int* bas_centers, const int* bas_spec, const double* bas_data,
+                        int nshells_aux, int ndata_aux, const int* bas_centers_aux, const int* bas_spec_aux,
+                        const double* bas_data_aux) {
+  BasisGuard orb, aux;
+  int st = pa_basis_create(nshells, ndata, bas_centers, bas_spec, bas_data, PA_LMAX, &orb.b);
+  if (st != PA_OK) return st;
+  st = pa_basis_create(nshells_aux, ndata_aux, bas_centers_aux, bas_spec_aux, bas_data_aux, PA_LAUXMAX, &aux.b);
+  if (st != PA_OK) return st;
+  std::printf("Main basis:%6d shells, %6d basis functions\n", nshells, orb.b->host.nsph);
+  std::printf("Aux. basis:%6d shells, %6d basis functions\n", nshells_aux, aux.b->host.nsph);
+  const auto t0 = std::chrono::steady_clock::now();
+  long long n = 0, skipped = 0;
+  st = pa_int3c2e_estimates(orb.b, aux.b, 0, nullptr, &n, &skipped);
+  if (st != PA_OK) return st;
+  std::vector<double> rec(static_cast<size_t>(4) * std::max(n, 1LL));
+  st = pa_int3c2e_estimates(orb.b, aux.b, n, rec.data(), &n, &skipped);
+  if (st != PA_OK) return st;
+  const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  std::printf("Estimates and block norms took %8.4f s.\n", dt);
+  const long long ntrip = static_cast<long long>(nshells) * (nshells + 1) / 2 * nshells_aux;
+  std::printf("Skipped %12lld of %12lld integral triplets (%8.2f%%)\n", skipped, ntrip,
+              ntrip ? 100.0 * static_cast<double>(skipped) / static_cast<double>(ntrip) : 0.0);
+  std::fflush(stdout);
+  FILE* f = std::fopen("int_estimates.bin", "wb");
+  if (!f) return fail(PA_ERR_ARG, "cannot open int_estimates.bin for writing");
+  const size_t w = std::fwrite(rec.data(), sizeof(double), static_cast<size_t>(4) * n, f);
+  std::fclose(f);
+  if (w != static_cast<size_t>(4) * n) return fail(PA_ERR_ARG, "short write to int_estimates.bin");
   return PA_OK;
 }
 

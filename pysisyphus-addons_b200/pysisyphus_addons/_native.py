@@ -118,6 +118,9 @@ SIGNATURES = {
     "pa_df_solve": [_vp, _i, _vp, _vp, _i, _vp, _vp],
     "pa_set_class_timing": [_i],
     "pa_get_class_times": [_i, _pi, _pi, _pd],
+    "f_benchmark_int3c2e": _BASIS + _BASIS,
+    "pa_int3c2e_estimates": [_vp, _vp, ctypes.c_longlong, _pd, ctypes.POINTER(ctypes.c_longlong),
+                             ctypes.POINTER(ctypes.c_longlong)],
     "f_eval_densities": _BASIS + [_i, _pd, _i, _i, _pd, _pd, _i, _d],
     "f_eval_prim_density": [_i, _i, _i, _pi, _pd, _pd, _pd, _d, _pd],
 }
