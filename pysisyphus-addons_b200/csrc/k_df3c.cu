@@ -109,15 +109,33 @@ struct Cfg {
     return t;
   }
   static constexpr int TPT = kPerThread ? pick_tpt() : 1;
-  // team mode: team size is a power of two <= 32, so teams never straddle warps
+  // team mode: team size is a power of two; teams of up to 32 lanes share a
+  // warp, larger ones are whole warps synchronized by a named barrier
   static constexpr int pick_ts() {
     int t = 1;
-    while (t < 32 && 2 * t * NTRIP <= kThreads) t *= 2;
+    while (t < kThreads && 2 * t * NTRIP <= kThreads) t *= 2;
     return t;
   }
   static constexpr int TS = kPerThread ? 1 : pick_ts();
+  static_assert(TS <= 32 || TS % 32 == 0, "multi-warp teams are whole warps");
+  static_assert(TS <= 32 || kThreads / TS < 16, "named barrier ids 1..15");
+  // DMMA product: with fewer row tiles than warps, KSPLIT warps share a row
+  // tile and split its k range; their accumulators are summed once per item
+  static constexpr int KSPLIT = MT >= kWarps ? 1 : kWarps / MT;
   static constexpr int SMEM = smem_for(TC);
+  static_assert(KSPLIT == 1 || KSPLIT * MT * 320 <= KP * (MPAD + kGStride),
+                "k-split reduction fits in the X and G tiles");
 };
+
+// Barrier of one team of TS threads (team mode): the warp for teams of up to
+// 32 lanes, a named barrier (ids 1..15; 0 is __syncthreads) for larger teams.
+template <int TS>
+__device__ __forceinline__ void team_sync(int team) {
+  if constexpr (TS <= 32)
+    __syncwarp();
+  else
+    asm volatile("bar.sync %0, %1;\n" ::"r"(1 + team), "r"(TS) : "memory");
+}
 
 __device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
@@ -275,13 +293,14 @@ __device__ __forceinline__ void x_triplet_thread(const Df3cArgs& a, double p, do
   }
 }
 
-// X of one triplet by a team of TS lanes of one warp (L > 5): orders of the
-// Boys function across lanes, R level by level in shared memory, X rows across
-// the lanes. Every lane of the warp calls this with the same Real (the caller
-// makes the precision choice warp-uniform), so the warp barriers pair up.
+// X of one triplet by a team of TS threads (L > 5): orders of the Boys
+// function across lanes, R level by level in shared memory, X rows across the
+// lanes. Every thread of a warp (of a team, for teams larger than a warp)
+// calls this with the same Real (the caller makes the precision choice
+// uniform), so the team barriers pair up.
 template <int LAB, int LC, int TS, class Real>
 __device__ __forceinline__ void x_triplet_team(const Df3cArgs& a, const uchar4* txyz, const int* rdesc,
-                                               double* rbuf, int tl, bool active, int np, int po,
+                                               double* rbuf, int team, int tl, bool active, int np, int po,
                                                int maxprim, double p, double X, double Y, double Z,
                                                double* xrow, int mpad) {
   constexpr int L = LAB + LC;
@@ -307,7 +326,7 @@ __device__ __forceinline__ void x_triplet_team(const Df3cArgs& a, const uchar4* 
         Rn[n] = static_cast<Real>(f) * F(a.dt, n);
       }
     }
-    __syncwarp();
+    team_sync<TS>(team);
     // Hermite R, level by level. The loops have compile-time trip counts and
     // are unrolled: the components of one level are independent, so their
     // descriptor and operand loads are issued back to back instead of one
@@ -315,7 +334,7 @@ __device__ __forceinline__ void x_triplet_team(const Df3cArgs& a, const uchar4* 
     {
       Real* top = (L & 1) ? b1 : b0;
       if (has && tl == 0) top[0] = Rn[L];
-      __syncwarp();
+      team_sync<TS>(team);
 #pragma unroll
       for (int n = L - 1; n >= 0; --n) {
         Real* dst = (n & 1) ? b1 : b0;
@@ -338,7 +357,7 @@ __device__ __forceinline__ void x_triplet_team(const Df3cArgs& a, const uchar4* 
             dst[idx] = v;
           }
         }
-        __syncwarp();
+        team_sync<TS>(team);
       }
     }
     // X rows: lanes over the Hermite components t of the bra, compile-time
@@ -354,7 +373,7 @@ __device__ __forceinline__ void x_triplet_team(const Df3cArgs& a, const uchar4* 
           sph_rows<LC, Real, true>(b0, e.x, e.y, e.z, xrow + t * mpad, std::make_integer_sequence<int, 2 * LC + 1>{});
       }
     }
-    __syncwarp();
+    team_sync<TS>(team);
   }
 }
 
@@ -422,6 +441,10 @@ __device__ __forceinline__ void df3c_item(const Df3cArgs& a, int bx, int by, int
   const double thr = a.thresh;
   const IndexTables* it = a.dt.idx;
   const int g = lane >> 2, t4 = lane & 3;
+  // DMMA work of this warp: its first row tile and its k slice (warps past
+  // MT * KSPLIT get slice KSPLIT, which has no k steps)
+  const int mt0 = C::KSPLIT > 1 ? warp % C::MT : warp;
+  const int ks = C::KSPLIT > 1 ? warp / C::MT : 0;
 
   double acc[C::MTW][5][2];
 #pragma unroll
@@ -530,29 +553,31 @@ __device__ __forceinline__ void df3c_item(const Df3cArgs& a, int bx, int by, int
         for (int t = tl; t < C::NH; t += C::TS)
 #pragma unroll
           for (int m = 0; m < C::NC; ++m) xrow[t * C::MPAD + m] = 0.0;
-      // FP32 recurrences only when every active team of the warp has a weak triplet
+      // FP32 recurrences only when every active team of the warp has a weak
+      // triplet (a team larger than a warp has one triplet: uniform over it)
       const bool weak = !active || est < a.thr32;
       const bool f32 = __all_sync(0xffffffffu, weak) && __any_sync(0xffffffffu, active);
       if (f32)
-        x_triplet_team<LAB, LC, C::TS, float>(a, txyz, rdesc, rbuf, tl, active, np, po, maxprim, up.x, X, Y, Z,
-                                              xrow, C::MPAD);
+        x_triplet_team<LAB, LC, C::TS, float>(a, txyz, rdesc, rbuf, team, tl, active, np, po, maxprim, up.x, X, Y,
+                                              Z, xrow, C::MPAD);
       else
-        x_triplet_team<LAB, LC, C::TS, double>(a, txyz, rdesc, rbuf, tl, active, np, po, maxprim, up.x, X, Y,
-                                               Z, xrow, C::MPAD);
+        x_triplet_team<LAB, LC, C::TS, double>(a, txyz, rdesc, rbuf, team, tl, active, np, po, maxprim, up.x, X,
+                                               Y, Z, xrow, C::MPAD);
     }
     cp_async_commit_wait_all();
     __syncthreads();
 
-    // 3. acc[aux fn][d] += X^T G on the FP64 tensor cores
+    // 3. acc[aux fn][d] += X^T G on the FP64 tensor cores (warp w: row tiles
+    //    w, w + 8, ...; with KSPLIT > 1 row tile w % MT, k steps w / MT + KSPLIT j)
 #pragma unroll 2
-    for (int k4 = 0; k4 < C::KP / 4; ++k4) {
+    for (int k4 = ks < C::KSPLIT ? ks : C::KP / 4; k4 < C::KP / 4; k4 += C::KSPLIT) {
       const int kr = 4 * k4 + t4;
       double bf[5];
 #pragma unroll
       for (int n = 0; n < 5; ++n) bf[n] = n < nt_rt ? Gs[kr * kGStride + 8 * n + g] : 0.0;
 #pragma unroll
       for (int j = 0; j < C::MTW; ++j) {
-        const int mt = warp + kWarps * j;
+        const int mt = mt0 + kWarps * j;
         if (mt < C::MT) {
           const double av = Xs[kr * C::MPAD + 8 * mt + g];
 #pragma unroll
@@ -563,11 +588,35 @@ __device__ __forceinline__ void df3c_item(const Df3cArgs& a, int bx, int by, int
     }
   }
 
-  // partial[y][fn][d]
+  if constexpr (C::KSPLIT > 1) {
+    // sum the k slices of each row tile in a fixed order (slice 0 first),
+    // through the X and G tiles (contiguous; free once every warp is past its
+    // last product, and rewritten before they are read again)
+    __syncthreads();
+    if (ks < C::KSPLIT) {
+      double* red = Xs + (ks * C::MT + mt0) * 320;
+#pragma unroll
+      for (int n = 0; n < 5; ++n)
+#pragma unroll
+        for (int i = 0; i < 2; ++i) red[(2 * n + i) * 32 + lane] = acc[0][n][i];
+    }
+    __syncthreads();
+    if (ks == 0) {
+#pragma unroll
+      for (int n = 0; n < 5; ++n)
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          double v = Xs[mt0 * 320 + (2 * n + i) * 32 + lane];
+          for (int q = 1; q < C::KSPLIT; ++q) v += Xs[(q * C::MT + mt0) * 320 + (2 * n + i) * 32 + lane];
+          acc[0][n][i] = v;
+        }
+    }
+  }
+  // partial[y][fn][d] (with KSPLIT > 1 only the warps of slice 0 hold sums)
   double* out = a.partial + static_cast<long long>(by) * a.n_aux * C::NC * a.nd;
 #pragma unroll
   for (int j = 0; j < C::MTW; ++j) {
-    const int mt = warp + kWarps * j;
+    const int mt = (ks == 0 ? mt0 : C::MT) + kWarps * j;
     const int row = 8 * mt + g;
     if (mt >= C::MT || row >= C::M || row / C::NC >= tile_n) continue;
     const long long fn = static_cast<long long>(c0) * C::NC + row;
