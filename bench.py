@@ -113,6 +113,12 @@ def parse():
                     help="cfg4: one pa_df_4d call per molecule (the reference's way) instead of the batched form")
     ap.add_argument("--profile", action="store_true",
                     help="device steps only (for ncu): no e2e, CPU baseline, FP64 probe or clocks")
+    ap.add_argument("--std", action="store_true",
+                    help="the sTDDFT tensors instead (int_df1c, int_eri2c, int_df2c_mo over 20 occupied + 40 "
+                         "virtual orbitals) on the chosen workload; one step = the three tensors")
+    ap.add_argument("--grid", action="store_true",
+                    help="grid densities instead (f_eval_densities, one density on a cube grid of 64^3 points "
+                         "around the molecule, blk_size 100, thresh 1e-8); one step = one evaluation")
     a = ap.parse_args()
     if a.boys is None:
         a.boys = "exact" if a.config in SHIFTED else "reference"
@@ -340,6 +346,67 @@ def run_reference(args):
 
 
 
+def aux_bench(args):
+    """The adjacent paths: the sTDDFT tensors (--std) or grid densities (--grid)
+    on the workload's molecule, timed with CUDA events over whole calls of the
+    public functions (host arrays in and out: these paths have no device-buffer
+    entry points). One JSON line; the time per step is the metric."""
+    import torch
+
+    from pysisyphus_addons import _native as nat
+    from pysisyphus_addons.grid import grid
+    from pysisyphus_addons.std import intor as std
+
+    torch.cuda.set_device(0)
+    nat.set_boys_mode(args.boys)
+    nat.set_metric_shift(SHIFTED.get(args.config, 0.0))
+    w = workloads(args)[0]
+    if args.std:
+        C = np.asfortranarray(w.mo_coeffs[:, :60])  # 20 occupied + 40 virtual orbitals
+
+        def step():
+            std.int_df1c(w.shells, w.shells_aux)
+            std.int_eri2c(w.shells, w.shells_aux)
+            std.int_df2c_mo(w.shells, w.shells_aux, C)
+        metric, unit = "sTDDFT tensors (int_df1c + int_eri2c + int_df2c_mo, 20 occ + 40 virt MOs) per second", "sets/s"
+        cfg = {"workload": workload_config(args, [w])["workload"], "nmos": 60, "boys_mode": args.boys}
+    else:
+        rng = np.random.default_rng(0)
+        ncart = sum((s.L + 1) * (s.L + 2) // 2 for s in w.shells)
+        Cc = rng.normal(size=(ncart, 20)) / np.sqrt(ncart)
+        D = Cc @ Cc.T  # a symmetric positive semidefinite Cartesian density
+        C = np.array([s.center for s in w.shells])
+        lo, hi = C.min(0) - 3.0, C.max(0) + 3.0
+        axes = [np.linspace(lo[d], hi[d], 64) for d in range(3)]
+        X, Y, Z = np.meshgrid(*axes, indexing="ij")
+        pts = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
+
+        def step():
+            grid.eval_density(w.shells, pts, D)
+        metric, unit = "grid density points per second (f_eval_densities)", "points/s"
+        cfg = {"workload": workload_config(args, [w])["workload"] + "_grid64cube", "npoints": len(pts),
+               "ncart": ncart, "blk_size": 100, "thresh": 1e-8}
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if args.profile:
+        for _ in range(args.steps):
+            step()
+        torch.cuda.synchronize()
+        return
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / args.steps
+    units = 1.0 if args.std else float(cfg["npoints"])
+    line = {"metric": metric, "value": units / dt, "unit": unit, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)", "config": cfg,
+            "timing": "host wall clock around whole calls of the public host-array functions"}
+    print(json.dumps(line), flush=True)
+
+
 def precision_report(args):
     """Raw contraction, df = L^-1 raw and the Coulomb tensor of the FP64 path
     and of the precision form at several FP32 thresholds; max |difference| and
@@ -408,6 +475,9 @@ def main():
         return
     if args.precision_report:
         precision_report(args)
+        return
+    if args.std or args.grid:
+        aux_bench(args)
         return
     import torch
     import torch.distributed as dist
