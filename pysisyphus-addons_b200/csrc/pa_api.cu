@@ -370,6 +370,7 @@ struct Ctx {
   cudaEvent_t ev_alloc = nullptr, ev_copied = nullptr;
   // batched form: metric chains of different molecules on their own streams
   cudaStream_t smet[kNs3c] = {};
+  cudaStream_t sscrw[kNs3c] = {};  // batched form: screening + folding (highest priority)
   cudaEvent_t jmet[kNs3c] = {};
   // lookahead streams of the Cholesky factorization: la2 for the chains on
   // stream2 and for pa_cholesky_solve, la_met[i] for the chain on smet[i]
@@ -427,12 +428,16 @@ int current_ctx(Ctx** out, DeviceTables* dt) {
     for (int i = 0; i < Ctx::kNs3c; ++i) {
       PA_CUDA(cudaStreamCreateWithFlags(&c->s3c[i], cudaStreamNonBlocking));
       PA_CUDA(cudaEventCreateWithFlags(&c->j3c[i], cudaEventDisableTiming));
-      PA_CUDA(cudaStreamCreateWithPriority(&c->smet[i], cudaStreamNonBlocking, prio_hi));
+      // batched form: screening and folding at the highest priority, the
+      // metric chains one level below, the class kernels at the default (as
+      // in the single-molecule path)
+      PA_CUDA(cudaStreamCreateWithPriority(&c->smet[i], cudaStreamNonBlocking, prio_met));
+      PA_CUDA(cudaStreamCreateWithPriority(&c->sscrw[i], cudaStreamNonBlocking, prio_hi));
       PA_CUDA(cudaEventCreateWithFlags(&c->jmet[i], cudaEventDisableTiming));
     }
     for (int i = 0; i <= Ctx::kNs3c; ++i) {
       CholLookahead& la = i < Ctx::kNs3c ? c->la_met[i] : c->la2;
-      PA_CUDA(cudaStreamCreateWithPriority(&la.aux, cudaStreamNonBlocking, i < Ctx::kNs3c ? prio_hi : prio_met));
+      PA_CUDA(cudaStreamCreateWithPriority(&la.aux, cudaStreamNonBlocking, prio_met));
       PA_CUDA(cudaEventCreateWithFlags(&la.ev_panel, cudaEventDisableTiming));
       PA_CUDA(cudaEventCreateWithFlags(&la.ev_rest, cudaEventDisableTiming));
     }
@@ -1162,20 +1167,22 @@ int record_batch(Ctx* c, BatchPlan& plan, const std::vector<BatchMol>& mols, con
   constexpr int W = Ctx::kNs3c;
   PA_CUDA(cudaEventRecord(c->fork, s));
   for (int i = 0; i < W; ++i) {
-    PA_CUDA(cudaStreamWaitEvent(c->s3c[i], c->fork, 0));
+    PA_CUDA(cudaStreamWaitEvent(c->sscrw[i], c->fork, 0));
     PA_CUDA(cudaStreamWaitEvent(c->smet[i], c->fork, 0));
   }
-  // per molecule: metric chain on a metric stream, screening + folding on a worker
+  // per molecule: screening + folding on a screening worker (enqueued first:
+  // the critical path), then the metric chain on a metric stream
   for (int m = 0; m < nmol; ++m) {
     const BatchMol& M = mols[m];
     DfBuffers& b = plan.bufs[m];
-    stage_metric(M.aux, b, dt, o, c->smet[m % W], &c->la_met[m % W], launches);
-    const int st = run_screening(M.orb, M.aux, dt, o, b, c->s3c[m % W], launches);
+    const int st = run_screening(M.orb, M.aux, dt, o, b, c->sscrw[m % W], launches);
     if (st != PA_OK) return st;
-    stage_bra_prep(M.orb, M.aux, M.nd, M.dens, M.sd, M.si, M.sj, b, o, c->s3c[m % W], launches);
+    stage_bra_prep(M.orb, M.aux, M.nd, M.dens, M.sd, M.si, M.sj, b, o, c->sscrw[m % W], launches);
   }
+  for (int m = 0; m < nmol; ++m)
+    stage_metric(mols[m].aux, plan.bufs[m], dt, o, c->smet[m % W], &c->la_met[m % W], launches);
   for (int i = 0; i < W; ++i) {
-    PA_CUDA(cudaEventRecord(c->j3c[i], c->s3c[i]));
+    PA_CUDA(cudaEventRecord(c->j3c[i], c->sscrw[i]));
     PA_CUDA(cudaStreamWaitEvent(s, c->j3c[i], 0));
   }
   // one persistent launch per class over all molecules
@@ -1284,8 +1291,10 @@ int batch_4d(int nmol, const pa_basis* orbs, const pa_basis* auxs, const int* nd
     // classes present in the batch, and for each the molecules' runs
     std::vector<int> class_lab, class_lc, class_nm, class_items;
     std::vector<std::vector<std::pair<int, int>>> class_runs;  // (molecule, run index)
-    for (int lab = 0; lab <= 2 * PA_LMAX; ++lab)
-      for (int lc = 0; lc <= PA_LAUXMAX; ++lc) {
+    // classes grouped by auxiliary L, highest first (as the single-molecule
+    // path orders its class launches)
+    for (int lc = PA_LAUXMAX; lc >= 0; --lc)
+      for (int lab = 0; lab <= 2 * PA_LMAX; ++lab) {
         class_lab.push_back(lab);
         class_lc.push_back(lc);
         class_runs.emplace_back();
@@ -1370,7 +1379,9 @@ int batch_4d(int nmol, const pa_basis* orbs, const pa_basis* auxs, const int* nd
         if (st != PA_OK) return st;
         return fail(PA_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
       }
-      const cudaError_t ei = cudaGraphInstantiate(&plan->exec, graph, 0);
+      // node priorities from the capturing streams (screening and metric
+      // chains ahead of the persistent class kernels)
+      const cudaError_t ei = cudaGraphInstantiateWithFlags(&plan->exec, graph, cudaGraphInstantiateFlagUseNodePriority);
       cudaGraphDestroy(graph);
       if (ei != cudaSuccess) {
         c->plan = nullptr;
