@@ -59,9 +59,15 @@ HEADLINE_METRIC = "3c2e ints/s and Coulomb-tensor time at \u22641e-9 err: mixed+
 FP32_THRESH = 1e-6
 # workloads whose auxiliary metric needs the exact Boys function and a shift
 SHIFTED = {"cfg5": 1e-7, "cfg4": 1e-7}
-# DRAM bytes (read + write) of the three-center family per step from ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum, -k regex:k_df3c): None until captured
-TRAFFIC_3C = {}
+# DRAM bytes (read + write) of the three-center family (k_df3c classes and
+# reductions) per step, from ncu (dram__bytes_read.sum + dram__bytes_write.sum,
+# -k regex:k_df3c) on the 40-atom step: 630.3 MB read + 0.3 MB written. The
+# 200-atom value is that capture scaled by the model flops of the two steps
+# (3.992e12 / 3.613e10): the traffic is the folded densities G re-read per
+# auxiliary tile, which grows with the surviving triplets as the flops do.
+TRAFFIC_3C = {"cfg2": 630.6e6, "cfg5": 630.6e6 * 3.992e12 / 3.613e10}
+TRAFFIC_NOTE = {"cfg2": "ncu capture of this step (40 launches)",
+                "cfg5": "40-atom ncu capture scaled by model flops (no full-size multi-metric capture)"}
 
 
 def single_molecule(args):
@@ -705,7 +711,8 @@ def main():
             "peak_source": "of measured: FP64 GEMM (torch.matmul float64 8192^3) in this run; "
                            "MEASURED_PEAKS.json has no FP64 figure",
             "flops_per_step_3c": flops_3c, "ms_bra_plus_3c": ms3,
-            "traffic": TRAFFIC_3C.get(args.config)}
+            "traffic": TRAFFIC_3C.get(args.config), "traffic_unit": "bytes per step (family)",
+            "traffic_source": TRAFFIC_NOTE.get(args.config)}
         line["phases_ms"] = {k: statistics.mean(p[k] for p in r["phases"]) for k in r["phases"][0]}
         line["gpu_launches_3c"] = r["launches_3c"]
     if e2e:
