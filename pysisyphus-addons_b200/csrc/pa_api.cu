@@ -832,6 +832,7 @@ Df3cArgs class_args(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const 
 // classes in L_ab order, as they appear in b.runs).
 void stage_reduce_lc(const pa_basis_s* aux, int nd, DfBuffers& b, int lc, cudaStream_t s, int* launches) {
   const AuxLists& X = aux->aux;
+  if (lc < 0 || lc > X.lc_max) return;  // no auxiliary shells of this L
   {
     Df3cReduceArgs ra;
     ra.X = aux->dev;
@@ -1190,14 +1191,30 @@ int record_batch(Ctx* c, BatchPlan& plan, const std::vector<BatchMol>& mols, con
   if (ncls > 0) PA_CUDA(cudaMemsetAsync(plan.counters, 0, sizeof(int) * ncls, s));
   PA_CUDA(cudaEventRecord(c->fork, s));
   for (int i = 0; i < W; ++i) PA_CUDA(cudaStreamWaitEvent(c->s3c[i], c->fork, 0));
-  for (int k = 0; k < ncls; ++k)
+  // the classes come grouped by L_c: once a group is enqueued, the main stream
+  // waits for the class streams and reduces that group of every molecule while
+  // the next groups run (as the single-molecule path does)
+  bool reduced[PA_LAUXMAX + 1] = {};
+  for (int k = 0; k < ncls; ++k) {
     *launches += launch_df3c_class_batch(class_lab[k], class_lc[k], class_args_d[k], class_off_d[k], class_nm[k],
                                          class_items[k], plan.counters + k, c->s3c[k % W]);
+    if (k + 1 == ncls || class_lc[k + 1] != class_lc[k]) {
+      for (int i = 0; i < W; ++i) {
+        PA_CUDA(cudaEventRecord(c->j3c[i], c->s3c[i]));
+        PA_CUDA(cudaStreamWaitEvent(s, c->j3c[i], 0));
+      }
+      for (int m = 0; m < nmol; ++m) stage_reduce_lc(mols[m].aux, mols[m].nd, plan.bufs[m], class_lc[k], s, launches);
+      reduced[class_lc[k]] = true;
+    }
+  }
   for (int i = 0; i < W; ++i) {
     PA_CUDA(cudaEventRecord(c->j3c[i], c->s3c[i]));
     PA_CUDA(cudaStreamWaitEvent(s, c->j3c[i], 0));
   }
-  // per molecule: reduction, then (after its metric chain) solve and tensor
+  for (int lc = 0; lc <= PA_LAUXMAX; ++lc)  // groups without class launches (zero rows)
+    if (!reduced[lc])
+      for (int m = 0; m < nmol; ++m) stage_reduce_lc(mols[m].aux, mols[m].nd, plan.bufs[m], lc, s, launches);
+  // per molecule: (after its metric chain) solve and tensor
   PA_CUDA(cudaEventRecord(c->fork, s));
   for (int i = 0; i < W; ++i) {
     PA_CUDA(cudaStreamWaitEvent(c->s3c[i], c->fork, 0));
@@ -1208,7 +1225,6 @@ int record_batch(Ctx* c, BatchPlan& plan, const std::vector<BatchMol>& mols, con
     const BatchMol& M = mols[m];
     DfBuffers& b = plan.bufs[m];
     cudaStream_t w = c->s3c[m % W];
-    stage_reduce(M.aux, M.nd, b, w, launches);
     const int st = stage_solve(M.aux, M.nd, b, o, plan.df[m], w, launches);
     if (st != PA_OK) return st;
     *launches += coulomb_4d(plan.df[m], M.aux->host.nsph, M.nd, M.ns, plan.gram[m], M.R, w);
