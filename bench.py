@@ -143,6 +143,21 @@ def workloads(args, rank=0):
     return [config_workload(args.config, seed=rank)]
 
 
+def tile_report():
+    """Which tile-shape variants the three-center classes ran in (the table
+    the library applied at start-up, pysisyphus_addons.tune)."""
+    from pysisyphus_addons import _native as nat
+
+    off = {f"{a},{b}": v for a in range(2 * nat.LMAX + 1) for b in range(nat.LAUXMAX + 1)
+           if (v := nat.get_tile_variant(a, b)) != 0}
+    src = os.environ.get("PA_B200_TILE_TABLE")
+    if src is None:
+        table = Path(nat.LIB_PATH).resolve().parent / "df3c_tiles.txt"
+        src = str(table.relative_to(ROOT)) if table.exists() and table.is_relative_to(ROOT) else (
+            str(table) if table.exists() else "none (default shapes)")
+    return {"table": src or "none (default shapes)", "classes_off_default": off}
+
+
 def workload_config(args, ws):
     """The `config` object; both arms (ours and --impl reference) print the same one."""
     from pysisyphus_addons.common.synthetic import CONFIGS
@@ -693,6 +708,7 @@ def main():
     }
     if world > 1:
         line["ranks"] = f"independent molecules x{world} (seed = rank)"
+    line["tiles"] = tile_report()
     if form_report:
         line["forms"] = form_report
     # roofline of the three-center family, timed in the plain form (its phase

@@ -184,6 +184,27 @@ int pa_get_stats(pa_stats* out);
  * entries) and returns their number. */
 int pa_set_class_timing(int on);
 int pa_get_class_times(int cap, int* lab, int* lc, double* ms);
+/* Tile-shape variants of the three-center class kernels (no counterpart in
+ * the reference; its OpenMP loop has no tiles). Each class (L_ab = la + lb in
+ * 0..2*PA_LMAX_ORBITAL, L_c in 0..PA_LMAX_AUX) has variants 0..PA_TILE_VARIANTS-1:
+ *   0: the largest auxiliary tile that fits two blocks per SM (default);
+ *   1: the tile, at least half as large, that keeps the most lanes of the
+ *      block busy while the integrals are built;
+ *   2: three blocks per SM for classes with L_ab + L_c > 5.
+ * Results agree to rounding between variants. The selection is process-wide
+ * and read at the start of each call. pa_tile_shape gives, for one variant,
+ * out[0] = auxiliary shells per tile, out[1] = bra units per step, out[2] =
+ * lanes per triplet, out[3] = blocks per SM, out[4] = shared memory bytes per
+ * block. pa_load_tile_table applies a table of "L_ab L_c variant" lines (#
+ * comments; NULL = the default table); the library applies its default table
+ * once per process before the first call: $PA_B200_TILE_TABLE when set (empty
+ * = none), else df3c_tiles.txt beside the library, when present. The package's
+ * autotuner (pysisyphus_addons.tune) writes such tables. */
+#define PA_TILE_VARIANTS 3
+int pa_set_tile_variant(int lab, int lc, int variant);
+int pa_get_tile_variant(int lab, int lc, int* variant);
+int pa_tile_shape(int lab, int lc, int variant, int* out);
+int pa_load_tile_table(const char* path, int* napplied);
 
 /* Device-resident path. A pa_basis holds an unpacked, normalized basis on the
  * host and its copy in device memory of the current device. */

@@ -1,712 +1,15 @@
-// Screened three-center contraction df[P][d] = sum_(a>=b) sum_(i in a, j in b)
-// (ij|P) [D_d(i,j) + (a != b) D_d(j,i)]  -- the hot loop of
-// contract_coulomb_densities_2d (diabatization/intor.f90:108-183).
-//
-// Formulation (McMurchie-Davidson with the density folded into the bra):
-//   df[P,m][d] += sum_tuv X_(u,P)[tuv][m] G_u[tuv][d]
-//   X_(u,P)[tuv][m] = pref(u,P) sum_(|tau|=lc) S_lc,m[tau] R_(tuv+tau)(alpha, P_u - C_P)
-// where u is a primitive pair ("bra unit") of a surviving shell pair, G_u its
-// density-folded Hermite expansion (k_bra_prep) and S the solid harmonic
-// coefficients of the auxiliary shell (Hobson's theorem: only Hermite
-// components of degree exactly lc appear on the auxiliary side).
-//
-// One kernel instance per class (LAB = la + lb, LC = l_aux). Bra units and
-// auxiliary shells are sorted by Schwarz value (descending) within their class,
-// so the surviving triplets Q_ab * Q_c >= threshold form a staircase: a block
-// stops at the first unit failing against the largest auxiliary shell of its
-// tile, and individual triplets below the threshold contribute exactly zero, as
-// the reference skips them (schwarz_estimate < 1e-10 -> cycle).
-//
-// A block (8 warps; two blocks per SM) owns a tile of TC auxiliary shells and a density chunk of
-// up to 40 columns, and walks a range of bra units, UB units per step:
-//   1. cp.async stages G of the UB units (one contiguous range) into shared
-//      memory while
-//   2. X of the UB x TC triplets is built into shared memory: the Boys function,
-//      the Hermite recurrence for R and the solid-harmonic contraction --
-//      per thread with R in registers and compile-time indices for L <= 5, by
-//      thread teams with R in shared memory above;
-//   3. the update acc[aux fn][d] += X^T G runs on the FP64 tensor cores
-//      (mma.sync m8n8k4 f64), accumulators in registers.
-// Each block writes its partial sums to a per-chunk slab; k_df3c_reduce sums the
-// slabs in a fixed order (deterministic results, no atomics).
-#include "boys.cuh"
+// Host side of the screened three-center contraction: the run-time dispatch
+// over (LAB, LC, tile-shape variant) to the class kernels (k_df3c_impl.cuh,
+// one translation unit per LAB), the per-class variant table, and the ordered
+// reduction of the per-chunk partial slabs.
 #include "k_df3c.cuh"
-#include "md.cuh"
-#include "sph_raw.cuh"
 
 #include <algorithm>
-#include <utility>
+#include <mutex>
 
 namespace pa {
 
 namespace {
-
-struct BlockSync {
-  __device__ void operator()() const { __syncthreads(); }
-};
-
-constexpr int kThreads = 256;
-constexpr int kWarps = kThreads / 32;
-constexpr int kSmemBudget = 110 * 1024 / 8;  // doubles (two blocks per SM)
-constexpr int kGStride = 44;                 // shared-memory row stride of G (>= 40, = 4 mod 16)
-
-__constant__ double c_sph_dense[1024];  // solid harmonics, row (l, m) at c_sph_off[l] + m * ncart(l)
-__constant__ int c_sph_off[PA_LAUXMAX + 2];
-__constant__ double c_sph_rownorm[(PA_LAUXMAX + 1) * (PA_LAUXMAX + 1)];  // [l*l + m + l]
-
-constexpr int round_up(int x, int m) { return (x + m - 1) / m * m; }
-// row stride = 4 (mod 16) doubles: conflict-free m8n8k4 fragment loads
-constexpr int pad_stride(int mp) { return mp + ((20 - mp % 16) % 16); }
-
-template <int LAB, int LC>
-struct Cfg {
-  static constexpr int NH = ncum(LAB);
-  static constexpr int NC = 2 * LC + 1;
-  static constexpr int NCC = ncart(LC);
-  static constexpr int L = LAB + LC;
-  static constexpr int NR = ncum(L);
-  static constexpr bool kPerThread = (L <= 5);
-  static constexpr int pick_ub(int tc) {
-    if (kPerThread) {
-      int ub = 64 / NH;
-      if (ub < 1) ub = 1;
-      if (ub * tc > 512) ub = 512 / tc;
-      return ub < 1 ? 1 : ub;
-    }
-    int ub = 40 / NH;
-    if (ub < 1) ub = 1;
-    if (ub * tc > 64) ub = 64 / tc;
-    return ub < 1 ? 1 : ub;
-  }
-  static constexpr int smem_for(int tc) {
-    const int ub = pick_ub(tc);
-    const int kp = round_up(ub * NH, 4);
-    const int mpad = pad_stride(round_up(tc * NC, 8));
-    const int team = kPerThread ? 0 : ub * tc * (2 * NR + 16) + 2 * NR;
-    return kp * mpad + kp * kGStride + team + 1024;
-  }
-  static constexpr int pick_tc() {
-    int tc = 128 / NC;
-    if (tc > 128) tc = 128;
-    if (!kPerThread && tc > 32) tc = 32;
-    while (tc > 1 && smem_for(tc) > kSmemBudget) --tc;
-    return tc;
-  }
-  static constexpr int TC = pick_tc();
-  static constexpr int UB = pick_ub(TC);
-  static constexpr int M = TC * NC;
-  static constexpr int MP = round_up(M, 8);
-  static constexpr int MPAD = pad_stride(MP);
-  static constexpr int MT = MP / 8;                 // m8n8k4 row tiles
-  static constexpr int MTW = (MT + kWarps - 1) / kWarps;
-  static constexpr int K = UB * NH;
-  static constexpr int KP = round_up(K, 4);
-  static constexpr int NTRIP = UB * TC;
-  // per-thread mode: threads per triplet (power of two, warp-uniform split of t)
-  static constexpr int pick_tpt() {
-    int t = 1;
-    while (t < 8 && 2 * t * NTRIP <= kThreads) t *= 2;
-    return t;
-  }
-  static constexpr int TPT = kPerThread ? pick_tpt() : 1;
-  // team mode: team size is a power of two; teams of up to 32 lanes share a
-  // warp, larger ones are whole warps synchronized by a named barrier
-  static constexpr int pick_ts() {
-    int t = 1;
-    while (t < kThreads && 2 * t * NTRIP <= kThreads) t *= 2;
-    return t;
-  }
-  static constexpr int TS = kPerThread ? 1 : pick_ts();
-  static_assert(TS <= 32 || TS % 32 == 0, "multi-warp teams are whole warps");
-  static_assert(TS <= 32 || kThreads / TS < 16, "named barrier ids 1..15");
-  // DMMA product: with fewer row tiles than warps, KSPLIT warps share a row
-  // tile and split its k range; their accumulators are summed once per item
-  static constexpr int KSPLIT = MT >= kWarps ? 1 : kWarps / MT;
-  static constexpr int SMEM = smem_for(TC);
-  static_assert(KSPLIT == 1 || KSPLIT * MT * 320 <= KP * (MPAD + kGStride),
-                "k-split reduction fits in the X and G tiles");
-};
-
-// Barrier of one team of TS threads (team mode): the warp for teams of up to
-// 32 lanes, a named barrier (ids 1..15; 0 is __syncthreads) for larger teams.
-template <int TS>
-__device__ __forceinline__ void team_sync(int team) {
-  if constexpr (TS <= 32)
-    __syncwarp();
-  else
-    asm volatile("bar.sync %0, %1;\n" ::"r"(1 + team), "r"(TS) : "memory");
-}
-
-__device__ __forceinline__ void dmma_m8n8k4(double& d0, double& d1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-               : "+d"(d0), "+d"(d1)
-               : "d"(a), "d"(b));
-}
-
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
-  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src));
-}
-__device__ __forceinline__ void cp_async_commit_wait_all() {
-  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::);
-}
-
-// Per-thread Hermite R (small L): in-place level recursion in registers.
-template <int L, class Real>
-__device__ __forceinline__ void hermite_R_thread(const Real* Rn, Real X, Real Y, Real Z, Real* R) {
-  R[0] = Rn[L];
-#pragma unroll
-  for (int n = L - 1; n >= 0; --n) {
-#pragma unroll
-    for (int deg = L - n; deg >= 1; --deg) {
-#pragma unroll
-      for (int t = deg; t >= 0; --t) {
-#pragma unroll
-        for (int u = deg - t; u >= 0; --u) {
-          const int v = deg - t - u;
-          Real val;
-          if (t > 0) {
-            val = X * R[cidx(t - 1, u, v)];
-            if (t > 1) val = fma(static_cast<Real>(t - 1), R[cidx(t - 2, u, v)], val);
-          } else if (u > 0) {
-            val = Y * R[cidx(0, u - 1, v)];
-            if (u > 1) val = fma(static_cast<Real>(u - 1), R[cidx(0, u - 2, v)], val);
-          } else {
-            val = Z * R[cidx(0, 0, v - 1)];
-            if (v > 1) val = fma(static_cast<Real>(v - 1), R[cidx(0, 0, v - 2)], val);
-          }
-          R[cidx(t, u, v)] = val;
-        }
-      }
-    }
-    R[0] = Rn[n];
-  }
-}
-
-// Decoded local Cartesian index c of degree l (x^l, x^(l-1) y, ...), compile time.
-__host__ __device__ constexpr int cart_x(int l, int c) {
-  int i = l, k = c;
-  while (k > l - i) {
-    k -= l - i + 1;
-    --i;
-  }
-  return i;
-}
-__host__ __device__ constexpr int cart_y(int l, int c) {
-  int i = l, k = c;
-  while (k > l - i) {
-    k -= l - i + 1;
-    --i;
-  }
-  return l - i - k;
-}
-
-// One solid-harmonic term w * R[t + tau] with w a compile-time constant (the
-// term vanishes at compile time when w == 0). Real is double, or float for the
-// FP32 recurrences of weak triplets.
-template <int LC, int M, int C, class Real>
-__device__ __forceinline__ Real sph_term(const Real* R, int tx, int ty, int tz) {
-  constexpr int ax = cart_x(LC, C), ay = cart_y(LC, C), az = LC - ax - ay;
-  constexpr double w = sph_raw(LC, M - LC, ax, ay, az);
-  if constexpr (w != 0.0)
-    return static_cast<Real>(w) * R[cidx(tx + ax, ty + ay, tz + az)];
-  else
-    return static_cast<Real>(-0.0);  // x + (-0.0) == x exactly, so the compiler drops the term
-}
-
-template <int LC, int M, class Real, int... Cs>
-__device__ __forceinline__ Real sph_row(const Real* R, int tx, int ty, int tz,
-                                        std::integer_sequence<int, Cs...>) {
-  return (static_cast<Real>(-0.0) + ... + sph_term<LC, M, Cs, Real>(R, tx, ty, tz));
-}
-
-// xr[m] (+)= N_lc,m * sum_tau S_lc,m[tau] R[t + tau] (in FP64). The first
-// auxiliary primitive stores (ACC = false), later ones accumulate: the X tile
-// needs no zeroing pass (fma(a, b, 0) and a * b round alike).
-template <int LC, class Real, bool ACC, int... Ms>
-__device__ __forceinline__ void sph_rows(const Real* R, int tx, int ty, int tz, double* xr,
-                                         std::integer_sequence<int, Ms...>) {
-  if constexpr (ACC)
-    ((xr[Ms] = fma(c_sph_rownorm[LC * LC + Ms],
-                   static_cast<double>(sph_row<LC, Ms, Real>(R, tx, ty, tz,
-                                                             std::make_integer_sequence<int, ncart(LC)>{})),
-                   xr[Ms])),
-     ...);
-  else
-    ((xr[Ms] = c_sph_rownorm[LC * LC + Ms] *
-               static_cast<double>(sph_row<LC, Ms, Real>(R, tx, ty, tz, std::make_integer_sequence<int, ncart(LC)>{}))),
-     ...);
-}
-
-// X rows of one triplet, per thread: rows t with t % TPT == part.
-template <int LAB, int LC, int TPT, class Real, bool ACC>
-__device__ __forceinline__ void x_rows_thread(const Real* R, double* xrow0, int mpad, int part) {
-#pragma unroll
-  for (int tl = 0; tl <= LAB; ++tl)
-#pragma unroll
-    for (int tx = tl; tx >= 0; --tx)
-#pragma unroll
-      for (int ty = tl - tx; ty >= 0; --ty) {
-        const int tz = tl - tx - ty;
-        const int th = cidx(tx, ty, tz);
-        if (th % TPT != part) continue;
-        sph_rows<LC, Real, ACC>(R, tx, ty, tz, xrow0 + th * mpad, std::make_integer_sequence<int, 2 * LC + 1>{});
-      }
-}
-
-// Zeros the X rows of a screened triplet (per thread: rows t % TPT == part).
-template <int LAB, int LC, int TPT>
-__device__ __forceinline__ void x_rows_zero(double* xrow0, int mpad, int part) {
-#pragma unroll
-  for (int th = part; th < ncum(LAB); th += TPT)
-#pragma unroll
-    for (int m = 0; m < 2 * LC + 1; ++m) xrow0[th * mpad + m] = 0.0;
-}
-
-// X of one triplet by one thread (L <= 5): Boys, R in registers, solid harmonics.
-template <int LAB, int LC, int NR, int MPAD, int TPT, class Real>
-__device__ __forceinline__ void x_triplet_thread(const Df3cArgs& a, double p, double X, double Y,
-                                                 double Z, int np, int po, double* xrow0, int part) {
-  constexpr int L = LAB + LC;
-  const double RPC2 = X * X + Y * Y + Z * Z;
-  for (int kp = 0; kp < np; ++kp) {
-    const double2 gp = a.X.prim[po + kp];
-    const double gam = gp.x, pg = p + gam, alpha = p * gam / pg;
-    double pref = kTwoPi52 / (p * gam * sqrt(pg)) * gp.y;
-#pragma unroll
-    for (int l = 0; l < LC; ++l) pref *= -0.5 / gam;  // (-1)^LC (2 gam)^-LC
-    Real F[L + 1];
-    boys_all(a.dt, a.boys_mode, L, alpha * RPC2, F);
-    Real Rn[L + 1];
-    double f = pref;
-#pragma unroll
-    for (int n = 0; n <= L; ++n) {
-      Rn[n] = static_cast<Real>(f) * F[n];
-      f *= -2.0 * alpha;
-    }
-    Real R[NR];
-    hermite_R_thread<L, Real>(Rn, static_cast<Real>(X), static_cast<Real>(Y), static_cast<Real>(Z), R);
-    if (kp == 0)
-      x_rows_thread<LAB, LC, TPT, Real, false>(R, xrow0, MPAD, part);
-    else
-      x_rows_thread<LAB, LC, TPT, Real, true>(R, xrow0, MPAD, part);
-  }
-}
-
-// X of one triplet by a team of TS threads (L > 5): orders of the Boys
-// function across lanes, R level by level in shared memory, X rows across the
-// lanes. Every thread of a warp (of a team, for teams larger than a warp)
-// calls this with the same Real (the caller makes the precision choice
-// uniform), so the team barriers pair up.
-template <int LAB, int LC, int TS, class Real>
-__device__ __forceinline__ void x_triplet_team(const Df3cArgs& a, const uchar4* txyz, const int* rdesc,
-                                               double* rbuf, int team, int tl, bool active, int np, int po,
-                                               int maxprim, double p, double X, double Y, double Z,
-                                               double* xrow, int mpad) {
-  constexpr int L = LAB + LC;
-  constexpr int NR = ncum(L);
-  constexpr int NH = ncum(LAB);
-  Real* Rn = reinterpret_cast<Real*>(rbuf);
-  Real* b0 = Rn + 16;
-  Real* b1 = b0 + NR;
-  const double RPC2 = X * X + Y * Y + Z * Z;
-  const Real Xr = static_cast<Real>(X), Yr = static_cast<Real>(Y), Zr = static_cast<Real>(Z);
-  for (int kp = 0; kp < maxprim; ++kp) {
-    const bool has = active && kp < np;
-    if (has) {
-      const double2 gp = a.X.prim[po + kp];
-      const double gam = gp.x, pg = p + gam, alpha = p * gam / pg;
-      double pref = kTwoPi52 / (p * gam * sqrt(pg)) * gp.y;
-      for (int l = 0; l < LC; ++l) pref *= -0.5 / gam;
-      // orders n = tl, tl + TS, ...: a team may have fewer lanes than L + 1
-      const typename BoysAtT<Real>::type F(a.boys_mode, alpha * RPC2);
-      for (int n = tl; n <= L; n += TS) {
-        double f = pref;
-        for (int k = 0; k < n; ++k) f *= -2.0 * alpha;
-        Rn[n] = static_cast<Real>(f) * F(a.dt, n);
-      }
-    }
-    team_sync<TS>(team);
-    // Hermite R, level by level. The loops have compile-time trip counts and
-    // are unrolled: the components of one level are independent, so their
-    // descriptor and operand loads are issued back to back instead of one
-    // dependent load chain per component.
-    {
-      Real* top = (L & 1) ? b1 : b0;
-      if (has && tl == 0) top[0] = Rn[L];
-      team_sync<TS>(team);
-#pragma unroll
-      for (int n = L - 1; n >= 0; --n) {
-        Real* dst = (n & 1) ? b1 : b0;
-        const Real* src = (n & 1) ? b0 : b1;
-        const int cnt = ncum(L - n);
-#pragma unroll
-        for (int it = 0; it < (cnt + TS - 1) / TS; ++it) {
-          const int idx = tl + it * TS;
-          if (has && idx < cnt) {
-            Real v;
-            if (idx == 0) {
-              v = Rn[n];
-            } else {
-              const int dsc = rdesc[idx];
-              const int d = rdesc_d(dsc), c = rdesc_c(dsc);
-              const Real xd = d == 0 ? Xr : (d == 1 ? Yr : Zr);
-              v = xd * src[rdesc_s1(dsc)];
-              if (c) v = fma(static_cast<Real>(c), src[rdesc_s2(dsc)], v);
-            }
-            dst[idx] = v;
-          }
-        }
-        team_sync<TS>(team);
-      }
-    }
-    // X rows: lanes over the Hermite components t of the bra, compile-time
-    // solid-harmonic terms of the auxiliary shell (the first primitive stores)
-#pragma unroll
-    for (int it = 0; it < (NH + TS - 1) / TS; ++it) {
-      const int t = tl + it * TS;
-      if (has && t < NH) {
-        const uchar4 e = txyz[t];
-        if (kp == 0)
-          sph_rows<LC, Real, false>(b0, e.x, e.y, e.z, xrow + t * mpad, std::make_integer_sequence<int, 2 * LC + 1>{});
-        else
-          sph_rows<LC, Real, true>(b0, e.x, e.y, e.z, xrow + t * mpad, std::make_integer_sequence<int, 2 * LC + 1>{});
-      }
-    }
-    team_sync<TS>(team);
-  }
-}
-
-// Screening estimate of triplet (unit slot us, auxiliary slot cs), unit Schwarz
-// value uq, auxiliary center cc.xyz: schwarz_estimate Q_ab Q_c
-// (common/screening.f90:301-313; cc.w = Q_c) or, with QVL screening,
-// qvl_estimate (:267-299): Q_ab Q_c within the sum of the extents, beyond it
-// Q_ab pi sqrt(2) beta_c / ((zeta_a + zeta_b)^(1/4) R^(L_c + 1)).
-template <int LC>
-__device__ __forceinline__ double triplet_estimate(const Df3cArgs& a, int us, int cs, double uq,
-                                                   const double4& cc) {
-  if (!a.qvl) return uq * cc.w;
-  const double4 aq = a.aux_qvl[a.aux_slot0 + cs];   // (Q_c, extent, beta, 0)
-  const double4 pq = a.slot_qvl[a.unit_slot0 + us];  // (contracted center, extent)
-  const double dx = pq.x - cc.x, dy = pq.y - cc.y, dz = pq.z - cc.z;
-  const double R = sqrt(dx * dx + dy * dy + dz * dz);
-  if (R <= pq.w + aq.y) return uq * aq.x;
-  double RL = R;
-#pragma unroll
-  for (int l = 0; l < LC; ++l) RL *= R;
-  return uq * kPi * 1.4142135623730951 * aq.z / (a.slot_den[a.unit_slot0 + us] * RL);
-}
-
-// One work item: aux tile bx (TC shells), bra-unit chunk by, density chunk bz.
-template <int LAB, int LC>
-__device__ __forceinline__ void df3c_item(const Df3cArgs& a, int bx, int by, int bz, double* smem) {
-  using C = Cfg<LAB, LC>;
-  double* Xs = smem;                               // [KP][MPAD]
-  double* Gs = Xs + C::KP * C::MPAD;               // [KP][kGStride]
-  double* misc = Gs + C::KP * kGStride;            // unit / aux parameters
-  double* Rteam = misc + 1024;                     // team scratch
-  double4* u_pP = reinterpret_cast<double4*>(misc);                   // [UB <= 64]
-  double* u_Q = misc + 256;                                           // [UB]
-  double4* c_C = reinterpret_cast<double4*>(misc + 320);              // [TC <= 128] (x, y, z, Q)
-  int* c_info = reinterpret_cast<int*>(misc + 320 + 512);             // [TC] (nprim, prim_off)
-
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int c0 = bx * C::TC;
-  const int tile_n = min(C::TC, a.n_aux - c0);
-  const int z = bz;
-  const int d0 = z * a.dw;
-  const int ndc = min(a.dw, a.nd - d0);
-  const int nt_rt = a.dw / 8;  // n-tiles of this launch (dw multiple of 8, <= 40)
-  const int ub = by * a.units_per_chunk;
-  const int ue = min(a.n_units, ub + a.units_per_chunk);
-
-  if (tid < C::TC) {
-    if (tid < tile_n) {
-      const int sh = a.sorted_aux[a.aux_slot0 + c0 + tid];
-      const int4 info = a.X.shell[sh];
-      const double4 cen = a.X.center[sh];
-      c_C[tid] = make_double4(cen.x, cen.y, cen.z, a.aux_Q[a.aux_slot0 + c0 + tid]);
-      c_info[2 * tid] = info.y;
-      c_info[2 * tid + 1] = info.z;
-    } else {
-      c_C[tid] = make_double4(0.0, 0.0, 0.0, 0.0);
-      c_info[2 * tid] = 0;
-      c_info[2 * tid + 1] = 0;
-    }
-  }
-  __syncthreads();
-  int maxprim = 0;
-  for (int i = 0; i < tile_n; ++i) maxprim = max(maxprim, c_info[2 * i]);
-  const double qc_max = tile_n > 0 ? c_C[0].w : 0.0;
-  const double thr = a.thresh;
-  const IndexTables* it = a.dt.idx;
-  const int g = lane >> 2, t4 = lane & 3;
-  // DMMA work of this warp: its first row tile and its k slice (warps past
-  // MT * KSPLIT get slice KSPLIT, which has no k steps)
-  const int mt0 = C::KSPLIT > 1 ? warp % C::MT : warp;
-  const int ks = C::KSPLIT > 1 ? warp / C::MT : 0;
-
-  double acc[C::MTW][5][2];
-#pragma unroll
-  for (int j = 0; j < C::MTW; ++j)
-#pragma unroll
-    for (int n = 0; n < 5; ++n) acc[j][n][0] = acc[j][n][1] = 0.0;
-
-  // unit data of the next step, loaded one step ahead by threads tid < UB
-  double nq = 0.0;
-  double4 npP = make_double4(1.0, 0.0, 0.0, 0.0);
-  if (tid < C::UB && ub + tid < ue) {
-    nq = a.unit_Q[a.unit_slot0 + ub + tid];
-    npP = a.slot_pP[a.unit_slot0 + ub + tid];
-  }
-  for (int u0 = ub; u0 < ue && tile_n > 0; u0 += C::UB) {
-    // units of this step that can meet the tile: a prefix, units are sorted.
-    // The unit data written here were last read by the previous step's X
-    // build (before its closing barrier); the barrier of the count below
-    // orders the previous step's product before this step's writes to Xs / Gs.
-    bool valid = false;
-    if (tid < C::UB) {
-      valid = u0 + tid < ue && nq * qc_max >= thr;
-      u_pP[tid] = valid ? npP : make_double4(1.0, 0.0, 0.0, 0.0);
-      u_Q[tid] = valid ? nq : 0.0;
-    }
-    const int nvalid = __syncthreads_count(valid);
-    if (nvalid == 0) break;  // sorted: nothing below survives
-    if (tid < C::UB) {
-      const int s = u0 + C::UB + tid;
-      nq = 0.0;
-      if (s < ue) {
-        nq = a.unit_Q[a.unit_slot0 + s];
-        npP = a.slot_pP[a.unit_slot0 + s];
-      }
-    }
-    // 1. G of the valid units: rows k = ui * NH + t, dw doubles each (16-byte chunks)
-    {
-      const double* gsrc = a.G + (static_cast<long long>(z) * a.n_units + u0) * C::NH * a.dw;
-      const int rows = nvalid * C::NH;
-      const int chunks_per_row = a.dw / 2;
-      for (int i = tid; i < rows * chunks_per_row; i += kThreads) {
-        const int r = i / chunks_per_row, c = i - r * chunks_per_row;
-        cp_async16(Gs + r * kGStride + 2 * c, gsrc + static_cast<long long>(r) * a.dw + 2 * c);
-      }
-      for (int i = tid; i < (C::KP - rows) * 40; i += kThreads) {
-        const int r = rows + i / 40, c = i % 40;
-        Gs[r * kGStride + c] = 0.0;
-      }
-      for (int i = tid; i < rows * (40 - a.dw); i += kThreads) {
-        const int r = i / (40 - a.dw), c = a.dw + i % (40 - a.dw);
-        Gs[r * kGStride + c] = 0.0;
-      }
-    }
-    // (no zeroing pass over X: every triplet of a valid unit and auxiliary
-    // shell writes its rows below -- values, or zeros when screened; rows of
-    // invalid units meet zero G rows, and columns of shells past the tile end
-    // feed accumulator rows that are not written out)
-    __syncthreads();
-
-    // 2. X
-    if constexpr (C::kPerThread) {
-      const int part = warp % C::TPT;
-      for (int tr = lane + 32 * (warp / C::TPT); tr < C::NTRIP; tr += 32 * (kWarps / C::TPT)) {
-        const int ui = tr / C::TC, ci = tr - ui * C::TC;
-        if (ci >= tile_n || ui >= nvalid) continue;
-        const double4 cc = c_C[ci];
-        const double est = triplet_estimate<LC>(a, u0 + ui, c0 + ci, u_Q[ui], cc);
-        double* xrow0 = Xs + (ui * C::NH) * C::MPAD + ci * C::NC;
-        if (est < thr) {
-          x_rows_zero<LAB, LC, C::TPT>(xrow0, C::MPAD, part);
-          continue;
-        }
-        const double4 up = u_pP[ui];
-        const double p = up.x;
-        const double X = up.y - cc.x, Y = up.z - cc.y, Z = up.w - cc.z;
-        const int np = c_info[2 * ci], po = c_info[2 * ci + 1];
-        if (est < a.thr32)
-          x_triplet_thread<LAB, LC, C::NR, C::MPAD, C::TPT, float>(a, p, X, Y, Z, np, po, xrow0, part);
-        else
-          x_triplet_thread<LAB, LC, C::NR, C::MPAD, C::TPT, double>(a, p, X, Y, Z, np, po, xrow0, part);
-      }
-    } else {
-      // team index tables (shared memory copies of the decoded multi-indices)
-      uchar4* txyz = reinterpret_cast<uchar4*>(Rteam + C::NTRIP * (2 * C::NR + 16));
-      int* rdesc = reinterpret_cast<int*>(txyz + C::NR);
-      if (u0 == ub) {
-        for (int i = tid; i < C::NR; i += kThreads) {
-          txyz[i] = *reinterpret_cast<const uchar4*>(it->xyz[i]);
-          rdesc[i] = a.dt.rdesc[i];
-        }
-        __syncthreads();
-      }
-      const int team = tid / C::TS, tl = tid - team * C::TS;
-      const bool in_team = team < C::NTRIP;
-      const int ui = in_team ? team / C::TC : 0, ci = in_team ? team - ui * C::TC : 0;
-      double* rbuf = Rteam + (in_team ? team : 0) * (2 * C::NR + 16);
-      const double4 cc = c_C[ci];
-      const bool valid = in_team && ci < tile_n && ui < nvalid;
-      const double est = valid ? triplet_estimate<LC>(a, u0 + ui, c0 + ci, u_Q[ui], cc) : 0.0;
-      const bool active = valid && est >= thr;
-      const double4 up = u_pP[ui];
-      const double X = up.y - cc.x, Y = up.z - cc.y, Z = up.w - cc.z;
-      const int np = active ? c_info[2 * ci] : 0, po = c_info[2 * ci + 1];
-      double* xrow = Xs + (ui * C::NH) * C::MPAD + ci * C::NC;
-      if (valid && !active)  // screened: its X rows are zero
-        for (int t = tl; t < C::NH; t += C::TS)
-#pragma unroll
-          for (int m = 0; m < C::NC; ++m) xrow[t * C::MPAD + m] = 0.0;
-      // FP32 recurrences only when every active team of the warp has a weak
-      // triplet (a team larger than a warp has one triplet: uniform over it)
-      const bool weak = !active || est < a.thr32;
-      const bool f32 = __all_sync(0xffffffffu, weak) && __any_sync(0xffffffffu, active);
-      if (f32)
-        x_triplet_team<LAB, LC, C::TS, float>(a, txyz, rdesc, rbuf, team, tl, active, np, po, maxprim, up.x, X, Y,
-                                              Z, xrow, C::MPAD);
-      else
-        x_triplet_team<LAB, LC, C::TS, double>(a, txyz, rdesc, rbuf, team, tl, active, np, po, maxprim, up.x, X,
-                                               Y, Z, xrow, C::MPAD);
-    }
-    cp_async_commit_wait_all();
-    __syncthreads();
-
-    // 3. acc[aux fn][d] += X^T G on the FP64 tensor cores (warp w: row tiles
-    //    w, w + 8, ...; with KSPLIT > 1 row tile w % MT, k steps w / MT + KSPLIT j)
-#pragma unroll 2
-    for (int k4 = ks < C::KSPLIT ? ks : C::KP / 4; k4 < C::KP / 4; k4 += C::KSPLIT) {
-      const int kr = 4 * k4 + t4;
-      double bf[5];
-#pragma unroll
-      for (int n = 0; n < 5; ++n) bf[n] = n < nt_rt ? Gs[kr * kGStride + 8 * n + g] : 0.0;
-#pragma unroll
-      for (int j = 0; j < C::MTW; ++j) {
-        const int mt = mt0 + kWarps * j;
-        if (mt < C::MT) {
-          const double av = Xs[kr * C::MPAD + 8 * mt + g];
-#pragma unroll
-          for (int n = 0; n < 5; ++n)
-            if (n < nt_rt) dmma_m8n8k4(acc[j][n][0], acc[j][n][1], av, bf[n]);
-        }
-      }
-    }
-  }
-
-  if constexpr (C::KSPLIT > 1) {
-    // sum the k slices of each row tile in a fixed order (slice 0 first),
-    // through the X and G tiles (contiguous; free once every warp is past its
-    // last product, and rewritten before they are read again)
-    __syncthreads();
-    if (ks < C::KSPLIT) {
-      double* red = Xs + (ks * C::MT + mt0) * 320;
-#pragma unroll
-      for (int n = 0; n < 5; ++n)
-#pragma unroll
-        for (int i = 0; i < 2; ++i) red[(2 * n + i) * 32 + lane] = acc[0][n][i];
-    }
-    __syncthreads();
-    if (ks == 0) {
-#pragma unroll
-      for (int n = 0; n < 5; ++n)
-#pragma unroll
-        for (int i = 0; i < 2; ++i) {
-          double v = Xs[mt0 * 320 + (2 * n + i) * 32 + lane];
-          for (int q = 1; q < C::KSPLIT; ++q) v += Xs[(q * C::MT + mt0) * 320 + (2 * n + i) * 32 + lane];
-          acc[0][n][i] = v;
-        }
-    }
-  }
-  // partial[y][fn][d] (with KSPLIT > 1 only the warps of slice 0 hold sums)
-  double* out = a.partial + static_cast<long long>(by) * a.n_aux * C::NC * a.nd;
-#pragma unroll
-  for (int j = 0; j < C::MTW; ++j) {
-    const int mt = (ks == 0 ? mt0 : C::MT) + kWarps * j;
-    const int row = 8 * mt + g;
-    if (mt >= C::MT || row >= C::M || row / C::NC >= tile_n) continue;
-    const long long fn = static_cast<long long>(c0) * C::NC + row;
-#pragma unroll
-    for (int n = 0; n < 5; ++n)
-#pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        const int col = 8 * n + 2 * t4 + i;
-        if (n < nt_rt && col < ndc) out[fn * a.nd + d0 + col] = acc[j][n][i];
-      }
-  }
-}
-
-// Persistent blocks: each pulls work items from the class's counter, heaviest
-// first (items are numbered with the bra-unit chunk slowest; units and aux
-// shells are sorted by Schwarz value, so early chunks and tiles carry the most
-// surviving triplets).
-// The X tile starts zeroed: entries that no step writes (padding rows and
-// columns) must be finite.
-template <int LAB, int LC>
-__device__ __forceinline__ void zero_x_tile(double* smem) {
-  using C = Cfg<LAB, LC>;
-  for (int i = threadIdx.x; i < C::KP * C::MPAD; i += blockDim.x) smem[i] = 0.0;
-}
-
-template <int LAB, int LC>
-__global__ void __launch_bounds__(kThreads, 2) k_df3c(Df3cArgs a) {
-  extern __shared__ __align__(16) double smem[];
-  __shared__ int s_item;
-  zero_x_tile<LAB, LC>(smem);
-  for (;;) {
-    __syncthreads();  // the previous item is done with shared memory and s_item
-    if (threadIdx.x == 0) s_item = atomicAdd(a.counter, 1);
-    __syncthreads();
-    const int item = s_item;
-    if (item >= a.n_items) return;
-    const int bz = item % a.nbz;
-    const int r = item / a.nbz;
-    df3c_item<LAB, LC>(a, r % a.nbx, r / a.nbx, bz, smem);
-  }
-}
-
-// Batched form: the work items of one class for many molecules in one
-// persistent launch. Molecule m owns items [item_off[m], item_off[m + 1]) and
-// its own descriptor args[m]; molecules are ordered by decreasing work, and a
-// molecule's items heavy-first, so the queue drains with light items last.
-template <int LAB, int LC>
-__global__ void __launch_bounds__(kThreads, 2) k_df3c_batch(const Df3cArgs* __restrict__ args,
-                                                            const int* __restrict__ item_off, int nm,
-                                                            int* counter) {
-  extern __shared__ __align__(16) double smem[];
-  __shared__ int s_item, s_m;
-  __shared__ __align__(16) unsigned char s_raw[sizeof(Df3cArgs)];
-  const Df3cArgs& sa = *reinterpret_cast<const Df3cArgs*>(s_raw);
-  const int total = item_off[nm];
-  zero_x_tile<LAB, LC>(smem);
-  for (;;) {
-    __syncthreads();  // the previous item is done with shared memory and the descriptor
-    if (threadIdx.x == 0) {
-      const int item = atomicAdd(counter, 1);
-      int m = 0;
-      if (item < total) {
-        int lo = 0, hi = nm - 1;  // last m with item_off[m] <= item
-        while (lo < hi) {
-          const int mid = (lo + hi + 1) / 2;
-          if (item_off[mid] <= item)
-            lo = mid;
-          else
-            hi = mid - 1;
-        }
-        m = lo;
-      }
-      s_item = item;
-      s_m = m;
-    }
-    __syncthreads();
-    const int item = s_item;
-    if (item >= total) return;
-    const int m = s_m;
-    static_assert(sizeof(Df3cArgs) % 4 == 0, "descriptor copied in 32-bit words");
-    const unsigned* src = reinterpret_cast<const unsigned*>(args + m);
-    unsigned* dst = reinterpret_cast<unsigned*>(s_raw);
-    for (int i = threadIdx.x; i < static_cast<int>(sizeof(Df3cArgs) / 4); i += blockDim.x) dst[i] = src[i];
-    __syncthreads();
-    const int local = item - item_off[m];
-    const int bz = local % sa.nbz;
-    const int r = local / sa.nbz;
-    df3c_item<LAB, LC>(sa, r % sa.nbx, r / sa.nbx, bz, smem);
-  }
-}
 
 // df_raw[sph_off(P) + m][d] (column-major, naux rows) = sum over LAB classes and
 // bra chunks of the partial slabs of class LC.
@@ -730,111 +33,44 @@ __global__ void k_df3c_reduce(Df3cReduceArgs r) {
   }
 }
 
-// Resident blocks of a kernel on the current device (cached per device and
-// kernel), after raising its dynamic shared-memory limit to smem.
-template <class K>
-int resident_blocks(K kernel, size_t smem, int* occ_cache) {
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 0 || dev >= 64) dev = 0;
-  if (occ_cache[dev] == 0) {
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    int o = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kernel, kThreads, smem);
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    occ_cache[dev] = (o > 0 ? o : 1) * sms;
-  }
-  return occ_cache[dev];
+constexpr int kNLab = 2 * PA_LMAX + 1;
+
+const Df3cRow* rows() {
+  static Df3cRow table[kNLab];
+  static std::once_flag once;
+  std::call_once(once, [] {
+    df3c_row_0(&table[0]);
+    df3c_row_1(&table[1]);
+    df3c_row_2(&table[2]);
+    df3c_row_3(&table[3]);
+    df3c_row_4(&table[4]);
+    df3c_row_5(&table[5]);
+    df3c_row_6(&table[6]);
+    df3c_row_7(&table[7]);
+    df3c_row_8(&table[8]);
+  });
+  return table;
 }
 
-template <int LAB, int LC>
-void fill_items(Df3cArgs* a, int ny) {
-  using C = Cfg<LAB, LC>;
-  a->nbx = (a->n_aux + C::TC - 1) / C::TC;
-  a->nby = ny;
-  a->nbz = (a->nd + a->dw - 1) / a->dw;
-  a->n_items = a->nbx * a->nby * a->nbz;
-}
-
-template <int LAB, int LC>
-int launch_class(const Df3cArgs& a, int ny, cudaStream_t s) {
-  using C = Cfg<LAB, LC>;
-  const size_t smem = sizeof(double) * C::SMEM;
-  static int occ[64] = {};
-  const int resident = resident_blocks(k_df3c<LAB, LC>, smem, occ);
-  Df3cArgs b = a;
-  fill_items<LAB, LC>(&b, ny);
-  if (b.n_items == 0) return 0;
-  k_df3c<LAB, LC><<<std::min(b.n_items, resident), kThreads, smem, s>>>(b);
-  return 1;
-}
-
-template <int LAB, int LC>
-int launch_class_batch(const Df3cArgs* d_args, const int* d_item_off, int nm, int total_items,
-                       int* counter, cudaStream_t s) {
-  using C = Cfg<LAB, LC>;
-  const size_t smem = sizeof(double) * C::SMEM;
-  static int occ[64] = {};
-  const int resident = resident_blocks(k_df3c_batch<LAB, LC>, smem, occ);
-  if (total_items <= 0 || nm <= 0) return 0;
-  k_df3c_batch<LAB, LC><<<std::min(total_items, resident), kThreads, smem, s>>>(d_args, d_item_off, nm,
-                                                                                 counter);
-  return 1;
-}
-
-template <int LAB, int LC>
-void class_info(Df3cClassInfo* ci) {
-  using C = Cfg<LAB, LC>;
-  ci->tc = C::TC;
-  ci->ub = C::UB;
-  ci->ndc = 40;
-  ci->smem = sizeof(double) * C::SMEM;
-}
-
-using LaunchFn = int (*)(const Df3cArgs&, int, cudaStream_t);
-using InfoFn = void (*)(Df3cClassInfo*);
-using FillFn = void (*)(Df3cArgs*, int);
-using BatchFn = int (*)(const Df3cArgs*, const int*, int, int, int*, cudaStream_t);
-
-#define PA_ROW(LAB)                                                                    \
-  {&launch_class<LAB, 0>, &launch_class<LAB, 1>, &launch_class<LAB, 2>, &launch_class<LAB, 3>, \
-   &launch_class<LAB, 4>, &launch_class<LAB, 5>}
-#define PA_IROW(LAB)                                                               \
-  {&class_info<LAB, 0>, &class_info<LAB, 1>, &class_info<LAB, 2>, &class_info<LAB, 3>, \
-   &class_info<LAB, 4>, &class_info<LAB, 5>}
-
-const LaunchFn kLaunch[2 * PA_LMAX + 1][PA_LAUXMAX + 1] = {
-    PA_ROW(0), PA_ROW(1), PA_ROW(2), PA_ROW(3), PA_ROW(4), PA_ROW(5), PA_ROW(6), PA_ROW(7), PA_ROW(8)};
-const InfoFn kInfo[2 * PA_LMAX + 1][PA_LAUXMAX + 1] = {
-    PA_IROW(0), PA_IROW(1), PA_IROW(2), PA_IROW(3), PA_IROW(4),
-    PA_IROW(5), PA_IROW(6), PA_IROW(7), PA_IROW(8)};
-#define PA_FROW(LAB)                                                                            \
-  {&fill_items<LAB, 0>, &fill_items<LAB, 1>, &fill_items<LAB, 2>, &fill_items<LAB, 3>,             \
-   &fill_items<LAB, 4>, &fill_items<LAB, 5>}
-const FillFn kFill[2 * PA_LMAX + 1][PA_LAUXMAX + 1] = {
-    PA_FROW(0), PA_FROW(1), PA_FROW(2), PA_FROW(3), PA_FROW(4),
-    PA_FROW(5), PA_FROW(6), PA_FROW(7), PA_FROW(8)};
-#define PA_BROW(LAB)                                                                            \
-  {&launch_class_batch<LAB, 0>, &launch_class_batch<LAB, 1>, &launch_class_batch<LAB, 2>,          \
-   &launch_class_batch<LAB, 3>, &launch_class_batch<LAB, 4>, &launch_class_batch<LAB, 5>}
-const BatchFn kBatch[2 * PA_LMAX + 1][PA_LAUXMAX + 1] = {
-    PA_BROW(0), PA_BROW(1), PA_BROW(2), PA_BROW(3), PA_BROW(4),
-    PA_BROW(5), PA_BROW(6), PA_BROW(7), PA_BROW(8)};
+int checked(int v) { return (v >= 0 && v < kDf3cVariants) ? v : 0; }
 
 }  // namespace
 
-void df3c_class_info(int lab, int lc, Df3cClassInfo* ci) { kInfo[lab][lc](ci); }
-
-int launch_df3c_class(int lab, int lc, const Df3cArgs& a, int ny, cudaStream_t s) {
-  return kLaunch[lab][lc](a, ny, s);
+void df3c_class_info(int lab, int lc, int variant, Df3cClassInfo* ci) {
+  rows()[lab].info[checked(variant)][lc](ci);
 }
 
-void df3c_fill_items(int lab, int lc, Df3cArgs* a, int ny) { kFill[lab][lc](a, ny); }
+int launch_df3c_class(int lab, int lc, int variant, const Df3cArgs& a, int ny, cudaStream_t s) {
+  return rows()[lab].launch[checked(variant)][lc](a, ny, s);
+}
 
-int launch_df3c_class_batch(int lab, int lc, const Df3cArgs* d_args, const int* d_item_off, int nm,
-                            int total_items, int* counter, cudaStream_t s) {
-  return kBatch[lab][lc](d_args, d_item_off, nm, total_items, counter, s);
+void df3c_fill_items(int lab, int lc, int variant, Df3cArgs* a, int ny) {
+  rows()[lab].fill[checked(variant)][lc](a, ny);
+}
+
+int launch_df3c_class_batch(int lab, int lc, int variant, const Df3cArgs* d_args, const int* d_item_off,
+                            int nm, int total_items, int* counter, cudaStream_t s) {
+  return rows()[lab].batch[checked(variant)][lc](d_args, d_item_off, nm, total_items, counter, s);
 }
 
 int launch_df3c_reduce(const Df3cReduceArgs& r, cudaStream_t s) {
@@ -845,17 +81,12 @@ int launch_df3c_reduce(const Df3cReduceArgs& r, cudaStream_t s) {
   return 1;
 }
 
-cudaError_t upload_sph_dense(const double* vals, int n, const int* offs, const double* rownorm,
-                             cudaStream_t s) {
-  cudaError_t e = cudaMemcpyToSymbolAsync(c_sph_dense, vals, sizeof(double) * n, 0,
-                                          cudaMemcpyHostToDevice, s);
-  if (e != cudaSuccess) return e;
-  e = cudaMemcpyToSymbolAsync(c_sph_rownorm, rownorm,
-                              sizeof(double) * (PA_LAUXMAX + 1) * (PA_LAUXMAX + 1), 0,
-                              cudaMemcpyHostToDevice, s);
-  if (e != cudaSuccess) return e;
-  return cudaMemcpyToSymbolAsync(c_sph_off, offs, sizeof(int) * (PA_LAUXMAX + 2), 0,
-                                 cudaMemcpyHostToDevice, s);
+cudaError_t upload_sph_rownorm(const double* rownorm, cudaStream_t s) {
+  for (int lab = 0; lab < kNLab; ++lab) {
+    const cudaError_t e = rows()[lab].upload_rownorm(rownorm, s);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace pa

@@ -1,4 +1,5 @@
-// Launch interface of the three-center contraction (k_df3c.cu).
+// Launch interface of the three-center contraction (k_df3c.cu, the class
+// kernels in k_df3c_impl.cuh instantiated by k_df3c_l<LAB>.cu).
 #pragma once
 
 #include "pa_internal.h"
@@ -54,19 +55,48 @@ struct Df3cReduceArgs {
 
 struct Df3cClassInfo {
   int tc = 0, ub = 0, ndc = 0;
+  int lanes = 0;          // lanes per triplet in the X build (TPT or team size)
+  int blocks_per_sm = 0;  // occupancy the shape is sized for
   size_t smem = 0;
 };
 
-void df3c_class_info(int lab, int lc, Df3cClassInfo* ci);
-int launch_df3c_class(int lab, int lc, const Df3cArgs& a, int ny, cudaStream_t s);
+// Tile-shape variants per class (k_df3c_impl.cuh, Cfg); Options::tile_variant
+// selects one per class.
+constexpr int kDf3cVariants = 3;
+
+void df3c_class_info(int lab, int lc, int variant, Df3cClassInfo* ci);
+int launch_df3c_class(int lab, int lc, int variant, const Df3cArgs& a, int ny, cudaStream_t s);
 // Fills a->nbx, nby, nbz and n_items of one class run (host side).
-void df3c_fill_items(int lab, int lc, Df3cArgs* a, int ny);
+void df3c_fill_items(int lab, int lc, int variant, Df3cArgs* a, int ny);
 // One persistent launch of class (lab, lc) over the runs of nm molecules:
 // d_args[m] (device) with items [d_item_off[m], d_item_off[m + 1]).
-int launch_df3c_class_batch(int lab, int lc, const Df3cArgs* d_args, const int* d_item_off, int nm,
-                            int total_items, int* counter, cudaStream_t s);
+int launch_df3c_class_batch(int lab, int lc, int variant, const Df3cArgs* d_args, const int* d_item_off,
+                            int nm, int total_items, int* counter, cudaStream_t s);
 int launch_df3c_reduce(const Df3cReduceArgs& r, cudaStream_t s);
-cudaError_t upload_sph_dense(const double* vals, int n, const int* offs, const double* rownorm,
-                             cudaStream_t s);
+// Row normalization of the solid harmonics (constant memory of every class
+// translation unit).
+cudaError_t upload_sph_rownorm(const double* rownorm, cudaStream_t s);
+
+// Dispatch row of one LAB (defined by k_df3c_l<LAB>.cu).
+struct Df3cRow {
+  using LaunchFn = int (*)(const Df3cArgs&, int, cudaStream_t);
+  using InfoFn = void (*)(Df3cClassInfo*);
+  using FillFn = void (*)(Df3cArgs*, int);
+  using BatchFn = int (*)(const Df3cArgs*, const int*, int, int, int*, cudaStream_t);
+  LaunchFn launch[kDf3cVariants][PA_LAUXMAX + 1] = {};
+  InfoFn info[kDf3cVariants][PA_LAUXMAX + 1] = {};
+  FillFn fill[kDf3cVariants][PA_LAUXMAX + 1] = {};
+  BatchFn batch[kDf3cVariants][PA_LAUXMAX + 1] = {};
+  cudaError_t (*upload_rownorm)(const double*, cudaStream_t) = nullptr;
+};
+void df3c_row_0(Df3cRow*);
+void df3c_row_1(Df3cRow*);
+void df3c_row_2(Df3cRow*);
+void df3c_row_3(Df3cRow*);
+void df3c_row_4(Df3cRow*);
+void df3c_row_5(Df3cRow*);
+void df3c_row_6(Df3cRow*);
+void df3c_row_7(Df3cRow*);
+void df3c_row_8(Df3cRow*);
 
 }  // namespace pa

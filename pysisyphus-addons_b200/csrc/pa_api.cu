@@ -17,8 +17,12 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <dlfcn.h>
+#include <fstream>
 #include <mutex>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -45,7 +49,50 @@ std::mutex g_opt_mu;
 Options g_opts;
 pa_stats g_stats{};
 
+// Applies "L_ab L_c variant" lines of a tile table (# starts a comment) to
+// g_opts; returns the number of entries applied, -1 if the file cannot be read,
+// -2 on a malformed or out-of-range entry (nothing applied then).
+int apply_tile_table(const char* path) {
+  std::ifstream in(path);
+  if (!in) return -1;
+  std::vector<int> ent;
+  std::string line;
+  while (std::getline(in, line)) {
+    const size_t h = line.find('#');
+    if (h != std::string::npos) line.resize(h);
+    std::istringstream ls(line);
+    int lab, lc, v;
+    if (!(ls >> lab)) continue;
+    std::string rest;
+    if (!(ls >> lc >> v) || (ls >> rest)) return -2;
+    if (lab < 0 || lab > 2 * PA_LMAX || lc < 0 || lc > PA_LAUXMAX || v < 0 || v >= kDf3cVariants) return -2;
+    ent.insert(ent.end(), {lab, lc, v});
+  }
+  std::lock_guard<std::mutex> lk(g_opt_mu);
+  for (size_t i = 0; i < ent.size(); i += 3)
+    g_opts.tile_variant[ent[i]][ent[i + 1]] = static_cast<signed char>(ent[i + 2]);
+  return static_cast<int>(ent.size() / 3);
+}
+
+// The tile table read once per process: $PA_B200_TILE_TABLE when set (empty:
+// none), else df3c_tiles.txt beside this library when present.
+std::string default_tile_table() {
+  if (const char* env = std::getenv("PA_B200_TILE_TABLE")) return env;
+  Dl_info info{};
+  if (!dladdr(reinterpret_cast<void*>(&apply_tile_table), &info) || !info.dli_fname) return "";
+  std::string lib = info.dli_fname;
+  const size_t slash = lib.rfind('/');
+  return (slash == std::string::npos ? std::string() : lib.substr(0, slash + 1)) + "df3c_tiles.txt";
+}
+
+static_assert(kDf3cVariants == PA_TILE_VARIANTS, "tile variants of the header and the kernels agree");
+std::once_flag g_tile_once;
+
 Options options() {
+  std::call_once(g_tile_once, [] {
+    const std::string path = default_tile_table();
+    if (!path.empty()) apply_tile_table(path.c_str());
+  });
   std::lock_guard<std::mutex> lk(g_opt_mu);
   return g_opts;
 }
@@ -562,6 +609,7 @@ struct DfBuffers {
   struct ClassRun {
     int lab, lc, ny, upc;
     double* partial;
+    int variant;  // tile-shape variant of the class kernel
   };
   std::vector<ClassRun> runs;
 };
@@ -607,7 +655,8 @@ int class_sort_desc(DfBuffers& b, const double* keys, const int* positions, cons
 
 // Lays out all buffers of a run (counting when c.base == nullptr).
 void layout_df(Carver& c, const pa_basis_s* orb, const pa_basis_s* aux, int nd, DfBuffers* b,
-               int items_per_sm) {
+               const Options& o) {
+  int items_per_sm = o.items_per_sm;
   const PairLists& P = orb->pairs;
   const int nx = static_cast<int>(aux->host.shells.size());
   const long long naux = aux->host.nsph;
@@ -667,8 +716,9 @@ void layout_df(Carver& c, const pa_basis_s* orb, const pa_basis_s* aux, int nd, 
     for (int lab = 0; lab <= P.lab_max; ++lab) {
       const int nu = P.class_off[lab + 1] - P.class_off[lab];
       if (nu == 0) continue;
+      const int variant = o.tile_variant[lab][lc];
       Df3cClassInfo ci;
-      df3c_class_info(lab, lc, &ci);
+      df3c_class_info(lab, lc, variant, &ci);
       const int bx = (nxc + ci.tc - 1) / ci.tc;
       const int bz = nz;
       const int target = items_per_sm * 148;  // work items per class (persistent blocks pull them)
@@ -678,7 +728,7 @@ void layout_df(Carver& c, const pa_basis_s* orb, const pa_basis_s* aux, int nd, 
       int upc = (nu + ny - 1) / ny;
       upc = ((upc + ci.ub - 1) / ci.ub) * ci.ub;
       ny = (nu + upc - 1) / upc;
-      DfBuffers::ClassRun r{lab, lc, ny, upc, nullptr};
+      DfBuffers::ClassRun r{lab, lc, ny, upc, nullptr, variant};
       b->runs.push_back(r);
       part_total += static_cast<size_t>(ny) * nxc * (2 * lc + 1) * nd;
     }
@@ -927,7 +977,7 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
       cudaStream_t cs = ctx->s3c[o.class_timing ? 0 : ri % Ctx::kNs3c];
       PA_CUDA(cudaStreamWaitEvent(cs, ctx->ev_bra[r.lab], 0));
       if (o.class_timing) PA_CUDA(cudaEventRecord(ctx->ct_ev[2 * ri], cs));
-      *launches += launch_df3c_class(r.lab, r.lc, a, r.ny, cs);
+      *launches += launch_df3c_class(r.lab, r.lc, r.variant, a, r.ny, cs);
       if (o.class_timing) PA_CUDA(cudaEventRecord(ctx->ct_ev[2 * ri + 1], cs));
       if (ri + 1 == nr || b.runs[ri + 1].lc != r.lc) {
         for (int i = 0; i < Ctx::kNs3c; ++i) {
@@ -1095,12 +1145,12 @@ int df_device(pa_basis orb, pa_basis aux, int ndens, int nbf, const double* d_de
   cudaStream_t s = user_stream;
   DfBuffers b;
   Carver cnt;
-  layout_df(cnt, orb, aux, ndens, &b, o.items_per_sm);
+  layout_df(cnt, orb, aux, ndens, &b, o);
   if (d_R) cnt.take<double>(static_cast<size_t>(ndens) * ndens);
   PA_CUDA(c->arena.reserve(cnt.used));
   Carver real;
   real.base = c->arena.base;
-  layout_df(real, orb, aux, ndens, &b, o.items_per_sm);
+  layout_df(real, orb, aux, ndens, &b, o);
   double* gram = d_R ? real.take<double>(static_cast<size_t>(ndens) * ndens) : nullptr;
   const long long n = nbf;
   long long sd, si, sj;
@@ -1196,7 +1246,8 @@ int record_batch(Ctx* c, BatchPlan& plan, const std::vector<BatchMol>& mols, con
   // the next groups run (as the single-molecule path does)
   bool reduced[PA_LAUXMAX + 1] = {};
   for (int k = 0; k < ncls; ++k) {
-    *launches += launch_df3c_class_batch(class_lab[k], class_lc[k], class_args_d[k], class_off_d[k], class_nm[k],
+    *launches += launch_df3c_class_batch(class_lab[k], class_lc[k], o.tile_variant[class_lab[k]][class_lc[k]],
+                                         class_args_d[k], class_off_d[k], class_nm[k],
                                          class_items[k], plan.counters + k, c->s3c[k % W]);
     if (k + 1 == ncls || class_lc[k + 1] != class_lc[k]) {
       for (int i = 0; i < W; ++i) {
@@ -1276,6 +1327,8 @@ int batch_4d(int nmol, const pa_basis* orbs, const pa_basis* auxs, const int* nd
   // signature of the batch: options, then per molecule handles, sizes, pointers
   std::vector<long long> sig{nmol, layout, use_graph ? 1 : 0, o.boys_mode, o.skip_metric, o.precision,
                              o.items_per_sm, o.screening};
+  for (const auto& row : o.tile_variant)
+    for (signed char v : row) sig.push_back(v);
   for (double v : {o.screen_thresh, o.fp32_thresh, o.metric_shift}) {
     long long bits;
     std::memcpy(&bits, &v, sizeof bits);
@@ -1322,7 +1375,7 @@ int batch_4d(int nmol, const pa_basis* orbs, const pa_basis* auxs, const int* nd
       if (pass == 1) cv.base = plan->dmem;
       for (int m = 0; m < nmol; ++m) {
         const BatchMol& M = mols[m];
-        layout_df(cv, M.orb, M.aux, M.nd, &plan->bufs[m], o.items_per_sm);
+        layout_df(cv, M.orb, M.aux, M.nd, &plan->bufs[m], o);
         plan->df[m] = cv.take<double>(static_cast<size_t>(M.aux->host.nsph) * M.nd);
         plan->gram[m] = cv.take<double>(static_cast<size_t>(M.nd) * M.nd);
       }
@@ -1356,7 +1409,7 @@ int batch_4d(int nmol, const pa_basis* orbs, const pa_basis* auxs, const int* nd
         for (const auto& r : b.runs) {
           if (r.lab != class_lab[k] || r.lc != class_lc[k]) continue;
           Df3cArgs a = class_args(M.orb, M.aux, M.nd, b, dt, o, r);
-          df3c_fill_items(r.lab, r.lc, &a, r.ny);
+          df3c_fill_items(r.lab, r.lc, r.variant, &a, r.ny);
           const long long work = static_cast<long long>(a.n_units) * a.n_aux * a.nd;
           if (a.n_items > 0) items.push_back({work, a});
         }
@@ -1772,6 +1825,47 @@ int pa_get_class_times(int cap, int* lab, int* lc, double* ms) {
     if (ms) ms[i] = g_class_times[i].ms;
   }
   return n;
+}
+
+int pa_set_tile_variant(int lab, int lc, int variant) {
+  if (lab < 0 || lab > 2 * PA_LMAX || lc < 0 || lc > PA_LAUXMAX)
+    return fail(PA_ERR_ARG, "tile variant: class (L_ab, L_c) out of range");
+  if (variant < 0 || variant >= kDf3cVariants) return fail(PA_ERR_ARG, "tile variant out of range");
+  options();  // the default table is applied first, so it cannot override this call later
+  std::lock_guard<std::mutex> lk(g_opt_mu);
+  g_opts.tile_variant[lab][lc] = static_cast<signed char>(variant);
+  return PA_OK;
+}
+
+int pa_get_tile_variant(int lab, int lc, int* variant) {
+  if (lab < 0 || lab > 2 * PA_LMAX || lc < 0 || lc > PA_LAUXMAX || !variant)
+    return fail(PA_ERR_ARG, "tile variant: class (L_ab, L_c) out of range");
+  *variant = options().tile_variant[lab][lc];
+  return PA_OK;
+}
+
+int pa_tile_shape(int lab, int lc, int variant, int* out) {
+  if (lab < 0 || lab > 2 * PA_LMAX || lc < 0 || lc > PA_LAUXMAX || variant < 0 || variant >= kDf3cVariants ||
+      !out)
+    return fail(PA_ERR_ARG, "tile shape: class or variant out of range");
+  Df3cClassInfo ci;
+  df3c_class_info(lab, lc, variant, &ci);
+  out[0] = ci.tc;
+  out[1] = ci.ub;
+  out[2] = ci.lanes;
+  out[3] = ci.blocks_per_sm;
+  out[4] = static_cast<int>(ci.smem);
+  return PA_OK;
+}
+
+int pa_load_tile_table(const char* path, int* napplied) {
+  options();  // the default table first (a later explicit table wins)
+  const std::string p = path ? std::string(path) : default_tile_table();
+  const int n = p.empty() ? 0 : apply_tile_table(p.c_str());
+  if (n == -1 && path) return fail(PA_ERR_ARG, "tile table: cannot read " + p);
+  if (n == -2) return fail(PA_ERR_ARG, "tile table: malformed or out-of-range entry in " + p);
+  if (napplied) *napplied = std::max(n, 0);
+  return PA_OK;
 }
 
 int pa_set_metric_shift(double shift) {

@@ -91,6 +91,8 @@ struct Options {
   int items_per_sm = 0;       // work items per SM and class of the three-center kernel (0 = by size)
   int screening = 0;          // triplet estimate: 0 = Schwarz (reference), 1 = QVL
   int class_timing = 0;       // 1: class launches serialized on one stream, each timed with events
+  // tile-shape variant of each three-center class [L_ab][L_c] (0 = default)
+  signed char tile_variant[2 * PA_LMAX + 1][PA_LAUXMAX + 1] = {};
 };
 
 struct Stats {

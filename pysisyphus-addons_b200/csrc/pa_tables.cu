@@ -142,18 +142,16 @@ int build_tables(TablesOnDevice* out, std::string* err) {
     boys_series_ld(kBoysRefNOrd - 1, xi, F);
     for (int n = 0; n < kBoysRefNOrd; ++n) ref[static_cast<size_t>(n) * kBoysRefNPts + i] = (double)F[n];
   }
-  // solid harmonics: sparse rows for l <= PA_LTOT_MAX/..., dense for l <= PA_LAUXMAX
+  // solid harmonics: sparse rows, and the row normalization of the auxiliary
+  // shells' terms (the class kernels carry the raw coefficients)
   std::vector<int> start{0};
   std::vector<int16_t> col;
-  std::vector<double> val, dense;
-  std::vector<int> dense_off;
+  std::vector<double> val;
   std::vector<double> rownorm((PA_LAUXMAX + 1) * (PA_LAUXMAX + 1), 0.0);
   const int lsph = std::max(PA_LMAX, PA_LAUXMAX);
   for (int l = 0; l <= lsph; ++l) {
     const std::vector<double> T = solid_harmonics(l);
     const int nc = ncart(l);
-    dense_off.push_back(static_cast<int>(dense.size()));
-    dense.insert(dense.end(), T.begin(), T.end());
     if (l <= PA_LAUXMAX)
       for (int m = 0; m < 2 * l + 1; ++m)
         for (int i = l, c = 0; i >= 0; --i)
@@ -172,7 +170,6 @@ int build_tables(TablesOnDevice* out, std::string* err) {
       start.push_back(static_cast<int>(col.size()));
     }
   }
-  dense_off.push_back(static_cast<int>(dense.size()));
   // multi-index sums of two bra Hermite components
   std::vector<int16_t> sum_idx(static_cast<size_t>(kNSum) * kNSum);
   for (int i = 0; i < kNSum; ++i)
@@ -188,10 +185,6 @@ int build_tables(TablesOnDevice* out, std::string* err) {
     const int c = e[d] - 1;
     const int s2 = c > 0 ? h_idx.minus[s1][d] : 0;
     rdesc[idx] = s1 | (s2 << 10) | (d << 20) | (c << 22);
-  }
-  if (dense.size() > 1024) {
-    *err = "solid-harmonic table exceeds its constant-memory slot";
-    return PA_ERR_ARG;
   }
   // upload
   const size_t bytes = sizeof(IndexTables) + sizeof(double) * (taylor.size() + ref.size() + val.size()) +
@@ -219,7 +212,7 @@ int build_tables(TablesOnDevice* out, std::string* err) {
   dt.sph_val = reinterpret_cast<const double*>(put(val.data(), sizeof(double) * val.size()));
   dt.sum_idx = reinterpret_cast<const int16_t*>(put(sum_idx.data(), sizeof(int16_t) * sum_idx.size()));
   dt.rdesc = reinterpret_cast<const int*>(put(rdesc.data(), sizeof(int) * rdesc.size()));
-  e = upload_sph_dense(dense.data(), static_cast<int>(dense.size()), dense_off.data(), rownorm.data(), 0);
+  e = upload_sph_rownorm(rownorm.data(), 0);
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
     *err = std::string("table upload: ") + cudaGetErrorString(e);

@@ -31,6 +31,7 @@ PA_SCREEN_SCHWARZ = 0
 PA_SCREEN_QVL = 1
 PA_LAYOUT_FORTRAN = 0
 PA_LAYOUT_C = 1
+LMAX, LAUXMAX = 4, 5  # PA_LMAX_ORBITAL, PA_LMAX_AUX of pa_b200.h
 PA_LMAX_ORBITAL = 4
 PA_LMAX_AUX = 5
 PA_NOALLOC_SCRATCH_DOUBLES = 1 << 20
@@ -118,6 +119,10 @@ SIGNATURES = {
     "pa_df_solve": [_vp, _i, _vp, _vp, _i, _vp, _vp],
     "pa_set_class_timing": [_i],
     "pa_get_class_times": [_i, _pi, _pi, _pd],
+    "pa_set_tile_variant": [_i, _i, _i],
+    "pa_get_tile_variant": [_i, _i, _pi],
+    "pa_tile_shape": [_i, _i, _i, _pi],
+    "pa_load_tile_table": [ctypes.c_char_p, _pi],
     "f_benchmark_int3c2e": _BASIS + _BASIS,
     "pa_int3c2e_estimates": [_vp, _vp, ctypes.c_longlong, _pd, ctypes.POINTER(ctypes.c_longlong),
                              ctypes.POINTER(ctypes.c_longlong)],
@@ -234,6 +239,35 @@ def get_class_times():
     lab, lc, ms = (ctypes.c_int * max(n, 1))(), (ctypes.c_int * max(n, 1))(), (ctypes.c_double * max(n, 1))()
     lib.pa_get_class_times(n, lab, lc, ms)
     return [(lab[i], lc[i], ms[i]) for i in range(n)]
+
+
+TILE_VARIANTS = 3
+
+
+def set_tile_variant(lab, lc, variant):
+    """Tile-shape variant of the three-center class (L_ab, L_c) (0 = default)."""
+    check(load().pa_set_tile_variant(int(lab), int(lc), int(variant)))
+
+
+def get_tile_variant(lab, lc):
+    v = ctypes.c_int()
+    check(load().pa_get_tile_variant(int(lab), int(lc), ctypes.byref(v)))
+    return v.value
+
+
+def tile_shape(lab, lc, variant):
+    """dict(tc, ub, lanes, blocks_per_sm, smem) of one class variant."""
+    out = (ctypes.c_int * 5)()
+    check(load().pa_tile_shape(int(lab), int(lc), int(variant), out))
+    return dict(zip(("tc", "ub", "lanes", "blocks_per_sm", "smem"), list(out)))
+
+
+def load_tile_table(path=None):
+    """Applies a tile table ("L_ab L_c variant" lines); None = the default
+    table beside the library. Returns the number of entries applied."""
+    n = ctypes.c_int()
+    check(load().pa_load_tile_table(None if path is None else str(path).encode(), ctypes.byref(n)))
+    return n.value
 
 
 def get_stats():
