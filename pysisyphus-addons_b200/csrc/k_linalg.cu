@@ -397,6 +397,88 @@ __global__ void __launch_bounds__(256) k_gemm(int m, int n, int k, double alpha,
       }
 }
 
+// Trailing update of the Cholesky factorization: C -= P P^T on the lower part
+// (i >= j) of C (m x ncols, ncols <= m, column-major, ldc), P (m x k,
+// column-major, ldp, k <= NB). One block per 64 x 64 tile of that lower part:
+// blockIdx.x enumerates the triangle of the first ncols tile rows, then the
+// full tile rows below. Both panels of a tile are staged whole (every k at
+// once) by 8-byte cp.async copies (ldp may be odd), in rows of 68 doubles
+// (4 mod 16: conflict-free m8n8k4 fragment loads); three blocks per SM keep
+// one block's copies in flight during another's products. The products run
+// in k_gemm's order (k ascending, four at a time, zeros up to a multiple of
+// 16), so the factor is the same bit for bit.
+constexpr int kSyrkLd = TM + 4;
+constexpr size_t kSyrkSmem = sizeof(double) * 2 * NB * kSyrkLd;
+
+__device__ __forceinline__ void cp_async8(double* smem_dst, const double* gmem_src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gmem_src));
+}
+
+__global__ void __launch_bounds__(256, 3) k_syrk_update(int m, int ncols, int k, const double* __restrict__ P,
+                                                         long long ldp, double* C, long long ldc) {
+  extern __shared__ __align__(16) double sm[];
+  double* As = sm;                  // As[c * kSyrkLd + r] = P[i0 + r, c]
+  double* Bs = sm + NB * kSyrkLd;   // Bs[c * kSyrkLd + r] = P[j0 + r, c]
+  const int nbc = (ncols + TN - 1) / TN;
+  const int t = blockIdx.x, ntri = nbc * (nbc + 1) / 2;
+  int bi, bj;
+  if (t < ntri) {
+    bi = static_cast<int>((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+    while ((bi + 1) * (bi + 2) / 2 <= t) ++bi;
+    while (bi * (bi + 1) / 2 > t) --bi;
+    bj = t - bi * (bi + 1) / 2;
+  } else {
+    bi = nbc + (t - ntri) / nbc;
+    bj = (t - ntri) % nbc;
+  }
+  const int i0 = bi * TM, j0 = bj * TN;
+  const int kq = (k + TK - 1) / TK * TK;
+  for (int idx = threadIdx.x; idx < kq * TM; idx += 256) {
+    const int r = idx % TM, c = idx / TM;
+    double* da = As + c * kSyrkLd + r;
+    double* db = Bs + c * kSyrkLd + r;
+    if (c < k && i0 + r < m)
+      cp_async8(da, P + (i0 + r) + ldp * c);
+    else
+      *da = 0.0;
+    if (c < k && j0 + r < ncols)
+      cp_async8(db, P + (j0 + r) + ldp * c);
+    else
+      *db = 0.0;
+  }
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t4 = lane & 3;
+  const int wm = (warp & 3) * 16, wn = (warp >> 2) * 32;
+  double acc[2][4][2] = {};
+#pragma unroll 4
+  for (int q = 0; q < kq; q += 4) {
+    double a[2], b[4];
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) a[mt] = As[(q + t4) * kSyrkLd + wm + 8 * mt + g];
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) b[nt] = Bs[(q + t4) * kSyrkLd + wn + 8 * nt + g];
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) dmma_m8n8k4(acc[mt][nt][0], acc[mt][nt][1], a[mt], b[nt]);
+  }
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int gi = i0 + wm + 8 * mt + g, gj = j0 + wn + 8 * nt + 2 * t4 + i;
+        if (gi < m && gj < ncols && gi >= gj) {
+          double* c = C + gi + ldc * gj;
+          *c = *c + -1.0 * acc[mt][nt][i];
+        }
+      }
+}
+
 // Gram matrix G[i + nd j] = sum_k df[k + naux i] df[k + naux j] of the fitted
 // densities, one warp per entry: lanes stride over k (contiguous columns),
 // then a fixed-order shuffle reduction. Used for nd <= kGramWarpMax, where the
@@ -458,6 +540,16 @@ int gemm_impl(bool ta, bool tb, int m, int n, int k, double alpha, const double*
   return 1;
 }
 
+// C -= P P^T on the lower part of C (m x ncols), P m x k (k <= NB).
+int syrk_update(int m, int ncols, int k, const double* P, long long ldp, double* C, long long ldc,
+                cudaStream_t s) {
+  if (m <= 0 || ncols <= 0) return 0;
+  const long long nbr = (m + TM - 1) / TM, nbc = (ncols + TN - 1) / TN;
+  const long long tiles = nbc * (nbc + 1) / 2 + (nbr - nbc) * nbc;
+  k_syrk_update<<<static_cast<unsigned>(tiles), 256, kSyrkSmem, s>>>(m, ncols, k, P, ldp, C, ldc);
+  return 1;
+}
+
 }  // namespace
 
 int gemm(bool ta, bool tb, int m, int n, int k, double alpha, const double* A, long long lda,
@@ -478,6 +570,7 @@ int cholesky_lower(double* A, int n, int* d_info, double* work, cudaStream_t s,
                        static_cast<int>(2 * kTileSmem));
   cudaFuncSetAttribute(k_potrf_diag_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        static_cast<int>(3 * kTileSmem));
+  cudaFuncSetAttribute(k_syrk_update, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSyrkSmem));
   cudaMemsetAsync(d_info, 0, sizeof(int), s);
   const int nblk = (n + NB - 1) / NB;
   bool rest_pending = false;  // a trailing update of the previous step is queued on la->aux
@@ -496,19 +589,19 @@ int cholesky_lower(double* A, int n, int* d_info, double* work, cudaStream_t s,
     double* P = A + (j0 + nb) + static_cast<long long>(n) * j0;
     double* A22 = A + (j0 + nb) + static_cast<long long>(n) * (j0 + nb);
     if (!la) {
-      launches += gemm_impl(false, true, rest, rest, nb, -1.0, P, n, P, n, 1.0, A22, n, true, false, s);
+      launches += syrk_update(rest, rest, nb, P, n, A22, n, s);
       continue;
     }
     const int nb1 = std::min(NB, rest), rest2 = rest - nb1;
     cudaEventRecord(la->ev_panel, s);
     // the previous step's remainder also updated this next block column
     if (rest_pending) cudaStreamWaitEvent(s, la->ev_rest, 0);
-    launches += gemm_impl(false, true, rest, nb1, nb, -1.0, P, n, P, n, 1.0, A22, n, true, false, s);
+    launches += syrk_update(rest, nb1, nb, P, n, A22, n, s);
     rest_pending = rest2 > 0;
     if (rest_pending) {
       cudaStreamWaitEvent(la->aux, la->ev_panel, 0);
-      launches += gemm_impl(false, true, rest2, rest2, nb, -1.0, P + nb1, n, P + nb1, n, 1.0,
-                            A22 + nb1 + static_cast<long long>(n) * nb1, n, true, false, la->aux);
+      launches += syrk_update(rest2, rest2, nb, P + nb1, n, A22 + nb1 + static_cast<long long>(n) * nb1, n,
+                              la->aux);
       cudaEventRecord(la->ev_rest, la->aux);
     }
   }
