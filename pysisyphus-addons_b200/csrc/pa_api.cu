@@ -418,7 +418,11 @@ struct Ctx {
   // batched form: metric chains of different molecules on their own streams
   cudaStream_t smet[kNs3c] = {};
   cudaStream_t sscrw[kNs3c] = {};  // batched form: screening + folding (highest priority)
+  // batched form: folding of each L_ab class done by screening worker i (for
+  // the last molecule it folds, hence for all of its molecules)
+  cudaEvent_t ev_bra_w[kNs3c][2 * PA_LMAX + 1] = {};
   cudaEvent_t jmet[kNs3c] = {};
+  cudaEvent_t jscr[kNs3c] = {};  // batched form: screening worker i done
   // lookahead streams of the Cholesky factorization: la2 for the chains on
   // stream2 and for pa_cholesky_solve, la_met[i] for the chain on smet[i]
   CholLookahead la2;
@@ -469,6 +473,8 @@ int current_ctx(Ctx** out, DeviceTables* dt) {
     PA_CUDA(cudaStreamCreateWithPriority(&c->stream2, cudaStreamNonBlocking, prio_met));
     PA_CUDA(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
     for (auto& e : c->ev_bra) PA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (auto& row : c->ev_bra_w)
+      for (auto& e : row) PA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     PA_CUDA(cudaStreamCreateWithFlags(&c->scopy, cudaStreamNonBlocking));
     PA_CUDA(cudaEventCreateWithFlags(&c->ev_alloc, cudaEventDisableTiming));
     PA_CUDA(cudaEventCreateWithFlags(&c->ev_copied, cudaEventDisableTiming));
@@ -481,6 +487,7 @@ int current_ctx(Ctx** out, DeviceTables* dt) {
       PA_CUDA(cudaStreamCreateWithPriority(&c->smet[i], cudaStreamNonBlocking, prio_met));
       PA_CUDA(cudaStreamCreateWithPriority(&c->sscrw[i], cudaStreamNonBlocking, prio_hi));
       PA_CUDA(cudaEventCreateWithFlags(&c->jmet[i], cudaEventDisableTiming));
+      PA_CUDA(cudaEventCreateWithFlags(&c->jscr[i], cudaEventDisableTiming));
     }
     for (int i = 0; i <= Ctx::kNs3c; ++i) {
       CholLookahead& la = i < Ctx::kNs3c ? c->la_met[i] : c->la2;
@@ -1212,48 +1219,72 @@ struct BatchMol {
 int record_batch(Ctx* c, BatchPlan& plan, const std::vector<BatchMol>& mols, const DeviceTables& dt,
                  const Options& o, const std::vector<int>& class_lab, const std::vector<int>& class_lc,
                  const std::vector<const Df3cArgs*>& class_args_d, const std::vector<const int*>& class_off_d,
-                 const std::vector<int>& class_nm, const std::vector<int>& class_items, int* launches) {
+                 const std::vector<int>& class_nm, const std::vector<int>& class_items,
+                 const std::vector<Df3cArgs>& class_single, int* launches) {
   cudaStream_t s = c->stream;
   const int nmol = static_cast<int>(mols.size());
   constexpr int W = Ctx::kNs3c;
+  constexpr int NLAB = 2 * PA_LMAX + 1;
+  const int ncls = static_cast<int>(class_lab.size());
+  // the class counters are zeroed and the class streams forked first: each
+  // class launch then waits only for the folding of its own L_ab on every
+  // screening worker, so the three-center work starts while later classes
+  // are still folded (as in the single-molecule path)
+  if (ncls > 0) PA_CUDA(cudaMemsetAsync(plan.counters, 0, sizeof(int) * ncls, s));
   PA_CUDA(cudaEventRecord(c->fork, s));
   for (int i = 0; i < W; ++i) {
     PA_CUDA(cudaStreamWaitEvent(c->sscrw[i], c->fork, 0));
     PA_CUDA(cudaStreamWaitEvent(c->smet[i], c->fork, 0));
+    PA_CUDA(cudaStreamWaitEvent(c->s3c[i], c->fork, 0));
   }
   // per molecule: screening + folding on a screening worker (enqueued first:
   // the critical path), then the metric chain on a metric stream
+  const int nworkers = std::min(nmol, W);
   for (int m = 0; m < nmol; ++m) {
     const BatchMol& M = mols[m];
     DfBuffers& b = plan.bufs[m];
-    const int st = run_screening(M.orb, M.aux, dt, o, b, c->sscrw[m % W], launches);
+    const int w = m % W;
+    const int st = run_screening(M.orb, M.aux, dt, o, b, c->sscrw[w], launches);
     if (st != PA_OK) return st;
-    stage_bra_prep(M.orb, M.aux, M.nd, M.dens, M.sd, M.si, M.sj, b, o, c->sscrw[m % W], launches);
+    const bool last = m + W >= nmol;  // the worker's last molecule
+    stage_bra_prep(M.orb, M.aux, M.nd, M.dens, M.sd, M.si, M.sj, b, o, c->sscrw[w], launches,
+                   last ? c->ev_bra_w[w] : nullptr);
+    if (last)  // classes above this molecule's L_ab: done with everything before
+      for (int lab = M.orb->pairs.lab_max + 1; lab < NLAB; ++lab)
+        PA_CUDA(cudaEventRecord(c->ev_bra_w[w][lab], c->sscrw[w]));
   }
   for (int m = 0; m < nmol; ++m)
     stage_metric(mols[m].aux, plan.bufs[m], dt, o, c->smet[m % W], &c->la_met[m % W], launches);
-  for (int i = 0; i < W; ++i) {
-    PA_CUDA(cudaEventRecord(c->j3c[i], c->sscrw[i]));
-    PA_CUDA(cudaStreamWaitEvent(s, c->j3c[i], 0));
-  }
-  // one persistent launch per class over all molecules
-  const int ncls = static_cast<int>(class_lab.size());
-  if (ncls > 0) PA_CUDA(cudaMemsetAsync(plan.counters, 0, sizeof(int) * ncls, s));
-  PA_CUDA(cudaEventRecord(c->fork, s));
-  for (int i = 0; i < W; ++i) PA_CUDA(cudaStreamWaitEvent(c->s3c[i], c->fork, 0));
   // the classes come grouped by L_c: once a group is enqueued, the main stream
   // waits for the class streams and reduces that group of every molecule while
   // the next groups run (as the single-molecule path does)
   bool reduced[PA_LAUXMAX + 1] = {};
+  bool joined = false;  // the main stream has waited for the screening workers
   for (int k = 0; k < ncls; ++k) {
-    *launches += launch_df3c_class_batch(class_lab[k], class_lc[k], o.tile_variant[class_lab[k]][class_lc[k]],
-                                         class_args_d[k], class_off_d[k], class_nm[k],
-                                         class_items[k], plan.counters + k, c->s3c[k % W]);
+    for (int w = 0; w < nworkers; ++w)
+      PA_CUDA(cudaStreamWaitEvent(c->s3c[k % W], c->ev_bra_w[w][class_lab[k]], 0));
+    const int variant = o.tile_variant[class_lab[k]][class_lc[k]];
+    if (class_nm[k] == 1) {
+      // one molecule has items of this class: the single-molecule kernel, its
+      // descriptor a kernel parameter (the batched kernel reads it from
+      // shared memory on every use)
+      Df3cArgs a1 = class_single[k];
+      a1.counter = plan.counters + k;
+      *launches += launch_df3c_class(class_lab[k], class_lc[k], variant, a1, a1.nby, c->s3c[k % W]);
+    } else {
+      *launches += launch_df3c_class_batch(class_lab[k], class_lc[k], variant, class_args_d[k], class_off_d[k],
+                                           class_nm[k], class_items[k], plan.counters + k, c->s3c[k % W]);
+    }
     if (k + 1 == ncls || class_lc[k + 1] != class_lc[k]) {
       for (int i = 0; i < W; ++i) {
         PA_CUDA(cudaEventRecord(c->j3c[i], c->s3c[i]));
         PA_CUDA(cudaStreamWaitEvent(s, c->j3c[i], 0));
+        if (!joined) {  // the reductions read the screening's sorted lists
+          PA_CUDA(cudaEventRecord(c->jscr[i], c->sscrw[i]));
+          PA_CUDA(cudaStreamWaitEvent(s, c->jscr[i], 0));
+        }
       }
+      joined = true;
       for (int m = 0; m < nmol; ++m) stage_reduce_lc(mols[m].aux, mols[m].nd, plan.bufs[m], class_lc[k], s, launches);
       reduced[class_lc[k]] = true;
     }
@@ -1261,6 +1292,10 @@ int record_batch(Ctx* c, BatchPlan& plan, const std::vector<BatchMol>& mols, con
   for (int i = 0; i < W; ++i) {
     PA_CUDA(cudaEventRecord(c->j3c[i], c->s3c[i]));
     PA_CUDA(cudaStreamWaitEvent(s, c->j3c[i], 0));
+    if (!joined) {
+      PA_CUDA(cudaEventRecord(c->jscr[i], c->sscrw[i]));
+      PA_CUDA(cudaStreamWaitEvent(s, c->jscr[i], 0));
+    }
   }
   for (int lc = 0; lc <= PA_LAUXMAX; ++lc)  // groups without class launches (zero rows)
     if (!reduced[lc])
@@ -1401,6 +1436,7 @@ int batch_4d(int nmol, const pa_basis* orbs, const pa_basis* auxs, const int* nd
     std::vector<const Df3cArgs*> args_d;
     std::vector<const int*> off_d;
     std::vector<int> keep_lab, keep_lc;
+    std::vector<Df3cArgs> class_single;  // the first (heaviest) molecule's descriptor of each class
     for (size_t k = 0; k < class_lab.size(); ++k) {
       std::vector<std::pair<long long, Df3cArgs>> items;
       for (int m = 0; m < nmol; ++m) {
@@ -1428,6 +1464,7 @@ int batch_4d(int nmol, const pa_basis* orbs, const pa_basis* auxs, const int* nd
       keep_lab.push_back(class_lab[k]);
       keep_lc.push_back(class_lc[k]);
       class_nm.push_back(static_cast<int>(items.size()));
+      class_single.push_back(items[0].second);
       class_items.push_back(ho[items.size()]);
       args_d.push_back(d_args + slot * std::max(nmol, 1));
       off_d.push_back(d_off + slot * (std::max(nmol, 1) + 1));
@@ -1439,7 +1476,8 @@ int batch_4d(int nmol, const pa_basis* orbs, const pa_basis* auxs, const int* nd
     if (use_graph) {
       cudaGraph_t graph = nullptr;
       PA_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
-      st = record_batch(c, *plan, mols, dt, o, keep_lab, keep_lc, args_d, off_d, class_nm, class_items, &launches);
+      st = record_batch(c, *plan, mols, dt, o, keep_lab, keep_lc, args_d, off_d, class_nm, class_items,
+                        class_single, &launches);
       const cudaError_t ec = cudaStreamEndCapture(c->stream, &graph);
       if (st != PA_OK || ec != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
@@ -1460,7 +1498,8 @@ int batch_4d(int nmol, const pa_basis* orbs, const pa_basis* auxs, const int* nd
       plan->launches = launches;
     } else {
       PA_CUDA(cudaEventRecord(c->ev0, c->stream));
-      st = record_batch(c, *plan, mols, dt, o, keep_lab, keep_lc, args_d, off_d, class_nm, class_items, &launches);
+      st = record_batch(c, *plan, mols, dt, o, keep_lab, keep_lc, args_d, off_d, class_nm, class_items,
+                        class_single, &launches);
       plan->launches = launches;
       if (st != PA_OK) {
         cudaStreamSynchronize(c->stream);
