@@ -273,6 +273,14 @@ int pa_metric(pa_basis aux, double* metric);
  * (n x nrhs) by L^-1 B. PA_ERR_NOT_SPD when A is not positive definite. */
 int pa_cholesky_solve(int n, double* A, int nrhs, double* B);
 
+/* Diagnostic of the precision form's density product (no counterpart in the
+ * reference, which has no tensor-core path): C (m x n) = A (m x k) B^T
+ * (B: n x k), all row-major host arrays, computed by one block with the
+ * split-BF16 tcgen05 product of the weak-triplet three-center kernels (three
+ * BF16 slices per operand, six slice products accumulated in FP32 in tensor
+ * memory). 1 <= m <= 128, 1 <= n <= 48, 1 <= k <= 128. Synchronous. */
+int pa_split_product_check(int m, int n, int k, const double* A, const double* B, double* C);
+
 /* The estimator study (replaces intor/benchmark_wrapper.f90:13-37,
  * f_benchmark_int3c2e, same arguments): prints the basis sizes, the time and
  * the number of shell triplets the QVL estimate skips, and writes

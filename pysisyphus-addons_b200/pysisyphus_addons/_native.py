@@ -128,6 +128,7 @@ SIGNATURES = {
                              ctypes.POINTER(ctypes.c_longlong)],
     "f_eval_densities": _BASIS + [_i, _pd, _i, _i, _pd, _pd, _i, _d],
     "f_eval_prim_density": [_i, _i, _i, _pi, _pd, _pd, _pd, _d, _pd],
+    "pa_split_product_check": [_i, _i, _i, _pd, _pd, _pd],
 }
 
 _lib = None
