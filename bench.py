@@ -550,7 +550,10 @@ def main():
     step_stats = []  # statistics of every call of the last step
 
     def set_form(form):
-        if form in ("mixed", "mixed_batched") or (form == "batched" and args.precision == "mixed"):
+        # mixed_split_batched: the weak triplets on their own kernels with the
+        # split-BF16 tensor-core product (pa_set_mixed_kernels(1))
+        nat.set_mixed_kernels(1 if form == "mixed_split_batched" else 0)
+        if form in ("mixed", "mixed_batched", "mixed_split_batched") or (form == "batched" and args.precision == "mixed"):
             nat.set_precision("mixed", FP32_THRESH)
         else:
             nat.set_precision("fp64")
@@ -571,7 +574,7 @@ def main():
 
     # the measured forms, in order; the last one gives `value`
     if headline(args):
-        forms = [("fp64", "plain"), ("mixed_batched", "batched")]
+        forms = [("fp64", "plain"), ("mixed_split_batched", "batched"), ("mixed_batched", "batched")]
     elif args.config == "cfg4":
         forms = [("mixed" if args.precision == "mixed" else "fp64", "plain" if args.sequential else "batched")]
     else:
@@ -586,6 +589,7 @@ def main():
                 step()
         torch.cuda.synchronize()
         nat.set_precision("fp64")
+        nat.set_mixed_kernels(0)
         return
 
     clocks = Clocks(local)
@@ -625,6 +629,7 @@ def main():
                          "ms3c": ms3c, "phases": phases, "launches": lc, "launches_3c": lc3}
     clk = clocks.stop()
     nat.set_precision("fp64")
+    nat.set_mixed_kernels(0)
     head = results[forms[-1][0]]
     step_s, value = head["step_s"], head["value"]
 
@@ -633,12 +638,22 @@ def main():
     if headline(args):
         Rf = outs["fp64"][0].cpu().numpy()
         Rm = outs["mixed_batched"][0].cpu().numpy()
+        Rs = outs["mixed_split_batched"][0].cpu().numpy()
         dmax = float(np.abs(Rm - Rf).max())
+        smax = float(np.abs(Rs - Rf).max())
         form_report = {
             "fp64_plain": {"ms_per_step": results["fp64"]["step_s"] * 1e3, "value": results["fp64"]["value"]},
             "mixed_batched": {"ms_per_step": step_s * 1e3, "value": value},
             "speedup_mixed_batched_vs_fp64": results["fp64"]["step_s"] / step_s,
             "tensor_err_vs_fp64": {"max_abs": dmax, "rel_of_max": dmax / float(np.abs(Rf).max())},
+            "mixed_split_batched": {
+                "kernels": "weak triplets on k_df3c_w: FP32 X build, split-BF16 tcgen05 product (3 slices per "
+                           "operand, 6 products, FP32 accumulation per step, FP64 across steps)",
+                "ms_per_step": results["mixed_split_batched"]["step_s"] * 1e3,
+                "value": results["mixed_split_batched"]["value"],
+                "speedup_vs_fp64": results["fp64"]["step_s"] / results["mixed_split_batched"]["step_s"],
+                "tensor_err_vs_fp64": {"max_abs": smax, "rel_of_max": smax / float(np.abs(Rf).max())},
+            },
             "fp32_thresh": FP32_THRESH,
         }
 

@@ -142,8 +142,16 @@ int pa_set_metric_shift(double shift);
  * PA_PRECISION_FP64 (default) or PA_PRECISION_MIXED, in which shell triplets
  * with Schwarz bound Q_ab * Q_c < fp32_thresh (e.g. 1e-6) evaluate the Boys
  * function (below T = 27 / 30), the Hermite recurrence and the solid-harmonic
- * contraction in FP32; their contributions are accumulated in FP64. */
+ * contraction in FP32. pa_set_mixed_kernels picks how: 0 (default) inside the
+ * FP64 class kernels, whose density product stays FP64; 1 on separate
+ * weak-triplet kernels whose density product is a split-BF16 tensor-core
+ * product (three BF16 slices per operand, six slice products, FP32
+ * accumulation over one step, FP64 across steps), the other triplets on the
+ * FP64 kernels. Both keep the accumulation across triplets in FP64. The
+ * reference is FP64 only. */
 int pa_set_precision(int mode, double fp32_thresh);
+int pa_set_mixed_kernels(int mode);
+int pa_get_mixed_kernels(void);
 /* Granularity of the three-center work queue: work items per SM and shell
  * class; 0 (default) picks it from the system size (2 at 40 atoms, 32 at 200).
  * Finer items shorten the tail of each class launch and cost more partial

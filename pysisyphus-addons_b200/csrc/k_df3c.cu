@@ -81,6 +81,19 @@ int launch_df3c_reduce(const Df3cReduceArgs& r, cudaStream_t s) {
   return 1;
 }
 
+void df3c_class_info_w(int lab, int lc, Df3cClassInfo* ci) { rows()[lab].info_w[lc](ci); }
+
+int launch_df3c_class_w(int lab, int lc, const Df3cArgs& a, int ny, cudaStream_t s) {
+  return rows()[lab].launch_w[lc](a, ny, s);
+}
+
+void df3c_fill_items_w(int lab, int lc, Df3cArgs* a, int ny) { rows()[lab].fill_w[lc](a, ny); }
+
+int launch_df3c_class_batch_w(int lab, int lc, const Df3cArgs* d_args, const int* d_item_off, int nm,
+                              int total_items, int* counter, cudaStream_t s) {
+  return rows()[lab].batch_w[lc](d_args, d_item_off, nm, total_items, counter, s);
+}
+
 cudaError_t upload_sph_rownorm(const double* rownorm, cudaStream_t s) {
   for (int lab = 0; lab < kNLab; ++lab) {
     const cudaError_t e = rows()[lab].upload_rownorm(rownorm, s);

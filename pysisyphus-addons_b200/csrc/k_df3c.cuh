@@ -41,15 +41,22 @@ struct Df3cArgs {
   // the launch)
   int* counter = nullptr;
   int n_items = 0, nbx = 0, nby = 0, nbz = 0;
+  // weak-triplet kernels (precision form): a device flag set to 1 when a
+  // tensor-core completion wait gave up
+  int* err = nullptr;
 };
+
+// Class runs of one auxiliary L: an FP64 run per L_ab, and in the mixed form a
+// weak-triplet run beside each.
+constexpr int kMaxRunsPerLc = 2 * (2 * PA_LMAX + 1);
 
 struct Df3cReduceArgs {
   DevBasis X;
   int aux_slot0 = 0, n_aux = 0, nc = 1, nd = 0, naux = 0;
   const int* sorted_aux = nullptr;
   int nclasses = 0;
-  const double* part[2 * PA_LMAX + 1] = {};
-  int ny[2 * PA_LMAX + 1] = {};
+  const double* part[kMaxRunsPerLc] = {};
+  int ny[kMaxRunsPerLc] = {};
   double* df = nullptr;              // [naux][nd] column-major (naux rows)
 };
 
@@ -73,6 +80,12 @@ void df3c_fill_items(int lab, int lc, int variant, Df3cArgs* a, int ny);
 int launch_df3c_class_batch(int lab, int lc, int variant, const Df3cArgs* d_args, const int* d_item_off,
                             int nm, int total_items, int* counter, cudaStream_t s);
 int launch_df3c_reduce(const Df3cReduceArgs& r, cudaStream_t s);
+// The same four entry points for the weak-triplet kernels (k_df3c_w.cuh).
+void df3c_class_info_w(int lab, int lc, Df3cClassInfo* ci);
+int launch_df3c_class_w(int lab, int lc, const Df3cArgs& a, int ny, cudaStream_t s);
+void df3c_fill_items_w(int lab, int lc, Df3cArgs* a, int ny);
+int launch_df3c_class_batch_w(int lab, int lc, const Df3cArgs* d_args, const int* d_item_off, int nm,
+                              int total_items, int* counter, cudaStream_t s);
 // Row normalization of the solid harmonics (constant memory of every class
 // translation unit).
 cudaError_t upload_sph_rownorm(const double* rownorm, cudaStream_t s);
@@ -87,6 +100,11 @@ struct Df3cRow {
   InfoFn info[kDf3cVariants][PA_LAUXMAX + 1] = {};
   FillFn fill[kDf3cVariants][PA_LAUXMAX + 1] = {};
   BatchFn batch[kDf3cVariants][PA_LAUXMAX + 1] = {};
+  // weak-triplet kernels of the precision form (one shape per class)
+  LaunchFn launch_w[PA_LAUXMAX + 1] = {};
+  InfoFn info_w[PA_LAUXMAX + 1] = {};
+  FillFn fill_w[PA_LAUXMAX + 1] = {};
+  BatchFn batch_w[PA_LAUXMAX + 1] = {};
   cudaError_t (*upload_rownorm)(const double*, cudaStream_t) = nullptr;
 };
 void df3c_row_0(Df3cRow*);

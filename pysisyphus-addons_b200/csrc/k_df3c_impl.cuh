@@ -37,6 +37,7 @@
 #include "k_df3c.cuh"
 #include "md.cuh"
 #include "sph_raw.cuh"
+#include "umma.cuh"
 
 #include <algorithm>
 #include <utility>
@@ -845,11 +846,14 @@ cudaError_t upload_rownorm(const double* rownorm, cudaStream_t s) {
 
 }  // namespace pa
 
+#include "k_df3c_w.cuh"
+
 // Defines df3c_row_<LAB>(): the dispatch row of this translation unit's LAB.
 #define PA_DF3C_ROW(LAB)                       \
   namespace pa {                               \
   void df3c_row_##LAB(Df3cRow* row) {          \
     fill_row<LAB, 0>(row);                     \
+    fill_row_w<LAB, 0>(row);                   \
     row->upload_rownorm = &upload_rownorm;     \
   }                                            \
   }

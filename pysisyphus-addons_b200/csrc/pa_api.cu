@@ -613,10 +613,12 @@ struct DfBuffers {
   size_t cub_bytes;
   std::vector<long long> g_off;      // per Lab class
   int dw = 8;                        // density chunk width of G (multiple of 8, <= 40)
+  bool split = false;                // mixed form: the weak triplets run on their own kernels
   struct ClassRun {
     int lab, lc, ny, upc;
     double* partial;
     int variant;  // tile-shape variant of the class kernel
+    bool weak;    // weak-triplet kernel (mixed form)
   };
   std::vector<ClassRun> runs;
 };
@@ -693,6 +695,8 @@ void layout_df(Carver& c, const pa_basis_s* orb, const pa_basis_s* aux, int nd, 
     b->g_off[lab + 1] = b->g_off[lab] + nu * ncum(lab) * nz * b->dw;
   }
   b->G = c.take<double>(b->g_off[P.lab_max + 1]);
+  b->split = o.precision == PA_PRECISION_MIXED && o.mixed_kernels != 0 && o.fp32_thresh > o.screen_thresh;
+
   b->M = c.take<double>(naux * naux);
   b->lawork = c.take<double>(linalg_workspace_doubles(static_cast<int>(naux)));
   b->df_raw = c.take<double>(static_cast<size_t>(naux) * nd);
@@ -724,20 +728,26 @@ void layout_df(Carver& c, const pa_basis_s* orb, const pa_basis_s* aux, int nd, 
       const int nu = P.class_off[lab + 1] - P.class_off[lab];
       if (nu == 0) continue;
       const int variant = o.tile_variant[lab][lc];
-      Df3cClassInfo ci;
-      df3c_class_info(lab, lc, variant, &ci);
-      const int bx = (nxc + ci.tc - 1) / ci.tc;
-      const int bz = nz;
-      const int target = items_per_sm * 148;  // work items per class (persistent blocks pull them)
-      int ny = std::max(1, (target + bx * bz - 1) / (bx * bz));
-      const int max_ny = (nu + ci.ub - 1) / ci.ub;
-      ny = std::min(ny, max_ny);
-      int upc = (nu + ny - 1) / ny;
-      upc = ((upc + ci.ub - 1) / ci.ub) * ci.ub;
-      ny = (nu + upc - 1) / upc;
-      DfBuffers::ClassRun r{lab, lc, ny, upc, nullptr, variant};
-      b->runs.push_back(r);
-      part_total += static_cast<size_t>(ny) * nxc * (2 * lc + 1) * nd;
+      // the FP64 run, then (mixed form) the weak-triplet run of the class
+      for (int weak = 0; weak <= (b->split ? 1 : 0); ++weak) {
+        Df3cClassInfo ci;
+        if (weak)
+          df3c_class_info_w(lab, lc, &ci);
+        else
+          df3c_class_info(lab, lc, variant, &ci);
+        const int bx = (nxc + ci.tc - 1) / ci.tc;
+        const int bz = nz;
+        const int target = items_per_sm * 148;  // work items per class (persistent blocks pull them)
+        int ny = std::max(1, (target + bx * bz - 1) / (bx * bz));
+        const int max_ny = (nu + ci.ub - 1) / ci.ub;
+        ny = std::min(ny, max_ny);
+        int upc = (nu + ny - 1) / ny;
+        upc = ((upc + ci.ub - 1) / ci.ub) * ci.ub;
+        ny = (nu + upc - 1) / upc;
+        DfBuffers::ClassRun r{lab, lc, ny, upc, nullptr, variant, weak != 0};
+        b->runs.push_back(r);
+        part_total += static_cast<size_t>(ny) * nxc * (2 * lc + 1) * nd;
+      }
     }
   }
   double* part = c.take<double>(part_total);
@@ -863,6 +873,12 @@ Df3cArgs class_args(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const 
   a.boys_mode = o.boys_mode;
   a.thresh = o.screen_thresh;
   a.thr32 = o.precision == PA_PRECISION_MIXED ? o.fp32_thresh : 0.0;
+  if (b.split && !r.weak) {
+    // the FP64 kernel takes the strong triplets only (Q_ab Q_c >= thr32)
+    a.thresh = std::max(o.screen_thresh, o.fp32_thresh);
+    a.thr32 = 0.0;
+  }
+  if (r.weak) a.err = b.info + 2;
   a.unit_slot0 = P.class_off[r.lab];
   a.n_units = P.class_off[r.lab + 1] - P.class_off[r.lab];
   a.unit_Q = b.slot_Q;
@@ -903,6 +919,7 @@ void stage_reduce_lc(const pa_basis_s* aux, int nd, DfBuffers& b, int lc, cudaSt
     ra.nclasses = 0;
     for (const auto& r : b.runs)
       if (r.lc == lc) {
+        if (ra.nclasses >= kMaxRunsPerLc) break;  // unreachable: layout_df makes at most two runs per (L_ab, L_c)
         ra.part[ra.nclasses] = r.partial;
         ra.ny[ra.nclasses] = r.ny;
         ++ra.nclasses;
@@ -958,6 +975,7 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
   const bool run3c = nd > 0 && !b.runs.empty();
   if (run3c) {
     PA_CUDA(cudaMemsetAsync(b.counters, 0, sizeof(int) * b.runs.size(), s));
+    PA_CUDA(cudaMemsetAsync(b.info + 2, 0, sizeof(int), s));
     PA_CUDA(cudaEventRecord(ctx->fork, s));
     for (int i = 0; i < Ctx::kNs3c; ++i) PA_CUDA(cudaStreamWaitEvent(ctx->s3c[i], ctx->fork, 0));
   }
@@ -984,7 +1002,8 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
       cudaStream_t cs = ctx->s3c[o.class_timing ? 0 : ri % Ctx::kNs3c];
       PA_CUDA(cudaStreamWaitEvent(cs, ctx->ev_bra[r.lab], 0));
       if (o.class_timing) PA_CUDA(cudaEventRecord(ctx->ct_ev[2 * ri], cs));
-      *launches += launch_df3c_class(r.lab, r.lc, r.variant, a, r.ny, cs);
+      *launches += r.weak ? launch_df3c_class_w(r.lab, r.lc, a, r.ny, cs)
+                          : launch_df3c_class(r.lab, r.lc, r.variant, a, r.ny, cs);
       if (o.class_timing) PA_CUDA(cudaEventRecord(ctx->ct_ev[2 * ri + 1], cs));
       if (ri + 1 == nr || b.runs[ri + 1].lc != r.lc) {
         for (int i = 0; i < Ctx::kNs3c; ++i) {
@@ -1004,7 +1023,7 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
 int finish(Ctx* c, const DfBuffers& b, cudaStream_t s, int launches, float* ms) {
   PA_CUDA(cudaGetLastError());
   PA_CUDA(cudaEventRecord(c->ev1, s));
-  PA_CUDA(cudaMemcpyAsync(c->h_info, b.info, sizeof(int), cudaMemcpyDeviceToHost, s));
+  PA_CUDA(cudaMemcpyAsync(c->h_info, b.info, sizeof(int) * 4, cudaMemcpyDeviceToHost, s));
   PA_CUDA(cudaStreamSynchronize(s));
   PA_CUDA(cudaEventElapsedTime(ms, c->ev0, c->ev1));
   float t[5];
@@ -1030,6 +1049,8 @@ int finish(Ctx* c, const DfBuffers& b, cudaStream_t s, int launches, float* ms) 
     std::lock_guard<std::mutex> lk(g_ct_mu);
     g_class_times = std::move(ct);
   }
+  if (b.split && c->h_info[2] != 0)
+    return fail(PA_ERR_TIMEOUT, "weak-triplet kernel: a tensor-core completion wait gave up");
   if (*c->h_info != 0)
     return fail(PA_ERR_NOT_SPD, "metric (P|Q) is not positive definite (Cholesky pivot " +
                                     std::to_string(*c->h_info) + ")");
@@ -1218,9 +1239,9 @@ struct BatchMol {
 // Records the whole batch on c->stream (the origin of a capture when graphed).
 int record_batch(Ctx* c, BatchPlan& plan, const std::vector<BatchMol>& mols, const DeviceTables& dt,
                  const Options& o, const std::vector<int>& class_lab, const std::vector<int>& class_lc,
-                 const std::vector<const Df3cArgs*>& class_args_d, const std::vector<const int*>& class_off_d,
-                 const std::vector<int>& class_nm, const std::vector<int>& class_items,
-                 const std::vector<Df3cArgs>& class_single, int* launches) {
+                 const std::vector<int>& class_weak, const std::vector<const Df3cArgs*>& class_args_d,
+                 const std::vector<const int*>& class_off_d, const std::vector<int>& class_nm,
+                 const std::vector<int>& class_items, const std::vector<Df3cArgs>& class_single, int* launches) {
   cudaStream_t s = c->stream;
   const int nmol = static_cast<int>(mols.size());
   constexpr int W = Ctx::kNs3c;
@@ -1231,6 +1252,8 @@ int record_batch(Ctx* c, BatchPlan& plan, const std::vector<BatchMol>& mols, con
   // screening worker, so the three-center work starts while later classes
   // are still folded (as in the single-molecule path)
   if (ncls > 0) PA_CUDA(cudaMemsetAsync(plan.counters, 0, sizeof(int) * ncls, s));
+  // status words of every molecule (the weak-triplet kernels' flag among them)
+  PA_CUDA(cudaMemsetAsync(plan.infos, 0, sizeof(int) * 4 * std::max(nmol, 1), s));
   PA_CUDA(cudaEventRecord(c->fork, s));
   for (int i = 0; i < W; ++i) {
     PA_CUDA(cudaStreamWaitEvent(c->sscrw[i], c->fork, 0));
@@ -1270,7 +1293,11 @@ int record_batch(Ctx* c, BatchPlan& plan, const std::vector<BatchMol>& mols, con
       // shared memory on every use)
       Df3cArgs a1 = class_single[k];
       a1.counter = plan.counters + k;
-      *launches += launch_df3c_class(class_lab[k], class_lc[k], variant, a1, a1.nby, c->s3c[k % W]);
+      *launches += class_weak[k] ? launch_df3c_class_w(class_lab[k], class_lc[k], a1, a1.nby, c->s3c[k % W])
+                                 : launch_df3c_class(class_lab[k], class_lc[k], variant, a1, a1.nby, c->s3c[k % W]);
+    } else if (class_weak[k]) {
+      *launches += launch_df3c_class_batch_w(class_lab[k], class_lc[k], class_args_d[k], class_off_d[k], class_nm[k],
+                                             class_items[k], plan.counters + k, c->s3c[k % W]);
     } else {
       *launches += launch_df3c_class_batch(class_lab[k], class_lc[k], variant, class_args_d[k], class_off_d[k],
                                            class_nm[k], class_items[k], plan.counters + k, c->s3c[k % W]);
@@ -1361,7 +1388,7 @@ int batch_4d(int nmol, const pa_basis* orbs, const pa_basis* auxs, const int* nd
   const Options o = options();
   // signature of the batch: options, then per molecule handles, sizes, pointers
   std::vector<long long> sig{nmol, layout, use_graph ? 1 : 0, o.boys_mode, o.skip_metric, o.precision,
-                             o.items_per_sm, o.screening};
+                             o.mixed_kernels, o.items_per_sm, o.screening};
   for (const auto& row : o.tile_variant)
     for (signed char v : row) sig.push_back(v);
   for (double v : {o.screen_thresh, o.fp32_thresh, o.metric_shift}) {
@@ -1393,16 +1420,18 @@ int batch_4d(int nmol, const pa_basis* orbs, const pa_basis* auxs, const int* nd
     plan->df.resize(nmol);
     plan->gram.resize(nmol);
     // classes present in the batch, and for each the molecules' runs
-    std::vector<int> class_lab, class_lc, class_nm, class_items;
-    std::vector<std::vector<std::pair<int, int>>> class_runs;  // (molecule, run index)
+    std::vector<int> class_lab, class_lc, class_weak, class_nm, class_items;
     // classes grouped by auxiliary L, highest first (as the single-molecule
-    // path orders its class launches)
+    // path orders its class launches); in the mixed form every class has an
+    // FP64 run and a weak-triplet run
+    const bool split = o.precision == PA_PRECISION_MIXED && o.mixed_kernels != 0 && o.fp32_thresh > o.screen_thresh;
     for (int lc = PA_LAUXMAX; lc >= 0; --lc)
-      for (int lab = 0; lab <= 2 * PA_LMAX; ++lab) {
-        class_lab.push_back(lab);
-        class_lc.push_back(lc);
-        class_runs.emplace_back();
-      }
+      for (int lab = 0; lab <= 2 * PA_LMAX; ++lab)
+        for (int weak = 0; weak <= (split ? 1 : 0); ++weak) {
+          class_lab.push_back(lab);
+          class_lc.push_back(lc);
+          class_weak.push_back(weak);
+        }
     // count, allocate, carve
     std::vector<size_t> off(nmol + 1, 0);
     for (int pass = 0; pass < 2; ++pass) {
@@ -1435,7 +1464,7 @@ int batch_4d(int nmol, const pa_basis* orbs, const pa_basis* auxs, const int* nd
     std::vector<int> h_off(class_lab.size() * (std::max(nmol, 1) + 1), 0);
     std::vector<const Df3cArgs*> args_d;
     std::vector<const int*> off_d;
-    std::vector<int> keep_lab, keep_lc;
+    std::vector<int> keep_lab, keep_lc, keep_weak;
     std::vector<Df3cArgs> class_single;  // the first (heaviest) molecule's descriptor of each class
     for (size_t k = 0; k < class_lab.size(); ++k) {
       std::vector<std::pair<long long, Df3cArgs>> items;
@@ -1443,9 +1472,12 @@ int batch_4d(int nmol, const pa_basis* orbs, const pa_basis* auxs, const int* nd
         const BatchMol& M = mols[m];
         const DfBuffers& b = plan->bufs[m];
         for (const auto& r : b.runs) {
-          if (r.lab != class_lab[k] || r.lc != class_lc[k]) continue;
+          if (r.lab != class_lab[k] || r.lc != class_lc[k] || r.weak != (class_weak[k] != 0)) continue;
           Df3cArgs a = class_args(M.orb, M.aux, M.nd, b, dt, o, r);
-          df3c_fill_items(r.lab, r.lc, r.variant, &a, r.ny);
+          if (r.weak)
+            df3c_fill_items_w(r.lab, r.lc, &a, r.ny);
+          else
+            df3c_fill_items(r.lab, r.lc, r.variant, &a, r.ny);
           const long long work = static_cast<long long>(a.n_units) * a.n_aux * a.nd;
           if (a.n_items > 0) items.push_back({work, a});
         }
@@ -1463,6 +1495,7 @@ int batch_4d(int nmol, const pa_basis* orbs, const pa_basis* auxs, const int* nd
       }
       keep_lab.push_back(class_lab[k]);
       keep_lc.push_back(class_lc[k]);
+      keep_weak.push_back(class_weak[k]);
       class_nm.push_back(static_cast<int>(items.size()));
       class_single.push_back(items[0].second);
       class_items.push_back(ho[items.size()]);
@@ -1476,8 +1509,8 @@ int batch_4d(int nmol, const pa_basis* orbs, const pa_basis* auxs, const int* nd
     if (use_graph) {
       cudaGraph_t graph = nullptr;
       PA_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
-      st = record_batch(c, *plan, mols, dt, o, keep_lab, keep_lc, args_d, off_d, class_nm, class_items,
-                        class_single, &launches);
+      st = record_batch(c, *plan, mols, dt, o, keep_lab, keep_lc, keep_weak, args_d, off_d, class_nm,
+                        class_items, class_single, &launches);
       const cudaError_t ec = cudaStreamEndCapture(c->stream, &graph);
       if (st != PA_OK || ec != cudaSuccess) {
         if (graph) cudaGraphDestroy(graph);
@@ -1498,8 +1531,8 @@ int batch_4d(int nmol, const pa_basis* orbs, const pa_basis* auxs, const int* nd
       plan->launches = launches;
     } else {
       PA_CUDA(cudaEventRecord(c->ev0, c->stream));
-      st = record_batch(c, *plan, mols, dt, o, keep_lab, keep_lc, args_d, off_d, class_nm, class_items,
-                        class_single, &launches);
+      st = record_batch(c, *plan, mols, dt, o, keep_lab, keep_lc, keep_weak, args_d, off_d, class_nm,
+                        class_items, class_single, &launches);
       plan->launches = launches;
       if (st != PA_OK) {
         cudaStreamSynchronize(c->stream);
@@ -1531,15 +1564,21 @@ int batch_4d(int nmol, const pa_basis* orbs, const pa_basis* auxs, const int* nd
     std::vector<int> infos(plan->h_infos, plan->h_infos + 4 * std::max(nm, 1));
     delete plan;
     for (int m = 0; m < nm; ++m)
+      if (infos[4 * m + 2] != 0)
+        return fail(PA_ERR_TIMEOUT, "molecule " + std::to_string(m) + ": weak-triplet kernel: a tensor-core completion wait gave up");
+    for (int m = 0; m < nm; ++m)
       if (infos[4 * m] != 0)
         return fail(PA_ERR_NOT_SPD, "molecule " + std::to_string(m) + ": metric (P|Q) is not positive definite (Cholesky pivot " +
                                         std::to_string(infos[4 * m]) + ")");
     return PA_OK;
   }
-  for (int m = 0; m < nmol; ++m)
+  for (int m = 0; m < nmol; ++m) {
+    if (plan->h_infos[4 * m + 2] != 0)
+      return fail(PA_ERR_TIMEOUT, "molecule " + std::to_string(m) + ": weak-triplet kernel: a tensor-core completion wait gave up");
     if (plan->h_infos[4 * m] != 0)
       return fail(PA_ERR_NOT_SPD, "molecule " + std::to_string(m) + ": metric (P|Q) is not positive definite (Cholesky pivot " +
                                       std::to_string(plan->h_infos[4 * m]) + ")");
+  }
   return PA_OK;
 }
 
@@ -1828,6 +1867,18 @@ int pa_set_precision(int mode, double fp32_thresh) {
 int pa_get_precision(void) {
   std::lock_guard<std::mutex> lk(g_opt_mu);
   return g_opts.precision;
+}
+
+int pa_set_mixed_kernels(int mode) {
+  if (mode != 0 && mode != 1) return fail(PA_ERR_ARG, "mixed-form kernels: 0 (FP32 recurrences in the FP64 kernels) or 1 (weak-triplet kernels)");
+  std::lock_guard<std::mutex> lk(g_opt_mu);
+  g_opts.mixed_kernels = mode;
+  return PA_OK;
+}
+
+int pa_get_mixed_kernels(void) {
+  std::lock_guard<std::mutex> lk(g_opt_mu);
+  return g_opts.mixed_kernels;
 }
 
 int pa_set_screening(int mode) {

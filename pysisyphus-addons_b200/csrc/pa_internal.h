@@ -88,6 +88,10 @@ struct Options {
   double metric_shift = 0.0;  // added to the diagonal of (P|Q) before the Cholesky
   int precision = 0;          // 0 = FP64 throughout, 1 = mixed (FP32 recurrences for weak triplets)
   double fp32_thresh = 1e-6;  // Schwarz bound below which the mixed form uses FP32
+  // mixed form: 0 = FP32 recurrences inside the FP64 class kernels (default),
+  // 1 = the weak triplets on their own kernels (FP32 X, split-BF16
+  // tensor-core product)
+  int mixed_kernels = 0;
   int items_per_sm = 0;       // work items per SM and class of the three-center kernel (0 = by size)
   int screening = 0;          // triplet estimate: 0 = Schwarz (reference), 1 = QVL
   int class_timing = 0;       // 1: class launches serialized on one stream, each timed with events

@@ -95,6 +95,8 @@ SIGNATURES = {
     "pa_set_precision": [_i, _d],
     "pa_set_items_per_sm": [_i],
     "pa_get_precision": [],
+    "pa_set_mixed_kernels": [_i],
+    "pa_get_mixed_kernels": [],
     "pa_set_screening": [_i],
     "pa_get_screening": [],
     "pa_get_stats": [ctypes.POINTER(PaStats)],
@@ -196,6 +198,17 @@ def set_precision(mode="fp64", fp32_thresh=1e-6):
     Schwarz bound is below fp32_thresh."""
     code = {"fp64": PA_PRECISION_FP64, "mixed": PA_PRECISION_MIXED}.get(mode, mode)
     check(load().pa_set_precision(int(code), float(fp32_thresh)))
+
+
+def set_mixed_kernels(mode):
+    """Kernels of the mixed form: 0 (default) keeps the weak triplets in the
+    FP64 class kernels with FP32 recurrences, 1 runs them on their own kernels
+    with the split-BF16 tensor-core product."""
+    check(load().pa_set_mixed_kernels(int(mode)))
+
+
+def get_mixed_kernels():
+    return int(load().pa_get_mixed_kernels())
 
 
 def set_items_per_sm(items):
