@@ -152,8 +152,12 @@ int pa_set_metric_shift(double shift);
 int pa_set_precision(int mode, double fp32_thresh);
 int pa_set_mixed_kernels(int mode);
 int pa_get_mixed_kernels(void);
+/* Grid of the three-center class launches (process-wide): 0 (default) =
+ * persistent blocks that pull work items until none is left, 1 = one block
+ * per work item. */
+int pa_set_class_grid(int mode);
 /* Granularity of the three-center work queue: work items per SM and shell
- * class; 0 (default) picks it from the system size (2 at 40 atoms, 32 at 200).
+ * class; 0 (default) picks it from the system size (2 at 40 atoms, 8 at 200).
  * Finer items shorten the tail of each class launch and cost more partial
  * sums. */
 int pa_set_items_per_sm(int items);

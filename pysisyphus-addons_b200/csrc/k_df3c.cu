@@ -5,6 +5,7 @@
 #include "k_df3c.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 
 namespace pa {
@@ -54,7 +55,15 @@ const Df3cRow* rows() {
 
 int checked(int v) { return (v >= 0 && v < kDf3cVariants) ? v : 0; }
 
+std::atomic<int> g_block_per_item{0};
+
 }  // namespace
+
+int df3c_grid(int n_items, int resident) {
+  return g_block_per_item.load(std::memory_order_relaxed) ? n_items : std::min(n_items, resident);
+}
+
+void set_df3c_block_per_item(int on) { g_block_per_item.store(on ? 1 : 0, std::memory_order_relaxed); }
 
 void df3c_class_info(int lab, int lc, int variant, Df3cClassInfo* ci) {
   rows()[lab].info[checked(variant)][lc](ci);

@@ -22,7 +22,6 @@ struct Df3cArgs {
   const double4* slot_pP = nullptr;  // [slot] (p, P)
   const double* G = nullptr;         // class base: [z][s][tuv][dw]
   int dw = 8;                        // density chunk width (multiple of 8, <= 40)
-  int units_per_chunk = 1;
   // auxiliary shells of class LC, sorted by Schwarz value (descending)
   int aux_slot0 = 0, n_aux = 0;
   const int* sorted_aux = nullptr;   // [slot] -> shell
@@ -89,6 +88,14 @@ int launch_df3c_class_batch_w(int lab, int lc, const Df3cArgs* d_args, const int
 // Row normalization of the solid harmonics (constant memory of every class
 // translation unit).
 cudaError_t upload_sph_rownorm(const double* rownorm, cudaStream_t s);
+
+// Grid of a class launch of n_items work items when `resident` blocks fit the
+// device: persistent (min(n_items, resident) blocks that pull items until none
+// is left), or one block per item (set_df3c_block_per_item(1)), whose blocks
+// retire item by item so that higher-priority streams (the metric chain) get
+// SM slots while the class runs.
+int df3c_grid(int n_items, int resident);
+void set_df3c_block_per_item(int on);
 
 // Dispatch row of one LAB (defined by k_df3c_l<LAB>.cu).
 struct Df3cRow {

@@ -427,6 +427,21 @@ __device__ __forceinline__ double triplet_estimate(const Df3cArgs& a, int us, in
   return uq * kPi * 1.4142135623730951 * aq.z / (a.slot_den[a.unit_slot0 + us] * RL);
 }
 
+// First unit slot i (class-relative, 0..n_units) with unit_Q[i] * q < bound:
+// the unit Schwarz values are sorted in descending order, so the products are
+// non-increasing. Evaluated alike by every thread (the same loads, in order).
+__device__ __forceinline__ int first_unit_below(const Df3cArgs& a, double bound, double q) {
+  int lo = 0, hi = a.n_units;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (a.unit_Q[a.unit_slot0 + mid] * q < bound)
+      hi = mid;
+    else
+      lo = mid + 1;
+  }
+  return lo;
+}
+
 // One work item: aux tile bx (TC shells), bra-unit chunk by, density chunk bz.
 template <int LAB, int LC, int V>
 __device__ __forceinline__ void df3c_item(const Df3cArgs& a, int bx, int by, int bz, double* smem) {
@@ -447,8 +462,6 @@ __device__ __forceinline__ void df3c_item(const Df3cArgs& a, int bx, int by, int
   const int d0 = z * a.dw;
   const int ndc = min(a.dw, a.nd - d0);
   const int nt_rt = a.dw / 8;  // n-tiles of this launch (dw multiple of 8, <= 40)
-  const int ub = by * a.units_per_chunk;
-  const int ue = min(a.n_units, ub + a.units_per_chunk);
 
   if (tid < C::TC) {
     if (tid < tile_n) {
@@ -470,6 +483,13 @@ __device__ __forceinline__ void df3c_item(const Df3cArgs& a, int bx, int by, int
   const double qc_max = tile_n > 0 ? c_C[0].w : 0.0;
   const double thr = a.thresh;
   const IndexTables* it = a.dt.idx;
+  // the units that can meet the tile form a prefix of the sorted class (the
+  // staircase); the item takes chunk `by` of nby equal chunks of that prefix,
+  // so every item of a tile has the same number of steps
+  const int ue0 = first_unit_below(a, thr, qc_max);
+  const int cs = (ue0 + a.nby - 1) / a.nby;
+  const int ub = by * cs;
+  const int ue = min(ue0, ub + cs);
   const int g = lane >> 2, t4 = lane & 3;
   // DMMA work of this warp: its first row tile and its k slice (warps past
   // MT * KSPLIT get slice KSPLIT, which has no k steps)
@@ -774,7 +794,7 @@ int launch_class(const Df3cArgs& a, int ny, cudaStream_t s) {
   Df3cArgs b = a;
   fill_items<LAB, LC, V>(&b, ny);
   if (b.n_items == 0) return 0;
-  k_df3c<LAB, LC, V><<<std::min(b.n_items, resident), kThreads, smem, s>>>(b);
+  k_df3c<LAB, LC, V><<<df3c_grid(b.n_items, resident), kThreads, smem, s>>>(b);
   return 1;
 }
 
@@ -786,8 +806,8 @@ int launch_class_batch(const Df3cArgs* d_args, const int* d_item_off, int nm, in
   static int occ[64] = {};
   const int resident = resident_blocks(k_df3c_batch<LAB, LC, V>, smem, occ);
   if (total_items <= 0 || nm <= 0) return 0;
-  k_df3c_batch<LAB, LC, V><<<std::min(total_items, resident), kThreads, smem, s>>>(d_args, d_item_off, nm,
-                                                                                 counter);
+  k_df3c_batch<LAB, LC, V><<<df3c_grid(total_items, resident), kThreads, smem, s>>>(d_args, d_item_off, nm,
+                                                                                     counter);
   return 1;
 }
 

@@ -269,21 +269,6 @@ __device__ __forceinline__ void x_triplet_team_w(const Df3cArgs& a, const uchar4
   }
 }
 
-// First unit slot i (class-relative, 0..n_units) with unit_Q[i] * q < bound:
-// the unit Schwarz values are sorted in descending order, so the products are
-// non-increasing. Evaluated alike by every thread (the same loads, in order).
-__device__ __forceinline__ int first_unit_below(const Df3cArgs& a, double bound, double q) {
-  int lo = 0, hi = a.n_units;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (a.unit_Q[a.unit_slot0 + mid] * q < bound)
-      hi = mid;
-    else
-      lo = mid + 1;
-  }
-  return lo;
-}
-
 // One work item of the weak kernel (same item decomposition as df3c_item).
 // Returns false when a tensor-core completion wait gave up (uniform over the
 // block).
@@ -635,7 +620,7 @@ int launch_class_w(const Df3cArgs& a, int ny, cudaStream_t s) {
   Df3cArgs b = a;
   fill_items_w<LAB, LC>(&b, ny);
   if (b.n_items == 0) return 0;
-  k_df3c_w<LAB, LC><<<std::min(b.n_items, resident), kThreads, C::SMEM, s>>>(b);
+  k_df3c_w<LAB, LC><<<df3c_grid(b.n_items, resident), kThreads, C::SMEM, s>>>(b);
   return 1;
 }
 
@@ -645,7 +630,8 @@ int launch_class_w_batch(const Df3cArgs* d_args, const int* d_item_off, int nm, 
   using C = CfgW<LAB, LC>;
   const int resident = weak_resident<LAB, LC>(k_df3c_w_batch<LAB, LC>);
   if (total_items <= 0 || nm <= 0) return 0;
-  k_df3c_w_batch<LAB, LC><<<std::min(total_items, resident), kThreads, C::SMEM, s>>>(d_args, d_item_off, nm, counter);
+  k_df3c_w_batch<LAB, LC><<<df3c_grid(total_items, resident), kThreads, C::SMEM, s>>>(d_args, d_item_off, nm,
+                                                                                        counter);
   return 1;
 }
 

@@ -710,11 +710,12 @@ void layout_df(Carver& c, const pa_basis_s* orb, const pa_basis_s* aux, int nd, 
   b->cub_bytes = cub_temp_bytes(orb, aux);
   b->cub_tmp = c.take<char>(b->cub_bytes);
   // partial slabs; the work-item granularity grows with the system size (on
-  // B200: 2 items per SM and class at 40 atoms, 32 at 200 atoms were best)
+  // B200, with every item a chunk of its tile's surviving units: 2 items per
+  // SM and class at 40 atoms, 8 at 200 atoms were best)
   if (items_per_sm <= 0) {
     const double T = static_cast<double>(P.npairs) * aux->host.shells.size();
     items_per_sm = static_cast<int>(std::lround(2.0 * std::pow(std::max(T, 1.0) / 1.85e7, 0.55)));
-    items_per_sm = std::min(32, std::max(2, items_per_sm));
+    items_per_sm = std::min(8, std::max(2, items_per_sm));
   }
   b->runs.clear();
   size_t part_total = 0;
@@ -885,7 +886,6 @@ Df3cArgs class_args(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const 
   a.slot_pP = b.slot_pP;
   a.G = b.G + b.g_off[r.lab];
   a.dw = b.dw;
-  a.units_per_chunk = r.upc;
   a.aux_slot0 = X.class_off[r.lc];
   a.n_aux = X.class_off[r.lc + 1] - X.class_off[r.lc];
   a.sorted_aux = b.sorted_aux;
@@ -1867,6 +1867,12 @@ int pa_set_precision(int mode, double fp32_thresh) {
 int pa_get_precision(void) {
   std::lock_guard<std::mutex> lk(g_opt_mu);
   return g_opts.precision;
+}
+
+int pa_set_class_grid(int mode) {
+  if (mode != 0 && mode != 1) return fail(PA_ERR_ARG, "class grid: 0 (persistent blocks) or 1 (one block per work item)");
+  pa::set_df3c_block_per_item(mode);
+  return PA_OK;
 }
 
 int pa_set_mixed_kernels(int mode) {

@@ -96,6 +96,7 @@ SIGNATURES = {
     "pa_set_items_per_sm": [_i],
     "pa_get_precision": [],
     "pa_set_mixed_kernels": [_i],
+    "pa_set_class_grid": [_i],
     "pa_get_mixed_kernels": [],
     "pa_set_screening": [_i],
     "pa_get_screening": [],
