@@ -59,6 +59,13 @@ def test_noalloc_cholesky_matches_allocating_entry_point():
         np.testing.assert_allclose(np.tril(L), np.tril(Lref), atol=1e-12 * np.abs(Lref).max(), rtol=0)
         np.testing.assert_array_equal(np.triu(L, 1), np.triu(A, 1))
         np.testing.assert_allclose(Y, Yref, atol=1e-12 * np.abs(Yref).max(), rtol=0)
+        # and directly against LAPACK (numpy's factor, scipy's triangular solve)
+        from scipy.linalg import solve_triangular
+
+        Lnp = np.linalg.cholesky(A)
+        np.testing.assert_allclose(np.tril(L), Lnp, atol=1e-12 * np.abs(Lnp).max(), rtol=0)
+        Ynp = solve_triangular(Lnp, B, lower=True)
+        np.testing.assert_allclose(Y, Ynp, atol=1e-12 * np.abs(Ynp).max(), rtol=0)
 
 
 def test_noalloc_cholesky_rejects_oversized_requests():
