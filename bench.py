@@ -86,7 +86,8 @@ def metric_name(args):
         form = "mixed precision" if args.precision == "mixed" else "FP64 plain"
         path = "Coulomb tensors of the batch, one call per molecule" if args.sequential else "batched Coulomb tensors"
     else:
-        form = "mixed precision" if args.form == "mixed" else "FP64 plain"
+        form = {"mixed": "mixed precision", "mixed_split": "mixed precision, split-BF16 tensor-core product"}.get(
+            args.form, "FP64 plain")
         path = "Coulomb tensor"
     if args.screening == "qvl":
         form += ", QVL screening"
@@ -101,9 +102,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default=CONFIG_KEY, choices=["cfg1", "cfg2", "cfg5", "cfg4"])
-    ap.add_argument("--form", default="headline", choices=["headline", "fp64", "mixed"],
-                    help="single-molecule workloads: headline = FP64 plain and mixed + batched back to back "
-                         "(value = mixed + batched); fp64 / mixed = one form through pa_df_4d")
+    ap.add_argument("--form", default="headline", choices=["headline", "fp64", "mixed", "mixed_split"],
+                    help="single-molecule workloads: headline = FP64 plain and both mixed + batched forms back "
+                         "to back (value = mixed + batched); fp64 / mixed / mixed_split = one form through "
+                         "pa_df_4d (mixed_split: weak triplets on the split-BF16 tensor-core kernels)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"], help="cfg4: precision of the batch")
     ap.add_argument("--boys", default=None, choices=["reference", "exact"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -552,8 +554,9 @@ def main():
     def set_form(form):
         # mixed_split_batched: the weak triplets on their own kernels with the
         # split-BF16 tensor-core product (pa_set_mixed_kernels(1))
-        nat.set_mixed_kernels(1 if form == "mixed_split_batched" else 0)
-        if form in ("mixed", "mixed_batched", "mixed_split_batched") or (form == "batched" and args.precision == "mixed"):
+        nat.set_mixed_kernels(1 if form in ("mixed_split_batched", "mixed_split") else 0)
+        if form in ("mixed", "mixed_split", "mixed_batched", "mixed_split_batched") or (
+                form == "batched" and args.precision == "mixed"):
             nat.set_precision("mixed", FP32_THRESH)
         else:
             nat.set_precision("fp64")
