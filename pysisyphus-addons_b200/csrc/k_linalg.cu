@@ -16,6 +16,8 @@
 
 #include "k_linalg.cuh"
 
+#include <cstdint>
+
 namespace pa {
 
 namespace {
@@ -402,9 +404,12 @@ __global__ void __launch_bounds__(256) k_gemm(int m, int n, int k, double alpha,
 // column-major, ldp, k <= NB). One block per 64 x 64 tile of that lower part:
 // blockIdx.x enumerates the triangle of the first ncols tile rows, then the
 // full tile rows below. Both panels of a tile are staged whole (every k at
-// once) by 8-byte cp.async copies (ldp may be odd), in rows of 68 doubles
-// (4 mod 16: conflict-free m8n8k4 fragment loads); three blocks per SM keep
-// one block's copies in flight during another's products. The products run
+// once) by cp.async copies (16 bytes when the columns are 16-byte aligned,
+// else 8 bytes: ldp may be odd), in rows of 68 doubles
+// (4 mod 16: conflict-free m8n8k4 fragment loads); two blocks per SM (128
+// registers: the C prefetch spills at three) keep one block's copies in
+// flight during another's products (standalone 13400 x 13400 factor: 66.0 ms
+// with three blocks and 8-byte copies, 49.2 ms now). The products run
 // in k_gemm's order (k ascending, four at a time, zeros up to a multiple of
 // 16), so the factor is the same bit for bit.
 constexpr int kSyrkLd = TM + 4;
@@ -415,8 +420,18 @@ __device__ __forceinline__ void cp_async8(double* smem_dst, const double* gmem_s
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gmem_src));
 }
 
-__global__ void __launch_bounds__(256, 3) k_syrk_update(int m, int ncols, int k, const double* __restrict__ P,
-                                                         long long ldp, double* C, long long ldc) {
+__device__ __forceinline__ void cp_async16_ld(double* smem_dst, const double* gmem_src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src));
+}
+
+// V16: the panel columns start on 16-byte boundaries (ldp even, P aligned), so
+// pairs of rows are copied 16 bytes at a time. The block's entries of C are
+// loaded into registers before the panels arrive, so their latency overlaps
+// the copies and the products.
+template <bool V16>
+__global__ void __launch_bounds__(256, 2) k_syrk_update(int m, int ncols, int k, const double* __restrict__ P,
+                                                        long long ldp, double* C, long long ldc) {
   extern __shared__ __align__(16) double sm[];
   double* As = sm;                  // As[c * kSyrkLd + r] = P[i0 + r, c]
   double* Bs = sm + NB * kSyrkLd;   // Bs[c * kSyrkLd + r] = P[j0 + r, c]
@@ -434,24 +449,56 @@ __global__ void __launch_bounds__(256, 3) k_syrk_update(int m, int ncols, int k,
   }
   const int i0 = bi * TM, j0 = bj * TN;
   const int kq = (k + TK - 1) / TK * TK;
-  for (int idx = threadIdx.x; idx < kq * TM; idx += 256) {
-    const int r = idx % TM, c = idx / TM;
-    double* da = As + c * kSyrkLd + r;
-    double* db = Bs + c * kSyrkLd + r;
-    if (c < k && i0 + r < m)
-      cp_async8(da, P + (i0 + r) + ldp * c);
-    else
-      *da = 0.0;
-    if (c < k && j0 + r < ncols)
-      cp_async8(db, P + (j0 + r) + ldp * c);
-    else
-      *db = 0.0;
+  if constexpr (V16) {
+    for (int idx = threadIdx.x; idx < kq * (TM / 2); idx += 256) {
+      const int r = 2 * (idx % (TM / 2)), c = idx / (TM / 2);
+      double* da = As + c * kSyrkLd + r;
+      double* db = Bs + c * kSyrkLd + r;
+      if (c < k && i0 + r + 1 < m) {
+        cp_async16_ld(da, P + (i0 + r) + ldp * c);
+      } else {
+        da[0] = (c < k && i0 + r < m) ? P[(i0 + r) + ldp * c] : 0.0;
+        da[1] = 0.0;
+      }
+      if (c < k && j0 + r + 1 < ncols) {
+        cp_async16_ld(db, P + (j0 + r) + ldp * c);
+      } else {
+        db[0] = (c < k && j0 + r < ncols) ? P[(j0 + r) + ldp * c] : 0.0;
+        db[1] = 0.0;
+      }
+    }
+  } else {
+    for (int idx = threadIdx.x; idx < kq * TM; idx += 256) {
+      const int r = idx % TM, c = idx / TM;
+      double* da = As + c * kSyrkLd + r;
+      double* db = Bs + c * kSyrkLd + r;
+      if (c < k && i0 + r < m)
+        cp_async8(da, P + (i0 + r) + ldp * c);
+      else
+        *da = 0.0;
+      if (c < k && j0 + r < ncols)
+        cp_async8(db, P + (j0 + r) + ldp * c);
+      else
+        *db = 0.0;
+    }
   }
-  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::);
-  __syncthreads();
+  asm volatile("cp.async.commit_group;\n" ::);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, t4 = lane & 3;
   const int wm = (warp & 3) * 16, wn = (warp >> 2) * 32;
+  // this thread's entries of C, in flight while the panels arrive
+  double cv[2][4][2];
+#pragma unroll
+  for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int gi = i0 + wm + 8 * mt + g, gj = j0 + wn + 8 * nt + 2 * t4 + i;
+        cv[mt][nt][i] = (gi < m && gj < ncols && gi >= gj) ? C[gi + ldc * gj] : 0.0;
+      }
+  asm volatile("cp.async.wait_group 0;\n" ::);
+  __syncthreads();
   double acc[2][4][2] = {};
 #pragma unroll 4
   for (int q = 0; q < kq; q += 4) {
@@ -472,10 +519,7 @@ __global__ void __launch_bounds__(256, 3) k_syrk_update(int m, int ncols, int k,
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
         const int gi = i0 + wm + 8 * mt + g, gj = j0 + wn + 8 * nt + 2 * t4 + i;
-        if (gi < m && gj < ncols && gi >= gj) {
-          double* c = C + gi + ldc * gj;
-          *c = *c + -1.0 * acc[mt][nt][i];
-        }
+        if (gi < m && gj < ncols && gi >= gj) C[gi + ldc * gj] = cv[mt][nt][i] + -1.0 * acc[mt][nt][i];
       }
 }
 
@@ -546,7 +590,10 @@ int syrk_update(int m, int ncols, int k, const double* P, long long ldp, double*
   if (m <= 0 || ncols <= 0) return 0;
   const long long nbr = (m + TM - 1) / TM, nbc = (ncols + TN - 1) / TN;
   const long long tiles = nbc * (nbc + 1) / 2 + (nbr - nbc) * nbc;
-  k_syrk_update<<<static_cast<unsigned>(tiles), 256, kSyrkSmem, s>>>(m, ncols, k, P, ldp, C, ldc);
+  if (ldp % 2 == 0 && reinterpret_cast<uintptr_t>(P) % 16 == 0)
+    k_syrk_update<true><<<static_cast<unsigned>(tiles), 256, kSyrkSmem, s>>>(m, ncols, k, P, ldp, C, ldc);
+  else
+    k_syrk_update<false><<<static_cast<unsigned>(tiles), 256, kSyrkSmem, s>>>(m, ncols, k, P, ldp, C, ldc);
   return 1;
 }
 
@@ -570,7 +617,8 @@ int cholesky_lower(double* A, int n, int* d_info, double* work, cudaStream_t s,
                        static_cast<int>(2 * kTileSmem));
   cudaFuncSetAttribute(k_potrf_diag_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        static_cast<int>(3 * kTileSmem));
-  cudaFuncSetAttribute(k_syrk_update, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSyrkSmem));
+  cudaFuncSetAttribute(k_syrk_update<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSyrkSmem));
+  cudaFuncSetAttribute(k_syrk_update<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSyrkSmem));
   cudaMemsetAsync(d_info, 0, sizeof(int), s);
   const int nblk = (n + NB - 1) / NB;
   bool rest_pending = false;  // a trailing update of the previous step is queued on la->aux
