@@ -32,6 +32,9 @@ struct BlockSync {
 };
 
 constexpr int kStdThreads = 128;
+// k_std_df2c_half: two blocks per SM (its shared memory: the integral
+// scratch and the half-transformed accumulator), so eight warps each
+constexpr int kStdHalfThreads = 256;
 constexpr int kLtot = 2 * PA_LMAX + PA_LAUXMAX;           // highest la + lb + lc
 constexpr int kNR = ncum(kLtot);                           // R entries of one build
 constexpr int kNHMax = ncum(2 * PA_LMAX);                  // Hermite components of a bra
@@ -166,7 +169,7 @@ __global__ void __launch_bounds__(kStdThreads) k_std_block_norm(StdArgs a, const
 }
 
 // One block per (aux shell c, target shell b, chunk of MOs).
-__global__ void __launch_bounds__(kStdThreads) k_std_df2c_half(StdArgs a, int c0, int k0, int nmos,
+__global__ void __launch_bounds__(kStdHalfThreads) k_std_df2c_half(StdArgs a, int c0, int k0, int nmos,
                                                                const double* __restrict__ mo,
                                                                double* __restrict__ W, int moc) {
   extern __shared__ double sm[];
@@ -268,7 +271,7 @@ int launch_std_df2c_half(const StdArgs& a, int c0, int c1, int k0, int nmos, con
   const size_t smem = sizeof(double) * (kBlk3cDoubles + kNSMax * moc + static_cast<size_t>(moc) * kNSMax * kNCMax);
   cudaFuncSetAttribute(k_std_df2c_half, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
   dim3 grid(c1 - c0, a.B.nshells, (nmos + moc - 1) / moc);
-  k_std_df2c_half<<<grid, kStdThreads, smem, s>>>(a, c0, k0, nmos, mo, W, moc);
+  k_std_df2c_half<<<grid, kStdHalfThreads, smem, s>>>(a, c0, k0, nmos, mo, W, moc);
   return 1;
 }
 
