@@ -22,9 +22,12 @@
 #include <dlfcn.h>
 #include <fstream>
 #include <mutex>
+#include <optional>
 #include <sstream>
 #include <string>
 #include <vector>
+
+#include <nvtx3/nvToolsExt.h>
 
 #include "boys.cuh"
 #include "k_df3c.cuh"
@@ -39,6 +42,16 @@ namespace pa {
 namespace {
 
 thread_local std::string tl_err;
+
+// NVTX range over the host-side enqueue of one phase (header-only NVTX v3:
+// no cost without a tool attached; Nsight Systems shows the ranges on the CPU
+// timeline, Nsight Compute can filter launches by them with --nvtx).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 int fail(int code, const std::string& msg) {
   tl_err = msg;
@@ -960,11 +973,18 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
   PA_CUDA(cudaEventRecord(ctx->fork, s));
   PA_CUDA(cudaEventRecord(ctx->ev_scr0, s));
   PA_CUDA(cudaStreamWaitEvent(ctx->sscr, ctx->ev_scr0, 0));
-  int st = run_screening(orb, aux, dt, o, b, ctx->sscr, launches);
+  int st = PA_OK;
+  {
+    NvtxRange r("pa: screening");
+    st = run_screening(orb, aux, dt, o, b, ctx->sscr, launches);
+  }
   if (st != PA_OK) return st;
   PA_CUDA(cudaStreamWaitEvent(s2, ctx->fork, 0));
   PA_CUDA(cudaEventRecord(ctx->m0, s2));
-  stage_metric(aux, b, dt, o, s2, &ctx->la2, launches);
+  {
+    NvtxRange r("pa: metric and Cholesky");
+    stage_metric(aux, b, dt, o, s2, &ctx->la2, launches);
+  }
   PA_CUDA(cudaEventRecord(ctx->m1, s2));
   PA_CUDA(cudaEventRecord(ctx->ev_scr1, ctx->sscr));
   PA_CUDA(cudaStreamWaitEvent(s, ctx->ev_scr1, 0));
@@ -979,10 +999,15 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
     PA_CUDA(cudaEventRecord(ctx->fork, s));
     for (int i = 0; i < Ctx::kNs3c; ++i) PA_CUDA(cudaStreamWaitEvent(ctx->s3c[i], ctx->fork, 0));
   }
-  stage_bra_prep(orb, aux, nd, d_dens, sd, si, sj, b, o, s, launches, ctx->ev_bra);
+  {
+    NvtxRange r("pa: density folding");
+    stage_bra_prep(orb, aux, nd, d_dens, sd, si, sj, b, o, s, launches, ctx->ev_bra);
+  }
   PA_CUDA(cudaEventRecord(ph[1], s));
   // three-center contraction: one persistent launch per class, on four streams
   const int before3c = *launches;
+  std::optional<NvtxRange> r3c;
+  r3c.emplace("pa: three-center classes");
   if (run3c) {
     // the runs come grouped by L_c: once a group is enqueued, the main stream
     // waits for the class streams and reduces that group while the next
@@ -1015,8 +1040,10 @@ int run_df(const pa_basis_s* orb, const pa_basis_s* aux, int nd, const double* d
     }
   }
   *launches_3c = *launches - before3c;
+  r3c.reset();
   PA_CUDA(cudaEventRecord(ph[2], s));
   PA_CUDA(cudaStreamWaitEvent(s, ctx->m1, 0));  // join the metric stream
+  NvtxRange rs("pa: solve");
   return stage_solve(aux, nd, b, o, d_df, s, launches);
 }
 
@@ -1352,6 +1379,7 @@ int record_batch(Ctx* c, BatchPlan& plan, const std::vector<BatchMol>& mols, con
 int batch_4d(int nmol, const pa_basis* orbs, const pa_basis* auxs, const int* ndens,
              const double* const* d_dens, int layout, const int* nstates, double* const* d_R,
              int use_graph, cudaStream_t user_stream) {
+  NvtxRange range("pa: batched Coulomb tensors");
   if (nmol < 0 || (nmol > 0 && (!orbs || !auxs || !ndens || !d_dens || !nstates || !d_R)))
     return fail(PA_ERR_ARG, "invalid batch arguments");
   if (layout != PA_LAYOUT_FORTRAN && layout != PA_LAYOUT_C) return fail(PA_ERR_ARG, "unknown layout");
@@ -1636,6 +1664,7 @@ constexpr size_t kStdWBudget = size_t(1) << 27;
 
 int std_device(pa_basis orb, pa_basis aux, int kind, int nmos, const double* d_mo, double* d_out,
                cudaStream_t s) {
+  NvtxRange range(kind == kStdDf1c ? "pa: std df1c" : (kind == kStdEri2c ? "pa: std eri2c" : "pa: std df2c_mo"));
   int st = check_pair(orb, aux);
   if (st != PA_OK) return st;
   if (kind == kStdDf2cMo && (nmos < 0 || (nmos > 0 && !d_mo))) return fail(PA_ERR_ARG, "invalid MO tensor");
