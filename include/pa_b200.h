@@ -156,6 +156,12 @@ int pa_get_mixed_kernels(void);
  * persistent blocks that pull work items until none is left, 1 = one block
  * per work item. */
 int pa_set_class_grid(int mode);
+/* The f_* entry points keep the device copies (with the shell-pair lists) of
+ * the last 8 bases they were given, for later calls with byte-identical basis
+ * arrays on the same device; pa_basis_cache_clear frees them. pa_get_device
+ * gives the CUDA device of the calling thread, on which calls run. */
+int pa_basis_cache_clear(void);
+int pa_get_device(int* device);
 /* Granularity of the three-center work queue: work items per SM and shell
  * class; 0 (default) picks it from the system size (2 at 40 atoms, 8 at 200).
  * Finer items shorten the tail of each class launch and cost more partial

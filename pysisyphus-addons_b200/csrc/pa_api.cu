@@ -21,6 +21,8 @@
 #include <cstring>
 #include <dlfcn.h>
 #include <fstream>
+#include <list>
+#include <memory>
 #include <mutex>
 #include <optional>
 #include <sstream>
@@ -1847,12 +1849,74 @@ int std_host(pa_basis orb, pa_basis aux, int kind, int nmos, const double* mo, d
   return PA_OK;
 }
 
+// Bases of the f_* entry points. Their callers pass the same basis arrays call
+// after call, so the unpacked basis with its device copy and shell-pair lists
+// is kept for later calls with byte-identical arrays (same device and angular
+// momentum limit): at most kBasisCacheSize per process, least recently used
+// first out. A call holds a reference for its duration, so an eviction by
+// another thread never frees a basis in use. pa_basis_cache_clear() empties
+// the cache.
+constexpr size_t kBasisCacheSize = 8;
+struct BasisEntry {
+  int device = 0, lmax = 0, nshells = 0, ndata = 0;
+  std::vector<int> centers, spec;
+  std::vector<double> data;
+  std::shared_ptr<pa_basis_s> basis;
+};
+struct BasisCache {
+  std::mutex mu;
+  std::list<BasisEntry> entries;  // most recently used first
+};
+// never destroyed: no device frees run during process teardown
+BasisCache& basis_cache() {
+  static BasisCache* c = new BasisCache();
+  return *c;
+}
+
 struct BasisGuard {
   pa_basis b = nullptr;
-  ~BasisGuard() {
-    if (b) pa_basis_destroy(b);
-  }
+  std::shared_ptr<pa_basis_s> keep;
 };
+
+int acquire_basis(int nshells, int ndata, const int* centers, const int* spec, const double* data, int lmax,
+                  BasisGuard* g) {
+  const bool valid = nshells >= 0 && ndata >= 0 && (nshells == 0 || (centers && spec)) && (ndata == 0 || data);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  BasisCache& cache = basis_cache();
+  if (valid) {
+    std::lock_guard<std::mutex> lk(cache.mu);
+    for (auto it = cache.entries.begin(); it != cache.entries.end(); ++it) {
+      if (it->device != dev || it->lmax != lmax || it->nshells != nshells || it->ndata != ndata) continue;
+      if (nshells > 0 && (std::memcmp(it->centers.data(), centers, sizeof(int) * 3 * nshells) != 0 ||
+                          std::memcmp(it->spec.data(), spec, sizeof(int) * 5 * nshells) != 0))
+        continue;
+      if (ndata > 0 && std::memcmp(it->data.data(), data, sizeof(double) * ndata) != 0) continue;
+      cache.entries.splice(cache.entries.begin(), cache.entries, it);
+      g->keep = cache.entries.front().basis;
+      g->b = g->keep.get();
+      return PA_OK;
+    }
+  }
+  pa_basis b = nullptr;
+  const int st = pa_basis_create(nshells, ndata, centers, spec, data, lmax, &b);
+  if (st != PA_OK) return st;
+  g->keep = std::shared_ptr<pa_basis_s>(b, [](pa_basis p) { pa_basis_destroy(p); });
+  g->b = b;
+  BasisEntry e;
+  e.device = dev;
+  e.lmax = lmax;
+  e.nshells = nshells;
+  e.ndata = ndata;
+  e.centers.assign(centers, centers + 3 * static_cast<size_t>(nshells));
+  e.spec.assign(spec, spec + 5 * static_cast<size_t>(nshells));
+  if (ndata > 0) e.data.assign(data, data + ndata);
+  e.basis = g->keep;
+  std::lock_guard<std::mutex> lk(cache.mu);
+  cache.entries.push_front(std::move(e));
+  while (cache.entries.size() > kBasisCacheSize) cache.entries.pop_back();
+  return PA_OK;
+}
 
 }  // namespace
 }  // namespace pa
@@ -1896,6 +1960,20 @@ int pa_set_precision(int mode, double fp32_thresh) {
 int pa_get_precision(void) {
   std::lock_guard<std::mutex> lk(g_opt_mu);
   return g_opts.precision;
+}
+
+int pa_basis_cache_clear(void) {
+  pa::BasisCache& cache = pa::basis_cache();
+  std::lock_guard<std::mutex> lk(cache.mu);
+  cache.entries.clear();
+  return PA_OK;
+}
+
+int pa_get_device(int* device) {
+  if (!device) return fail(PA_ERR_ARG, "null output pointer");
+  const cudaError_t e = cudaGetDevice(device);
+  if (e != cudaSuccess) return fail(PA_ERR_NO_DEVICE, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+  return PA_OK;
 }
 
 int pa_set_class_grid(int mode) {
@@ -2158,10 +2236,10 @@ int f_contract_coulomb_densities_2d(int nshells, int ndata, const int* bas_cente
                                     int ndens, int nbfs, const double* densities, int naux,
                                     double* df_tensor) {
   BasisGuard orb, aux;
-  int st = pa_basis_create(nshells, ndata, bas_centers, bas_spec, bas_data, PA_LMAX, &orb.b);
+  int st = acquire_basis(nshells, ndata, bas_centers, bas_spec, bas_data, PA_LMAX, &orb);
   if (st != PA_OK) return st;
-  st = pa_basis_create(nshells_aux, ndata_aux, bas_centers_aux, bas_spec_aux, bas_data_aux,
-                       PA_LAUXMAX, &aux.b);
+  st = acquire_basis(nshells_aux, ndata_aux, bas_centers_aux, bas_spec_aux, bas_data_aux,
+                       PA_LAUXMAX, &aux);
   if (st != PA_OK) return st;
   if (naux != aux.b->host.nsph)
     return fail(PA_ERR_ARG, "naux (" + std::to_string(naux) + ") does not match the auxiliary basis (" +
@@ -2178,10 +2256,10 @@ int f_contract_coulomb_densities_4d(int nshells, int ndata, const int* bas_cente
   if (nstates <= 0 || nstates * (nstates + 1) / 2 != ndens)
     return fail(PA_ERR_ARG, "ndens must equal nstates (nstates + 1) / 2");
   BasisGuard orb, aux;
-  int st = pa_basis_create(nshells, ndata, bas_centers, bas_spec, bas_data, PA_LMAX, &orb.b);
+  int st = acquire_basis(nshells, ndata, bas_centers, bas_spec, bas_data, PA_LMAX, &orb);
   if (st != PA_OK) return st;
-  st = pa_basis_create(nshells_aux, ndata_aux, bas_centers_aux, bas_spec_aux, bas_data_aux,
-                       PA_LAUXMAX, &aux.b);
+  st = acquire_basis(nshells_aux, ndata_aux, bas_centers_aux, bas_spec_aux, bas_data_aux,
+                       PA_LAUXMAX, &aux);
   if (st != PA_OK) return st;
   return df_host(orb.b, aux.b, ndens, nbfs, densities, PA_LAYOUT_FORTRAN, coulomb_tensor, nstates);
 }
@@ -2238,7 +2316,7 @@ static int schwarz_impl(pa_basis orb, pa_basis aux, double* q_bra, double* q_aux
 int f_int_schwarz_aux(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
                       const double* bas_data, double* integrals) {
   BasisGuard b;
-  int st = pa_basis_create(nshells, ndata, bas_centers, bas_spec, bas_data, PA_LAUXMAX, &b.b);
+  int st = acquire_basis(nshells, ndata, bas_centers, bas_spec, bas_data, PA_LAUXMAX, &b);
   if (st != PA_OK) return st;
   if (nshells > 0 && !integrals) return fail(PA_ERR_ARG, "null output pointer");
   return schwarz_impl(nullptr, b.b, nullptr, integrals);
@@ -2247,7 +2325,7 @@ int f_int_schwarz_aux(int nshells, int ndata, const int* bas_centers, const int*
 int f_int_schwarz_bra(int nshells, int ndata, const int* bas_centers, const int* bas_spec,
                       const double* bas_data, double* integrals) {
   BasisGuard b;
-  int st = pa_basis_create(nshells, ndata, bas_centers, bas_spec, bas_data, PA_LMAX, &b.b);
+  int st = acquire_basis(nshells, ndata, bas_centers, bas_spec, bas_data, PA_LMAX, &b);
   if (st != PA_OK) return st;
   if (nshells > 0 && !integrals) return fail(PA_ERR_ARG, "null output pointer");
   return schwarz_impl(b.b, nullptr, integrals, nullptr);
@@ -2464,9 +2542,9 @@ int f_benchmark_int3c2e(int nshells, int ndata, const int* bas_centers, const in
                         int nshells_aux, int ndata_aux, const int* bas_centers_aux, const int* bas_spec_aux,
                         const double* bas_data_aux) {
   BasisGuard orb, aux;
-  int st = pa_basis_create(nshells, ndata, bas_centers, bas_spec, bas_data, PA_LMAX, &orb.b);
+  int st = acquire_basis(nshells, ndata, bas_centers, bas_spec, bas_data, PA_LMAX, &orb);
   if (st != PA_OK) return st;
-  st = pa_basis_create(nshells_aux, ndata_aux, bas_centers_aux, bas_spec_aux, bas_data_aux, PA_LAUXMAX, &aux.b);
+  st = acquire_basis(nshells_aux, ndata_aux, bas_centers_aux, bas_spec_aux, bas_data_aux, PA_LAUXMAX, &aux);
   if (st != PA_OK) return st;
   std::printf("Main basis:%6d shells, %6d basis functions\n", nshells, orb.b->host.nsph);
   std::printf("Aux. basis:%6d shells, %6d basis functions\n", nshells_aux, aux.b->host.nsph);
@@ -2663,10 +2741,10 @@ int f_intor_eri2c(int nshells, int ndata, const int* bas_centers, const int* bas
                   const int* bas_centers_aux, const int* bas_spec_aux,
                   const double* bas_data_aux, int nbfs, double* eri2c_tensor) {
   BasisGuard orb, aux;
-  int st = pa_basis_create(nshells, ndata, bas_centers, bas_spec, bas_data, PA_LMAX, &orb.b);
+  int st = acquire_basis(nshells, ndata, bas_centers, bas_spec, bas_data, PA_LMAX, &orb);
   if (st != PA_OK) return st;
-  st = pa_basis_create(nshells_aux, ndata_aux, bas_centers_aux, bas_spec_aux, bas_data_aux,
-                       PA_LAUXMAX, &aux.b);
+  st = acquire_basis(nshells_aux, ndata_aux, bas_centers_aux, bas_spec_aux, bas_data_aux,
+                       PA_LAUXMAX, &aux);
   if (st != PA_OK) return st;
   if (nbfs != orb.b->host.nsph)
     return fail(PA_ERR_ARG, "nbfs does not match the orbital basis");
@@ -2680,10 +2758,10 @@ int f_intor_df1c(int nshells, int ndata, const int* bas_centers, const int* bas_
                  const int* bas_centers_aux, const int* bas_spec_aux, const double* bas_data_aux,
                  int nbfs, int nbfs_aux, double* df1c_tensor) {
   BasisGuard orb, aux;
-  int st = pa_basis_create(nshells, ndata, bas_centers, bas_spec, bas_data, PA_LMAX, &orb.b);
+  int st = acquire_basis(nshells, ndata, bas_centers, bas_spec, bas_data, PA_LMAX, &orb);
   if (st != PA_OK) return st;
-  st = pa_basis_create(nshells_aux, ndata_aux, bas_centers_aux, bas_spec_aux, bas_data_aux,
-                       PA_LAUXMAX, &aux.b);
+  st = acquire_basis(nshells_aux, ndata_aux, bas_centers_aux, bas_spec_aux, bas_data_aux,
+                       PA_LAUXMAX, &aux);
   if (st != PA_OK) return st;
   if (nbfs != orb.b->host.nsph || nbfs_aux != aux.b->host.nsph)
     return fail(PA_ERR_ARG, "nbfs / nbfs_aux do not match the bases");
@@ -2698,10 +2776,10 @@ int f_intor_df2c_mo(int nshells, int ndata, const int* bas_centers, const int* b
                     const double* bas_data_aux, int nbfs, int nmos, const double* mo_tensor,
                     int nbfs_aux, double* df2c_mo_tensor) {
   BasisGuard orb, aux;
-  int st = pa_basis_create(nshells, ndata, bas_centers, bas_spec, bas_data, PA_LMAX, &orb.b);
+  int st = acquire_basis(nshells, ndata, bas_centers, bas_spec, bas_data, PA_LMAX, &orb);
   if (st != PA_OK) return st;
-  st = pa_basis_create(nshells_aux, ndata_aux, bas_centers_aux, bas_spec_aux, bas_data_aux,
-                       PA_LAUXMAX, &aux.b);
+  st = acquire_basis(nshells_aux, ndata_aux, bas_centers_aux, bas_spec_aux, bas_data_aux,
+                       PA_LAUXMAX, &aux);
   if (st != PA_OK) return st;
   if (nbfs != orb.b->host.nsph || nbfs_aux != aux.b->host.nsph)
     return fail(PA_ERR_ARG, "nbfs / nbfs_aux do not match the bases");

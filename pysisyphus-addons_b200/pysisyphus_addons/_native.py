@@ -8,6 +8,8 @@ library has not been built, importing this module raises.
 
 import ctypes
 import os
+import threading
+from collections import OrderedDict
 from pathlib import Path
 
 import numpy as np
@@ -97,6 +99,8 @@ SIGNATURES = {
     "pa_get_precision": [],
     "pa_set_mixed_kernels": [_i],
     "pa_set_class_grid": [_i],
+    "pa_basis_cache_clear": [],
+    "pa_get_device": [_pi],
     "pa_get_mixed_kernels": [],
     "pa_set_screening": [_i],
     "pa_get_screening": [],
@@ -303,9 +307,9 @@ def boys(nmax, T, mode="reference"):
 class Basis:
     """A basis unpacked, normalized and resident in device memory (pa_basis)."""
 
-    def __init__(self, shells, role="orbital"):
+    def __init__(self, shells, role="orbital", _args=None):
         lib = load()
-        keep, args = basis_args(shells)
+        keep, args = _args if _args is not None else basis_args(shells)
         lmax = PA_LMAX_ORBITAL if role == "orbital" else PA_LMAX_AUX
         handle = _vp()
         check(lib.pa_basis_create(*args, lmax, ctypes.byref(handle)))
@@ -325,6 +329,45 @@ class Basis:
             self.close()
         except Exception:
             pass
+
+
+def current_device():
+    """The CUDA device the next library call runs on (of the calling thread)."""
+    d = _i()
+    check(load().pa_get_device(ctypes.byref(d)))
+    return d.value
+
+
+# Bases of the reference-facing functions: callers pass the same shells call
+# after call, so the device copy (with its shell-pair lists, built on first use)
+# is kept for later calls with byte-identical basis arrays on the same device;
+# least recently used first out.
+BASIS_CACHE_SIZE = 8
+_basis_cache = OrderedDict()
+_basis_lock = threading.Lock()
+
+
+def cached_basis(shells, role="orbital"):
+    keep, args = basis_args(shells)
+    key = (current_device(), role) + tuple((a.shape, a.tobytes()) for a in keep)
+    with _basis_lock:
+        b = _basis_cache.get(key)
+        if b is not None:
+            _basis_cache.move_to_end(key)
+            return b
+    b = Basis(shells, role, _args=(keep, args))
+    with _basis_lock:
+        _basis_cache[key] = b
+        while len(_basis_cache) > BASIS_CACHE_SIZE:
+            _basis_cache.popitem(last=False)
+    return b
+
+
+def clear_basis_cache():
+    """Frees the cached device bases of this module and of the f_* entry points."""
+    with _basis_lock:
+        _basis_cache.clear()
+    check(load().pa_basis_cache_clear())
 
 
 def count_triplets(orbital, aux):

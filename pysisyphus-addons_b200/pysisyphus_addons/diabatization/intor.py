@@ -24,8 +24,8 @@ def contract_coulomb_densities_2d(shells, shells_aux, densities):
     (diabatization/intor.f90:28-200)."""
     D, layout = _densities(densities)
     ndens, nbf, _ = D.shape
-    orb = nat.Basis(shells, "orbital")
-    aux = nat.Basis(shells_aux, "aux")
+    orb = nat.cached_basis(shells, "orbital")
+    aux = nat.cached_basis(shells_aux, "aux")
     out = np.zeros((aux.nsph, ndens), dtype=np.float64, order="F")
     nat.check(nat.load().pa_contract_coulomb_densities_2d(orb.handle, aux.handle, ndens, nbf,
                                                           nat.ptr(D), layout, nat.ptr(out)))
@@ -39,8 +39,8 @@ def contract_coulomb_densities_4d(shells, shells_aux, densities):
     ndens, nbf, _ = D.shape
     nstates = int(math.isqrt(8 * ndens + 1) / 2.0 - 0.5)
     assert nstates * (nstates + 1) // 2 == ndens
-    orb = nat.Basis(shells, "orbital")
-    aux = nat.Basis(shells_aux, "aux")
+    orb = nat.cached_basis(shells, "orbital")
+    aux = nat.cached_basis(shells_aux, "aux")
     out = np.zeros((nstates,) * 4, dtype=np.float64, order="F")
     nat.check(nat.load().pa_contract_coulomb_densities_4d(orb.handle, aux.handle, ndens, nbf,
                                                           nat.ptr(D), layout, nstates,
