@@ -463,14 +463,19 @@ def precision_report(args):
             nat.set_skip_metric(0)
 
     res = {}
-    for prec, thr in (("fp64", 0.0), ("mixed", 1e-8), ("mixed", 1e-6), ("mixed", 1e-4)):
-        nat.set_precision(prec, thr)
+    # mixed = FP32 recurrences inside the FP64 kernels; mixed_split = the weak
+    # triplets on their own kernels with the split-BF16 tensor-core product
+    for prec, thr, kernels in (("fp64", 0.0, 0), ("mixed", 1e-8, 0), ("mixed", 1e-6, 0), ("mixed", 1e-4, 0),
+                               ("mixed_split", 1e-8, 1), ("mixed_split", 1e-6, 1), ("mixed_split", 1e-4, 1)):
+        nat.set_precision("fp64" if prec == "fp64" else "mixed", thr)
+        nat.set_mixed_kernels(kernels)
         t = {"raw": run(1, False)[0], "df": run(0, False)[0], "R": run(0, True)[0]}
         times = [run(0, True)[1] for _ in range(6)][2:]
         t["ms_total"] = statistics.median(x["ms_total"] for x in times)
         t["ms_3c"] = statistics.median(x["ms_3c"] for x in times)
         res[f"{prec}@{thr:g}"] = t
     nat.set_precision("fp64", 0.0)
+    nat.set_mixed_kernels(0)
     base = res["fp64@0"]
     fixture = None
     if args.config == "cfg2" and args.boys == "reference":

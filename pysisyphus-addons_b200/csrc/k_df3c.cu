@@ -13,24 +13,50 @@ namespace pa {
 namespace {
 
 // df_raw[sph_off(P) + m][d] (column-major, naux rows) = sum over LAB classes and
-// bra chunks of the partial slabs of class LC.
-__global__ void k_df3c_reduce(Df3cReduceArgs r) {
+// bra chunks of the partial slabs of class LC. A block takes 32 consecutive
+// outputs (one per lane, coalesced reads of every slab); its eight warps sum
+// eight consecutive ranges of the slab sequence (classes in L_ab order, chunks
+// in order), and warp 0 adds the eight partial sums in order: a fixed order,
+// so the results are deterministic, with dependent chains an eighth as long.
+__global__ void __launch_bounds__(256) k_df3c_reduce(Df3cReduceArgs r) {
+  __shared__ double part[8][32];
   const long long total = static_cast<long long>(r.n_aux) * r.nc * r.nd;
-  for (long long idx = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; idx < total;
-       idx += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const long long fn = idx / r.nd;
-    const int d = static_cast<int>(idx - fn * r.nd);
+  const long long slab = static_cast<long long>(r.n_aux) * r.nc * r.nd;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int nslabs = 0;
+  for (int c = 0; c < r.nclasses; ++c)
+    if (r.part[c]) nslabs += r.ny[c];
+  const int j0 = static_cast<int>(static_cast<long long>(nslabs) * w / 8);
+  const int j1 = static_cast<int>(static_cast<long long>(nslabs) * (w + 1) / 8);
+  for (long long base = blockIdx.x * 32LL; base < total; base += gridDim.x * 32LL) {
+    const long long idx = base + lane;
     double s = 0.0;
-    for (int c = 0; c < r.nclasses; ++c) {
-      const double* p = r.part[c];
-      if (!p) continue;
-      const long long slab = static_cast<long long>(r.n_aux) * r.nc * r.nd;
-      for (int y = 0; y < r.ny[c]; ++y) s += p[y * slab + fn * r.nd + d];
+    if (idx < total) {
+      int j = 0;
+      for (int c = 0; c < r.nclasses && j < j1; ++c) {
+        const double* p = r.part[c];
+        if (!p) continue;
+        const int ny = r.ny[c];
+        // chunks y of this class with j0 <= j + y < j1
+        const int y0 = max(0, j0 - j), y1 = min(ny, j1 - j);
+        for (int y = y0; y < y1; ++y) s += p[y * slab + idx];
+        j += ny;
+      }
     }
-    const int pos = static_cast<int>(fn / r.nc), m = static_cast<int>(fn - pos * r.nc);
-    const int sh = r.sorted_aux[r.aux_slot0 + pos];
-    const long long row = r.X.shell[sh].w + m;
-    r.df[row + static_cast<long long>(r.naux) * d] = s;
+    part[w][lane] = s;
+    __syncthreads();
+    if (w == 0 && idx < total) {
+      double t = part[0][lane];
+#pragma unroll
+      for (int k = 1; k < 8; ++k) t += part[k][lane];
+      const long long fn = idx / r.nd;
+      const int d = static_cast<int>(idx - fn * r.nd);
+      const int pos = static_cast<int>(fn / r.nc), m = static_cast<int>(fn - pos * r.nc);
+      const int sh = r.sorted_aux[r.aux_slot0 + pos];
+      const long long row = r.X.shell[sh].w + m;
+      r.df[row + static_cast<long long>(r.naux) * d] = t;
+    }
+    __syncthreads();
   }
 }
 
@@ -85,7 +111,7 @@ int launch_df3c_class_batch(int lab, int lc, int variant, const Df3cArgs* d_args
 int launch_df3c_reduce(const Df3cReduceArgs& r, cudaStream_t s) {
   const long long total = static_cast<long long>(r.n_aux) * r.nc * r.nd;
   if (total == 0) return 0;
-  const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148 * 16));
+  const int blocks = static_cast<int>(std::min<long long>((total + 31) / 32, 148 * 8));
   k_df3c_reduce<<<blocks, 256, 0, s>>>(r);
   return 1;
 }
