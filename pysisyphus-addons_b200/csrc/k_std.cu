@@ -185,33 +185,56 @@ __global__ void __launch_bounds__(kStdHalfThreads) k_std_df2c_half(StdArgs a, in
   const int nw = nm * nb * NC;
   for (int i = tid; i < nw; i += blockDim.x) Wacc[i] = 0.0;
   const double qc = a.Qc[c];
-  for (int sh = 0; sh < a.B.nshells; ++sh) {
-    const int hi = max(sh, b), lo = min(sh, b);
-    const int pair = hi * (hi + 1) / 2 + lo;
-    if (a.Qab[pair] * qc < a.thresh) continue;  // schwarz_estimate(a, b, c) < 1e-10
-    block_3c(a, pair, c, s);
-    const int4 sa = a.B.shell[sh];
-    const int na = 2 * sa.x + 1;
-    for (int i = tid; i < na * nm; i += blockDim.x) {
-      const int ii = i / nm, mm = i - ii * nm;
-      Cs[ii * moc + mm] = mo[(sa.w + ii) + static_cast<long long>(nbf) * (mo0 + mm)];
-    }
-    for (int i = tid; i < na * nb * NC; i += blockDim.x)
-      if (fabs(s.I[i]) <= kSkip1) s.I[i] = 0.0;
-    __syncthreads();
-    // h[mo][j][m] = sum_(i in a) C[i, mo] (a_i b_j | c_m); the stored block is
-    // (hi lo | c), so (a b|c) is its transpose when a < b
-    const bool a_first = sh >= b;
-    for (int idx = tid; idx < nw; idx += blockDim.x) {
-      const int mm = idx / (nb * NC), rem = idx - mm * (nb * NC);
-      const int j = rem / NC, m = rem - j * NC;
-      double h = 0.0;
-      for (int i = 0; i < na; ++i) {
-        const double iv = a_first ? s.I[(i * nb + j) * NC + m] : s.I[(j * na + i) * NC + m];
-        h = fma(Cs[i * moc + mm], iv, h);
+  // partners in ascending order (the reference's loop order), tested
+  // kStdHalfThreads at a time: each thread tests one partner, the warps'
+  // ballots go to shared memory, and the block walks the surviving partners
+  // of the chunk bit by bit (warp by warp)
+  __shared__ unsigned s_alive[kStdHalfThreads / 32];
+  for (int sh0 = 0; sh0 < a.B.nshells; sh0 += kStdHalfThreads) {
+    {
+      const int sh = sh0 + tid;
+      bool alive = false;
+      if (sh < a.B.nshells) {
+        const int hi = max(sh, b), lo = min(sh, b);
+        alive = !(a.Qab[hi * (hi + 1) / 2 + lo] * qc < a.thresh);  // schwarz_estimate(a, b, c) >= 1e-10
       }
-      if (fabs(h) > kSkip2) Wacc[idx] += h;
+      const unsigned m = __ballot_sync(0xffffffffu, alive);
+      if ((tid & 31) == 0) s_alive[tid >> 5] = m;
     }
+    __syncthreads();
+    for (int wi = 0; wi < kStdHalfThreads / 32; ++wi) {
+      unsigned m = s_alive[wi];
+      while (m) {
+        const int sh = sh0 + 32 * wi + __ffs(m) - 1;
+        m &= m - 1;
+        const int hi = max(sh, b), lo = min(sh, b);
+        const int pair = hi * (hi + 1) / 2 + lo;
+        block_3c(a, pair, c, s);
+        const int4 sa = a.B.shell[sh];
+        const int na = 2 * sa.x + 1;
+        for (int i = tid; i < na * nm; i += blockDim.x) {
+          const int ii = i / nm, mm = i - ii * nm;
+          Cs[ii * moc + mm] = mo[(sa.w + ii) + static_cast<long long>(nbf) * (mo0 + mm)];
+        }
+        for (int i = tid; i < na * nb * NC; i += blockDim.x)
+          if (fabs(s.I[i]) <= kSkip1) s.I[i] = 0.0;
+        __syncthreads();
+        // h[mo][j][m] = sum_(i in a) C[i, mo] (a_i b_j | c_m); the stored block is
+        // (hi lo | c), so (a b|c) is its transpose when a < b
+        const bool a_first = sh >= b;
+        for (int idx = tid; idx < nw; idx += blockDim.x) {
+          const int mm = idx / (nb * NC), rem = idx - mm * (nb * NC);
+          const int j = rem / NC, m = rem - j * NC;
+          double h = 0.0;
+          for (int i = 0; i < na; ++i) {
+            const double iv = a_first ? s.I[(i * nb + j) * NC + m] : s.I[(j * na + i) * NC + m];
+            h = fma(Cs[i * moc + mm], iv, h);
+          }
+          if (fabs(h) > kSkip2) Wacc[idx] += h;
+        }
+      }
+    }
+    __syncthreads();  // s_alive is rewritten by the next chunk
   }
   __syncthreads();
   for (int idx = tid; idx < nw; idx += blockDim.x) {
