@@ -630,7 +630,7 @@ struct DfBuffers {
   int dw = 8;                        // density chunk width of G (multiple of 8, <= 40)
   bool split = false;                // mixed form: the weak triplets run on their own kernels
   struct ClassRun {
-    int lab, lc, ny, upc;
+    int lab, lc, ny;
     double* partial;
     int variant;  // tile-shape variant of the class kernel
     bool weak;    // weak-triplet kernel (mixed form)
@@ -760,7 +760,7 @@ void layout_df(Carver& c, const pa_basis_s* orb, const pa_basis_s* aux, int nd, 
         int upc = (nu + ny - 1) / ny;
         upc = ((upc + ci.ub - 1) / ci.ub) * ci.ub;
         ny = (nu + upc - 1) / upc;
-        DfBuffers::ClassRun r{lab, lc, ny, upc, nullptr, variant, weak != 0};
+        DfBuffers::ClassRun r{lab, lc, ny, nullptr, variant, weak != 0};
         b->runs.push_back(r);
         part_total += static_cast<size_t>(ny) * nxc * (2 * lc + 1) * nd;
       }

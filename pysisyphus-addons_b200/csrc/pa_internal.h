@@ -152,24 +152,4 @@ int launch_schwarz_aux(const DevBasis& X, const DeviceTables& dt, int boys_mode,
 int launch_metric(const DevBasis& X, const DeviceTables& dt, int boys_mode, double* M,
                   cudaStream_t s);
 
-// 3c2e contraction with densities for all classes.
-struct Df3cPlan {
-  // sorted (by Q desc within class) unit slots
-  int lab_max = 0, lc_max = 0;
-  std::vector<int> unit_class_off;  // [lab_max + 2]
-  std::vector<int> aux_class_off;   // [lc_max + 2]
-  int nd = 0;
-};
-
-struct Df3cDev {
-  const int* sorted_unit;    // slot -> unit (host order id)
-  const double* unit_Q;      // slot -> Q (sorted)
-  double4* slot_pP;          // slot -> (p, P)
-  double* G;                 // G blocks per slot: class offsets g_off[c]
-  const long long* g_off;    // host array copy is in plan
-  const int* sorted_aux;     // aux slot -> shell
-  const double* aux_Q;       // aux slot -> Q (sorted)
-  double* partial;
-};
-
 }  // namespace pa
