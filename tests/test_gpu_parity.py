@@ -171,6 +171,29 @@ def test_deterministic():
     np.testing.assert_array_equal(a, b)
 
 
+def test_class_grid_forms_agree():
+    """One block per work item (pa_set_class_grid(1)) and persistent blocks run
+    the same items into the same partial slabs: the same tensor bit for bit,
+    in the FP64 form and with the weak-triplet kernels."""
+    w = config_workload("cfg2")
+    lib = nat.load()
+    try:
+        for mixed in (None, 1):
+            if mixed:
+                nat.set_precision("mixed", 1e-6)
+                nat.set_mixed_kernels(mixed)
+            nat.check(lib.pa_set_class_grid(0))
+            a = dia.contract_coulomb_densities_4d(w.shells, w.shells_aux, w.densities)
+            nat.check(lib.pa_set_class_grid(1))
+            b = dia.contract_coulomb_densities_4d(w.shells, w.shells_aux, w.densities)
+            np.testing.assert_array_equal(a, b)
+    finally:
+        nat.check(lib.pa_set_class_grid(0))
+        nat.set_precision("fp64")
+        nat.set_mixed_kernels(0)
+    assert lib.pa_set_class_grid(2) == nat.PA_ERR_ARG
+
+
 def test_screening_counts_match_oracle():
     w = config_workload("cfg1")
     oracle.set_boys_mode("reference")
