@@ -465,10 +465,14 @@ struct SwBlk {
   static constexpr int KT = (NH + 3) / 4;
   // Rn, R0, R1, Z_i [NH][nab], A [nab][nab]
   static constexpr int SMEM = 32 + 2 * NR + NH * NABM + NABM * NABM;
+  // blocks per SM that the shared memory allows (at most 4): the register
+  // budget of the launch follows from it
+  static constexpr int fit = (227 * 1024) / (SMEM * 8 + 1024);
+  static constexpr int kMinBlocks = fit < 1 ? 1 : (fit > 4 ? 4 : fit);
 };
 
 template <int LAB>
-__global__ void __launch_bounds__(32 * kSbWarps) k_schwarz_bra(DevBasis B, const int2* __restrict__ pair_ab,
+__global__ void __launch_bounds__(32 * kSbWarps, SwBlk<LAB>::kMinBlocks) k_schwarz_bra(DevBasis B, const int2* __restrict__ pair_ab,
                                                             const int* __restrict__ pair_unit0,
                                                             const int* __restrict__ pair_list, UnitArrays U,
                                                             int npairs, DeviceTables dt, int boys_mode,
@@ -515,6 +519,9 @@ __global__ void __launch_bounds__(32 * kSbWarps) k_schwarz_bra(DevBasis B, const
         const int mt = tile / ntr, nt = tile - mt * ntr;
         const int t = 8 * mt + g, c = 8 * nt + g;
         double z0 = 0.0, z1 = 0.0;
+        // unrolled: the index, R and E loads of several k steps in flight
+        // ahead of the products (same k order, same results)
+#pragma unroll 7
         for (int k4 = 0; k4 < KT; ++k4) {
           const int tp = 4 * k4 + t4;
           const double a = (t < NH && tp < NH) ? R0[__ldg(dt.sum_idx + t * kNSum + tp)] : 0.0;
@@ -536,6 +543,7 @@ __global__ void __launch_bounds__(32 * kSbWarps) k_schwarz_bra(DevBasis B, const
       const int mt = tile / ntr, nt = tile - mt * ntr;
       const int r = 8 * mt + g, c = 8 * nt + g;
       double o0 = 0.0, o1 = 0.0;
+#pragma unroll 7
       for (int k4 = 0; k4 < KT; ++k4) {
         const int t = 4 * k4 + t4;
         const double a = (r < nab && t < NH) ? Ei[r * NH + t] : 0.0;
