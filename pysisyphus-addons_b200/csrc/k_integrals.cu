@@ -80,26 +80,45 @@ __global__ void __launch_bounds__(128) k_unit_setup(DevBasis B, const int2* __re
   }
   __syncthreads();
   const IndexTables* it = dt.idx;
-  const int nsb = 2 * lb + 1;
-  const int nab = (2 * la + 1) * nsb;
+  const int nsa = 2 * la + 1, nsb = 2 * lb + 1;
+  const int nab = nsa * nsb;
   const int NH = ncum(la + lb);
   const int nt = la + lb + 1, nj = lb + 1;
   const int offa = ncum(la - 1 < 0 ? -1 : la - 1), offb = ncum(lb - 1 < 0 ? -1 : lb - 1);
   const double pref = sh[4];
   double* out = U.esph + U.unit_esph[u];
+  // the sparse solid-harmonic rows of both shells (coefficients and decoded
+  // Cartesian powers) in shared memory: the inner loop below reads no table
+  // from global memory; same terms in the same order as the table rows
+  constexpr int kRowMax = ncart(PA_LMAX);
+  __shared__ double rv[2][2 * PA_LMAX + 1][kRowMax];
+  __shared__ uchar4 rx[2][2 * PA_LMAX + 1][kRowMax];
+  __shared__ int rn[2][2 * PA_LMAX + 1];
+  for (int i = threadIdx.x; i < nsa + nsb; i += blockDim.x) {
+    const int side = i < nsa ? 0 : 1, m = side ? i - nsa : i;
+    const int l = side ? lb : la, off = side ? offb : offa;
+    const int row = sph_row(l, m);
+    const int k0 = dt.sph_start[row], k1 = dt.sph_start[row + 1];
+    rn[side][m] = k1 - k0;
+    for (int k = k0; k < k1; ++k) {
+      rv[side][m][k - k0] = dt.sph_val[k];
+      rx[side][m][k - k0] = *reinterpret_cast<const uchar4*>(it->xyz[off + dt.sph_col[k]]);
+    }
+  }
+  __syncthreads();
   for (int idx = threadIdx.x; idx < nab * NH; idx += blockDim.x) {
     const int r = idx / NH, t = idx - r * NH;
     const int ma = r / nsb, mb = r - ma * nsb;
     const uchar4 tt = *reinterpret_cast<const uchar4*>(it->xyz[t]);
-    const int rowa = sph_row(la, ma), rowb = sph_row(lb, mb);
+    const int na = rn[0][ma], nbk = rn[1][mb];
     double v = 0.0;
-    for (int ka = dt.sph_start[rowa]; ka < dt.sph_start[rowa + 1]; ++ka) {
-      const uchar4 ea = *reinterpret_cast<const uchar4*>(it->xyz[offa + dt.sph_col[ka]]);
-      const double ca = dt.sph_val[ka];
-      for (int kb = dt.sph_start[rowb]; kb < dt.sph_start[rowb + 1]; ++kb) {
-        const uchar4 eb = *reinterpret_cast<const uchar4*>(it->xyz[offb + dt.sph_col[kb]]);
+    for (int ka = 0; ka < na; ++ka) {
+      const uchar4 ea = rx[0][ma][ka];
+      const double ca = rv[0][ma][ka];
+      for (int kb = 0; kb < nbk; ++kb) {
+        const uchar4 eb = rx[1][mb][kb];
         if (tt.x > ea.x + eb.x || tt.y > ea.y + eb.y || tt.z > ea.z + eb.z) continue;
-        v += ca * dt.sph_val[kb] * E[0][(ea.x * nj + eb.x) * nt + tt.x] *
+        v += ca * rv[1][mb][kb] * E[0][(ea.x * nj + eb.x) * nt + tt.x] *
              E[1][(ea.y * nj + eb.y) * nt + tt.y] * E[2][(ea.z * nj + eb.z) * nt + tt.z];
       }
     }
