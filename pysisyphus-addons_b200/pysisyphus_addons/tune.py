@@ -44,7 +44,7 @@ def choose(times, margin=0.03, shapes=None):
     above 1 + margin. shapes ({(lab, lc): {variant: shape}}, optional) drops
     variants whose shape equals a lower variant's: they run the same kernel,
     so their differences are timing noise. Classes missing from a workload's
-    variant-0 run are judged on the other workloads."""
+    variant-0 run are decided by the other workloads."""
     ratios = {}
     for per_v in times.values():
         base = per_v.get(0, {})
